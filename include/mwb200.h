@@ -1,0 +1,106 @@
+/* mwb200.h -- C-ABI of the B200-native multiwavelet (MW) operator apply.
+ *
+ * Plain pointers and sizes only; every entry point returns an int status (0 = ok, < 0 = error) and
+ * never throws.  The text of the last error on the calling thread is returned by mw_last_error().
+ * The C++ front-end in mrcpp_b200.h maps a non-zero status to the reference's abort convention
+ * (MSG_FATAL), and the Python mirror (mrchem_b200/mrcpp.py) maps it to an exception.
+ *
+ * Each entry point names the reference interface it replaces.  The reference (MRChem) calls these
+ * MRCPP functions; MRCPP itself is an un-vendored submodule (.gitmodules:4-6), so the citations are
+ * the reference's call sites, which fix the contract.
+ *
+ * Data layout shared by every tree buffer crossing this boundary:
+ *   node i: depth[i] (0 = root scale n0 = min_scale), translation trans[3*i+d] >= 0 relative to the
+ *   world corner at that depth, parent[i] (-1 for roots), child0[i] (index of the first of 8
+ *   consecutive children, child c = cx + 2 cy + 4 cz; -1 for leaves), and coef[i*(2k)^3 ...]: the
+ *   node block as a (2k)^3 tensor, x fastest, per-dimension index a = c*k + j with c = 0 scaling /
+ *   1 wavelet (compressed form).  Parents precede children.
+ */
+#ifndef MWB200_H
+#define MWB200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct mw_ctx_s* mw_ctx;   /* device + stream + memory pool */
+typedef struct mw_mra_s* mw_mra;   /* world, basis, filters (host and device copies) */
+typedef struct mw_tree_s* mw_tree; /* one function: device SoA node arrays + hash index */
+typedef struct mw_op_s* mw_op;     /* separated-Gaussian convolution operator, device tables */
+
+enum { MW_OK = 0, MW_ERR_ARG = -1, MW_ERR_CUDA = -2, MW_ERR_STATE = -3, MW_ERR_CAPACITY = -4 };
+enum { MW_BASIS_INTERPOLATING = 0, MW_BASIS_LEGENDRE = 1 };
+enum { MW_FUNC_GAUSSIANS = 1, MW_FUNC_HYDROGEN_PRODUCTS = 2 };
+/* apply flags */
+enum { MW_APPLY_FP64 = 0 };
+
+const char* mw_last_error(void);
+int mw_version(int* major, int* minor);
+
+/* Device context on CUDA device `device`; work is issued on `stream` (NULL = a private stream). */
+int mw_ctx_create(int device, void* stream, mw_ctx* out);
+int mw_ctx_destroy(mw_ctx ctx);
+int mw_ctx_synchronize(mw_ctx ctx);
+
+/* World and basis.  Replaces BoundingBox<3>(min_scale, corner, boxes) +
+ * InterpolatingBasis(order) / LegendreBasis(order) + MultiResolutionAnalysis<3>(world, basis,
+ * max_depth): reference src/mrenv.cpp:52,64-72 and tests/unit_tests.cpp:36-43. */
+int mw_mra_create(mw_ctx ctx, int min_scale, const int* corner, const int* boxes, int basis_type,
+                  int order, int max_depth, mw_mra* out);
+int mw_mra_destroy(mw_mra mra);
+/* (2k)x(2k) two-scale filter [[H0 H1];[G0 G1]], row-major */
+int mw_mra_filter(mw_mra mra, double* F);
+/* effective depth limit (max_depth clamped to the 19-bit translation key) */
+int mw_mra_max_depth(mw_mra mra, int* depth);
+
+/* Function trees.  Replaces FunctionTree<3>(const MRA&): reference src/qmfunctions/QMFunction.cpp:68-77. */
+int mw_tree_create(mw_mra mra, mw_tree* out);
+int mw_tree_destroy(mw_tree tree);
+/* getNNodes / getSquareNorm: reference src/scf_solver/HelmholtzVector.cpp:84-89 */
+int mw_tree_nnodes(mw_tree tree, int* n);
+int mw_tree_square_norm(mw_tree tree, double* out);
+/* copy a host tree (layout above) to the device; builds the hash index and norms */
+int mw_tree_upload(mw_tree tree, int n, const int* depth, const long long* trans, const int* parent,
+                   const int* child0, const double* coef);
+/* copy the device tree to host buffers sized with mw_tree_nnodes (any pointer may be NULL) */
+int mw_tree_download(mw_tree tree, int* depth, long long* trans, int* parent, int* child0, double* coef);
+/* device pointers of the node arrays (coef: n*(2k)^3 doubles, key: n uint64, norm2: n doubles) */
+int mw_tree_device_arrays(mw_tree tree, void** coef, void** key, void** norm2);
+/* rescale(c): reference src/scf_solver/HelmholtzVector.cpp:81 (out[i].rescale(-1/2pi)) */
+int mw_tree_rescale(mw_tree tree, double c);
+
+/* Adaptive projection of an analytic function on the device.  Replaces mrcpp::project(prec, tree, f):
+ * reference src/qmfunctions/qmfunction_utils.cpp:88-114, src/initial_guess/gto.cpp:159.
+ *   MW_FUNC_GAUSSIANS: params = [ng, then per Gaussian: c, alpha, X, Y, Z, px, py, pz]
+ *     f(r) = sum c (x-X)^px (y-Y)^py (z-Z)^pz exp(-alpha |r-R|^2)
+ *   MW_FUNC_HYDROGEN_PRODUCTS: params = [nt, then per term: c, n1, l1, m1, n2, l2, m2, Z, ox, oy, oz]
+ *     f(r) = sum c phi_{n1 l1 m1}(r) phi_{n2 l2 m2}(r) (n2 = 0: no second factor), orbitals as in
+ *     reference src/analyticfunctions/HydrogenFunction.cpp:28-160. */
+int mw_project(double prec, mw_tree tree, int func_type, int nparams, const double* params);
+
+/* Inner product <a|b> of two compressed trees (reference: orbital::dot via mrcpp::dot,
+ * tests/qmoperators/coulomb_operator.cpp:90). */
+int mw_dot(mw_tree a, mw_tree b, double* out);
+
+/* Convolution operators.  Replace mrcpp::PoissonOperator(MRA, prec) (reference src/SCFDriver.cpp:279,
+ * tests/qmoperators/coulomb_operator.cpp:84) and mrcpp::HelmholtzOperator(MRA, mu, prec)
+ * (reference src/scf_solver/HelmholtzVector.cpp:171).  Kernels 1/|r| and exp(-mu|r|)/|r|. */
+int mw_op_create_poisson(mw_mra mra, double prec, mw_op* out);
+int mw_op_create_helmholtz(mw_mra mra, double mu, double prec, mw_op* out);
+int mw_op_destroy(mw_op op);
+int mw_op_nterms(mw_op op, int* n);
+int mw_op_terms(mw_op op, double* alpha, double* beta);
+
+/* out = op * inp, adaptive.  Replaces mrcpp::apply(prec, out, op, inp): reference
+ * src/scf_solver/HelmholtzVector.cpp:176,180, src/qmoperators/two_electron/CoulombPotential.cpp:85,
+ * src/qmoperators/two_electron/ExchangePotential.cpp:137,259,318.  `out` is overwritten and left
+ * compressed with valid norms. */
+int mw_apply(double prec, mw_tree out, mw_op op, mw_tree inp, int flags);
+/* statistics of the last apply into `out`: [0] contracted (out node, in node, term) triples,
+ * [1] of which with a generated input node, [2] refinement passes, [3] output nodes */
+int mw_apply_stats(mw_tree out, long long* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MWB200_H */

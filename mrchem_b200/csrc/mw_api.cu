@@ -1,0 +1,846 @@
+// mw_api.cu -- host driver behind the C-ABI (include/mwb200.h): contexts, worlds, device trees,
+// operator tables, and the adaptive projection / apply loops that issue the sm_100a kernels.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <string>
+#include <tuple>
+
+#include "../../include/mwb200.h"
+#include "mw_kernels.cuh"
+
+namespace mwb {
+
+uint64_t host_make_key(int depth, long long tx, long long ty, long long tz);
+void host_key_trans(uint64_t k, long long t[3]);
+
+static thread_local std::string g_err;
+
+void* dalloc(Ctx* ctx, size_t bytes) {
+    void* p = nullptr;
+    if (bytes == 0) bytes = 16;
+    MWB_CUDA(cudaMallocAsync(&p, bytes, ctx->stream));
+    return p;
+}
+void dfree(Ctx* ctx, void* p) {
+    if (p) cudaFreeAsync(p, ctx->stream);
+}
+
+// ---------------------------------------------------------------------------------------------
+// screening constants of the apply (same values as the CPU oracle)
+// ---------------------------------------------------------------------------------------------
+constexpr double kScreen = 0.1;  // skip a contribution below kScreen x the output split threshold
+inline double split_threshold(double prec, double ref, int depth) { return prec * ref * std::pow(2.0, -0.5 * depth); }
+
+// ---------------------------------------------------------------------------------------------
+// trees
+// ---------------------------------------------------------------------------------------------
+
+Tree::~Tree() {
+    if (!mra) return;
+    Ctx* c = mra->ctx;
+    cudaSetDevice(c->device);
+    dfree(c, key);
+    dfree(c, parent);
+    dfree(c, child0);
+    dfree(c, coef);
+    dfree(c, norm2);
+    dfree(c, wnorm2);
+    dfree(c, hkey);
+    dfree(c, hval);
+    cudaStreamSynchronize(c->stream);
+}
+
+static void tree_reserve(Tree& t, int need) {
+    Ctx* ctx = t.mra->ctx;
+    cudaStream_t s = ctx->stream;
+    if (need > t.cap) {
+        int ncap = std::max(need, std::max(64, t.cap * 2));
+        const size_t BS = t.mra->bsize();
+        auto grow = [&](auto*& p, size_t elem) {
+            using T = std::remove_reference_t<decltype(*p)>;
+            T* q = (T*)dalloc(ctx, elem * ncap);
+            if (p && t.n > 0) MWB_CUDA(cudaMemcpyAsync(q, p, elem * t.n, cudaMemcpyDeviceToDevice, s));
+            dfree(ctx, p);
+            p = q;
+        };
+        grow(t.key, sizeof(uint64_t));
+        grow(t.parent, sizeof(int));
+        grow(t.child0, sizeof(int));
+        grow(t.coef, sizeof(double) * BS);
+        grow(t.norm2, sizeof(double));
+        grow(t.wnorm2, sizeof(double));
+        t.cap = ncap;
+    }
+    // hash index at most half full
+    uint32_t hneed = 1024;
+    while (hneed < 2u * (uint32_t)std::max(need, 1)) hneed <<= 1;
+    if (hneed > t.hcap) {
+        dfree(ctx, t.hkey);
+        dfree(ctx, t.hval);
+        t.hcap = hneed;
+        t.hkey = (uint64_t*)dalloc(ctx, sizeof(uint64_t) * t.hcap);
+        t.hval = (int*)dalloc(ctx, sizeof(int) * t.hcap);
+        launch_hash_reset(t, s);
+        launch_hash_insert(t, 0, t.n, s);
+    }
+}
+
+// root boxes in Morton order
+static void tree_make_roots(Tree& t) {
+    const Mra& m = *t.mra;
+    std::vector<uint64_t> keys;
+    for (int z = 0; z < m.boxes[2]; ++z)
+        for (int y = 0; y < m.boxes[1]; ++y)
+            for (int x = 0; x < m.boxes[0]; ++x) keys.push_back(host_make_key(0, x, y, z));
+    std::sort(keys.begin(), keys.end());
+    t.n = 0;
+    t.level_begin.clear();
+    tree_reserve(t, (int)keys.size());
+    cudaStream_t s = m.ctx->stream;
+    launch_hash_reset(t, s);
+    const int n = (int)keys.size();
+    std::vector<int> par(n, -1);
+    MWB_CUDA(cudaMemcpyAsync(t.key, keys.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s));
+    MWB_CUDA(cudaMemcpyAsync(t.parent, par.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    MWB_CUDA(cudaMemcpyAsync(t.child0, par.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    MWB_CUDA(cudaMemsetAsync(t.norm2, 0, sizeof(double) * n, s));
+    MWB_CUDA(cudaMemsetAsync(t.wnorm2, 0, sizeof(double) * n, s));
+    MWB_CUDA(cudaStreamSynchronize(s));  // host vectors leave scope
+    t.n = n;
+    t.level_begin = {0, n};
+    launch_hash_insert(t, 0, n, s);
+}
+
+// split the nodes of the last level whose wavelet norm exceeds thr; returns the number of new nodes
+static int tree_refine_last_level(Tree& t, double thr) {
+    Ctx* ctx = t.mra->ctx;
+    cudaStream_t s = ctx->stream;
+    const int b = t.level_begin[t.levels() - 1], e = t.level_begin[t.levels()];
+    const int depth = t.levels() - 1;
+    int* d_list = (int*)dalloc(ctx, sizeof(int) * std::max(1, e - b));
+    int ns = launch_split(t, b, e, depth, thr, t.mra->depth_limit, d_list, s);
+    if (ns > 0) {
+        tree_reserve(t, t.n + 8 * ns);
+        launch_make_children(t, d_list, ns, s);
+        launch_hash_insert(t, t.n, t.n + 8 * ns, s);
+        t.n += 8 * ns;
+        t.level_begin.push_back(t.n);
+    }
+    dfree(ctx, d_list);
+    return 8 * ns;
+}
+
+static int* range_list(Ctx* ctx, int begin, int end) {
+    std::vector<int> v(end - begin);
+    std::iota(v.begin(), v.end(), begin);
+    int* d = (int*)dalloc(ctx, sizeof(int) * std::max<size_t>(1, v.size()));
+    MWB_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice, ctx->stream));
+    MWB_CUDA(cudaStreamSynchronize(ctx->stream));
+    return d;
+}
+
+// bottom-up: every internal node becomes the compression of its children's scaling parts
+static void tree_compress_bottom_up(Tree& t) {
+    Ctx* ctx = t.mra->ctx;
+    cudaStream_t s = ctx->stream;
+    for (int d = t.levels() - 2; d >= 0; --d) {
+        const int b = t.level_begin[d], e = t.level_begin[d + 1];
+        int* d_list = (int*)dalloc(ctx, sizeof(int) * (e - b));
+        int ni = launch_internal_list(t, b, e, d_list, s);
+        launch_transform_nodes(t, TM_COMPRESS, d_list, ni, nullptr, s);
+        dfree(ctx, d_list);
+    }
+}
+
+// top-down sum-up of an NS-form output: children's scaling parts += reconstruction of the parent
+static void tree_sumup_top_down(Tree& t) {
+    Ctx* ctx = t.mra->ctx;
+    cudaStream_t s = ctx->stream;
+    for (int d = 0; d + 1 < t.levels(); ++d) {
+        const int b = t.level_begin[d], e = t.level_begin[d + 1];
+        int* d_list = (int*)dalloc(ctx, sizeof(int) * (e - b));
+        int ni = launch_internal_list(t, b, e, d_list, s);
+        launch_transform_nodes(t, TM_SUMUP, d_list, ni, nullptr, s);
+        dfree(ctx, d_list);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// projection
+// ---------------------------------------------------------------------------------------------
+
+static void project(double prec, Tree& t, int type, int np, const double* params) {
+    Ctx* ctx = t.mra->ctx;
+    cudaStream_t s = ctx->stream;
+    if (np < 1) throw Error(MW_ERR_ARG, "empty parameter block");
+    const int nterm = (int)params[0];
+    const int per = (type == MW_FUNC_GAUSSIANS) ? 8 : (type == MW_FUNC_HYDROGEN_PRODUCTS ? 11 : -1);
+    if (per < 0) throw Error(MW_ERR_ARG, "unknown function type");
+    if (np < 1 + per * nterm) throw Error(MW_ERR_ARG, "parameter block too short");
+    double* d_p = (double*)dalloc(ctx, sizeof(double) * np);
+    MWB_CUDA(cudaMemcpyAsync(d_p, params, sizeof(double) * np, cudaMemcpyHostToDevice, s));
+    FuncDesc f{type, nterm, d_p};
+    tree_make_roots(t);
+    int b = 0, e = t.n;
+    while (e > b) {
+        int* d_list = range_list(ctx, b, e);
+        launch_transform_nodes(t, TM_PROJECT, d_list, e - b, &f, s);
+        dfree(ctx, d_list);
+        if (prec <= 0.0) break;
+        const double ref = std::sqrt(reduce_leaf_norm2(t, s));
+        const int added = tree_refine_last_level(t, split_threshold(prec, ref, t.levels() - 1));
+        if (added == 0) break;
+        b = e;
+        e = t.n;
+    }
+    tree_compress_bottom_up(t);
+    launch_node_norms(t, 0, t.n, s);
+    MWB_CUDA(cudaStreamSynchronize(s));
+    dfree(ctx, d_p);
+}
+
+// ---------------------------------------------------------------------------------------------
+// operators
+// ---------------------------------------------------------------------------------------------
+
+Op::~Op() {
+    if (!mra) return;
+    Ctx* c = mra->ctx;
+    cudaSetDevice(c->device);
+    for (auto& kv : depths) {
+        dfree(c, kv.second->d_mats);
+        dfree(c, kv.second->d_deltas);
+        dfree(c, kv.second->d_terms);
+    }
+    cudaStreamSynchronize(c->stream);
+}
+
+struct BandTmp {
+    bool active = false;
+    int L = -1;
+    std::vector<double> ns;  // l = -L..L
+    std::vector<double> t2, x2;
+};
+
+static std::vector<BandTmp> op_bands(Op& op, int depth) {
+    const Mra& m = *op.mra;
+    const int k = m.k, K2 = 2 * k, n = m.n0 + depth;
+    long extent = 0;
+    for (int d = 0; d < 3; ++d) extent = std::max<long>(extent, (long)m.boxes[d] << depth);
+    const double cut = depth == 0 ? 0.0 : 1e-6 * op.eps * op.B0 * std::pow(4.0, -depth);
+    std::vector<BandTmp> bs(op.terms.size());
+    for (size_t mi = 0; mi < op.terms.size(); ++mi) {
+        BandTmp& b = bs[mi];
+        std::vector<std::pair<long, std::vector<double>>> cache;
+        std::vector<std::vector<double>> mats;
+        std::vector<double> t2, x2;
+        auto compute = [&](long l) {
+            std::vector<double> NS(K2 * K2);
+            op.builder->ns(op.terms[mi].alpha, n, l, NS.data(), cache);
+            double tt = 0.0, xx = 0.0;
+            for (int a = 0; a < K2; ++a)
+                for (int c = 0; c < K2; ++c) {
+                    const double v = NS[a * K2 + c] * NS[a * K2 + c];
+                    if (a < k && c < k) tt += v; else xx += v;
+                }
+            mats.push_back(std::move(NS));
+            t2.push_back(tt);
+            x2.push_back(xx);
+        };
+        compute(0);
+        compute(1);
+        const double beta = op.terms[mi].beta;
+        double S2 = std::max(t2[0] + x2[0], t2[1] + x2[1]);
+        if (depth > 0) {
+            const double xmax = std::sqrt(std::max(x2[0], x2[1]));
+            if (beta * 10.0 * xmax * S2 < cut) continue;
+        }
+        long L = 1;
+        while (L + 1 < extent) {
+            const double last = std::sqrt(t2[L] + x2[L]);
+            if (depth > 0 && beta * last * S2 < cut) break;
+            if (depth == 0 && last <= 1e-300) break;
+            if (depth == 0 && last < 1e-17 * std::sqrt(S2)) break;
+            compute(L + 1);
+            S2 = std::max(S2, t2[L + 1] + x2[L + 1]);
+            ++L;
+        }
+        while (L > 0 && depth > 0 && beta * std::sqrt(t2[L] + x2[L]) * S2 < cut) --L;
+        if (L >= extent) L = extent - 1;
+        b.active = true;
+        b.L = (int)L;
+        b.ns.assign((size_t)(2 * L + 1) * K2 * K2, 0.0);
+        b.t2.assign(2 * L + 1, 0.0);
+        b.x2.assign(2 * L + 1, 0.0);
+        for (long l = -L; l <= L; ++l) {
+            const long al = l < 0 ? -l : l;
+            double* dst = &b.ns[(size_t)(l + L) * K2 * K2];
+            const std::vector<double>& src = mats[al];
+            for (int a = 0; a < K2; ++a)
+                for (int c = 0; c < K2; ++c) dst[a * K2 + c] = (l >= 0) ? src[a * K2 + c] : src[c * K2 + a];
+            b.t2[l + L] = t2[al];
+            b.x2[l + L] = x2[al];
+        }
+    }
+    return bs;
+}
+
+static double bound3(double beta, const double* t, const double* x, bool root) {
+    if (root) return beta * std::sqrt((t[0] + x[0]) * (t[1] + x[1]) * (t[2] + x[2]));
+    const double v = x[0] * (t[1] + x[1]) * (t[2] + x[2]) + t[0] * x[1] * (t[2] + x[2]) + t[0] * t[1] * x[2];
+    return beta * std::sqrt(v);
+}
+
+// build (once) and upload the tables of one depth
+static const OpDepth& op_depth(Op& op, int depth) {
+    std::lock_guard<std::mutex> g(op.mtx);
+    auto it = op.depths.find(depth);
+    if (it != op.depths.end()) return *it->second;
+    const Mra& m = *op.mra;
+    const int K2 = 2 * m.k;
+    std::vector<BandTmp> bs = op_bands(op, depth);
+    auto od = std::make_unique<OpDepth>();
+    std::vector<int> base(bs.size(), -1);
+    for (size_t mi = 0; mi < bs.size(); ++mi) {
+        if (!bs[mi].active) continue;
+        base[mi] = (int)(od->mats.size() / (K2 * K2));
+        od->mats.insert(od->mats.end(), bs[mi].ns.begin(), bs[mi].ns.end());
+    }
+    const bool root = depth == 0;
+    const double cut = root ? 0.0 : 1e-6 * op.eps * op.B0 * std::pow(4.0, -depth);
+    std::map<std::tuple<int, int, int>, std::vector<std::pair<double, int>>> acc;
+    for (size_t mi = 0; mi < bs.size(); ++mi) {
+        const BandTmp& b = bs[mi];
+        if (!b.active) continue;
+        const double beta = op.terms[mi].beta;
+        double S2 = 0.0;
+        for (int i = 0; i < 2 * b.L + 1; ++i) S2 = std::max(S2, b.t2[i] + b.x2[i]);
+        for (int dx = -b.L; dx <= b.L; ++dx) {
+            const double ax = b.t2[dx + b.L] + b.x2[dx + b.L];
+            if (!root && beta * std::sqrt(ax) * S2 < cut) continue;
+            for (int dy = -b.L; dy <= b.L; ++dy) {
+                const double ay = b.t2[dy + b.L] + b.x2[dy + b.L];
+                if (!root && beta * std::sqrt(ax * ay * S2) < cut) continue;
+                for (int dz = -b.L; dz <= b.L; ++dz) {
+                    const double t[3] = {b.t2[dx + b.L], b.t2[dy + b.L], b.t2[dz + b.L]};
+                    const double x[3] = {b.x2[dx + b.L], b.x2[dy + b.L], b.x2[dz + b.L]};
+                    const double bd = bound3(beta, t, x, root);
+                    if (bd <= 0.0 || bd < cut) continue;
+                    acc[std::make_tuple(dx, dy, dz)].push_back({bd, (int)mi});
+                }
+            }
+        }
+    }
+    std::vector<std::pair<DeltaRec, std::vector<TermRec>>> rows;
+    rows.reserve(acc.size());
+    for (auto& kv : acc) {
+        auto& v = kv.second;
+        std::stable_sort(v.begin(), v.end(), [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
+            return a.first > b.first || (a.first == b.first && a.second < b.second);
+        });
+        DeltaRec dr{};
+        dr.d[0] = std::get<0>(kv.first);
+        dr.d[1] = std::get<1>(kv.first);
+        dr.d[2] = std::get<2>(kv.first);
+        dr.maxb = v.front().first;
+        std::vector<TermRec> trs;
+        for (auto& pr : v) {
+            const int mi = pr.second;
+            const BandTmp& b = bs[mi];
+            TermRec tr{};
+            tr.m = mi;
+            tr.mx = base[mi] + dr.d[0] + b.L;
+            tr.my = base[mi] + dr.d[1] + b.L;
+            tr.mz = base[mi] + dr.d[2] + b.L;
+            tr.beta = op.terms[mi].beta;
+            tr.bound = pr.first;
+            trs.push_back(tr);
+        }
+        rows.emplace_back(dr, std::move(trs));
+    }
+    std::stable_sort(rows.begin(), rows.end(),
+                     [](const auto& a, const auto& b) { return a.first.maxb > b.first.maxb; });
+    for (auto& r : rows) {
+        r.first.t0 = (int)od->terms.size();
+        od->terms.insert(od->terms.end(), r.second.begin(), r.second.end());
+        r.first.t1 = (int)od->terms.size();
+        od->deltas.push_back(r.first);
+    }
+    Ctx* ctx = m.ctx;
+    cudaStream_t s = ctx->stream;
+    od->d_mats = (double*)dalloc(ctx, sizeof(double) * std::max<size_t>(1, od->mats.size()));
+    od->d_deltas = (DeltaRec*)dalloc(ctx, sizeof(DeltaRec) * std::max<size_t>(1, od->deltas.size()));
+    od->d_terms = (TermRec*)dalloc(ctx, sizeof(TermRec) * std::max<size_t>(1, od->terms.size()));
+    if (!od->mats.empty())
+        MWB_CUDA(cudaMemcpyAsync(od->d_mats, od->mats.data(), sizeof(double) * od->mats.size(), cudaMemcpyHostToDevice, s));
+    if (!od->deltas.empty())
+        MWB_CUDA(cudaMemcpyAsync(od->d_deltas, od->deltas.data(), sizeof(DeltaRec) * od->deltas.size(), cudaMemcpyHostToDevice, s));
+    if (!od->terms.empty())
+        MWB_CUDA(cudaMemcpyAsync(od->d_terms, od->terms.data(), sizeof(TermRec) * od->terms.size(), cudaMemcpyHostToDevice, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
+    return *op.depths.emplace(depth, std::move(od)).first->second;
+}
+
+static void op_init(Op& op, Mra* m, double mu, double prec) {
+    if (!(prec > 0.0)) throw Error(MW_ERR_ARG, "operator precision must be positive");
+    if (mu < 0.0) throw Error(MW_ERR_ARG, "mu must be non-negative");
+    op.mra = m;
+    op.mu = mu;
+    op.prec = prec;
+    op.eps = 0.1 * prec;
+    const double root_edge = std::ldexp(1.0, -m->n0);
+    double r_max = 0.0;
+    for (int d = 0; d < 3; ++d) r_max += std::pow(m->boxes[d] * root_edge, 2);
+    r_max = std::sqrt(r_max);
+    const double r_min = 0.01 * std::ldexp(root_edge, -m->max_depth);
+    op.terms = kernel_expansion(mu, op.eps, r_min, r_max);
+    op.builder = std::make_unique<GaussianOperatorBuilder>(m->basis, m->F);
+    // operator scale from the root-depth bands
+    std::vector<BandTmp> b0 = op_bands(op, 0);
+    op.B0 = 0.0;
+    for (size_t mi = 0; mi < op.terms.size(); ++mi) {
+        if (!b0[mi].active) continue;
+        const int L = b0[mi].L;
+        op.B0 = std::max(op.B0, op.terms[mi].beta * std::pow(b0[mi].t2[L] + b0[mi].x2[L], 1.5));
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// apply
+// ---------------------------------------------------------------------------------------------
+
+static void apply(double prec, Tree& out, Op& op, Tree& inp) {
+    if (out.mra != inp.mra || op.mra != inp.mra) throw Error(MW_ERR_ARG, "trees and operator must share the world");
+    if (&out == &inp) throw Error(MW_ERR_ARG, "in-place apply is not supported");
+    if (inp.n == 0) throw Error(MW_ERR_STATE, "input tree is empty");
+    const Mra& m = *inp.mra;
+    Ctx* ctx = m.ctx;
+    cudaStream_t s = ctx->stream;
+    tree_make_roots(out);
+    const double fnorm = std::sqrt(reduce_leaf_norm2(inp, s));
+    const double nu_max = std::sqrt(reduce_max_norm2(inp, s));
+    double g0 = 0.0;
+    long long trip = 0;
+    int passes = 0;
+    for (int depth = 0;; ++depth) {
+        const int b = out.level_begin[depth], e = out.level_begin[depth + 1];
+        if (e <= b) break;
+        ++passes;
+        const OpDepth& tab = op_depth(op, depth);
+        ApplyPass ps;
+        ps.depth = depth;
+        ps.root = depth == 0;
+        ps.tab = &tab;
+        if (ps.root) {
+            const double nu0 = tab.deltas.empty() ? 0.0 : tab.deltas.front().maxb;
+            ps.theta = kScreen * prec * fnorm * nu0;
+        } else {
+            ps.theta = kScreen * split_threshold(prec, g0, depth);
+        }
+        int np = 0;
+        while (np < (int)tab.deltas.size() && !(tab.deltas[np].maxb * nu_max < ps.theta)) ++np;
+        ps.nprefix = np;
+        for (int d = 0; d < 3; ++d) ps.ext[d] = (long long)m.boxes[d] << depth;
+        run_apply_pass(out, b, e, inp, ps, s);
+        trip += ps.triples;
+        if (ps.root) g0 = std::sqrt(reduce_range_norm2(out, b, e, s));
+        if (!(prec > 0.0) || !(g0 > 0.0)) break;
+        if (tree_refine_last_level(out, split_threshold(prec, g0, depth)) == 0) break;
+    }
+    tree_sumup_top_down(out);
+    tree_compress_bottom_up(out);
+    launch_node_norms(out, 0, out.n, s);
+    MWB_CUDA(cudaStreamSynchronize(s));
+    out.stats[0] = trip;
+    out.stats[1] = 0;
+    out.stats[2] = passes;
+    out.stats[3] = out.n;
+}
+
+}  // namespace mwb
+
+// =============================================================================================
+// C-ABI
+// =============================================================================================
+using namespace mwb;
+
+struct mw_ctx_s : Ctx {};
+struct mw_mra_s : Mra {};
+struct mw_tree_s : Tree {};
+struct mw_op_s : Op {};
+
+#define MW_TRY(...)                                        \
+    try {                                                  \
+        __VA_ARGS__;                                       \
+        return MW_OK;                                      \
+    } catch (const mwb::Error& e) {                        \
+        g_err = e.what();                                  \
+        return e.code;                                     \
+    } catch (const std::exception& e) {                    \
+        g_err = e.what();                                  \
+        return MW_ERR_STATE;                               \
+    }
+
+#define MW_ARG(cond, msg) \
+    if (!(cond)) throw mwb::Error(MW_ERR_ARG, msg)
+
+extern "C" {
+
+const char* mw_last_error(void) { return g_err.c_str(); }
+
+int mw_version(int* major, int* minor) {
+    MW_TRY({
+        MW_ARG(major && minor, "null pointer");
+        *major = 0;
+        *minor = 1;
+    })
+}
+
+int mw_ctx_create(int device, void* stream, mw_ctx* out) {
+    MW_TRY({
+        MW_ARG(out, "null pointer");
+        int ndev = 0;
+        MWB_CUDA(cudaGetDeviceCount(&ndev));
+        MW_ARG(device >= 0 && device < ndev, "invalid CUDA device");
+        MWB_CUDA(cudaSetDevice(device));
+        auto* c = new mw_ctx_s();
+        c->device = device;
+        if (stream) {
+            c->stream = (cudaStream_t)stream;
+        } else {
+            MWB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+            c->own_stream = true;
+        }
+        MWB_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+        cudaMemPool_t pool;
+        MWB_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t thr = ~0ull;
+        MWB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+        *out = c;
+    })
+}
+
+int mw_ctx_destroy(mw_ctx ctx) {
+    MW_TRY({
+        if (!ctx) return MW_OK;
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+        if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+        delete ctx;
+    })
+}
+
+int mw_ctx_synchronize(mw_ctx ctx) {
+    MW_TRY({
+        MW_ARG(ctx, "null context");
+        MWB_CUDA(cudaSetDevice(ctx->device));
+        MWB_CUDA(cudaStreamSynchronize(ctx->stream));
+    })
+}
+
+int mw_mra_create(mw_ctx ctx, int min_scale, const int* corner, const int* boxes, int basis_type, int order,
+                  int max_depth, mw_mra* out) {
+    MW_TRY({
+        MW_ARG(ctx && corner && boxes && out, "null pointer");
+        MW_ARG(basis_type == MW_BASIS_INTERPOLATING || basis_type == MW_BASIS_LEGENDRE, "invalid basis type");
+        MW_ARG(order >= 3 && order <= 11, "order must be in [3, 11]");
+        MW_ARG(max_depth >= 0 && max_depth <= 30, "max_depth must be in [0, 30]");
+        int maxb = 1;
+        for (int d = 0; d < 3; ++d) {
+            MW_ARG(boxes[d] >= 1 && boxes[d] <= 4096, "boxes must be in [1, 4096]");
+            maxb = std::max(maxb, boxes[d]);
+        }
+        MWB_CUDA(cudaSetDevice(ctx->device));
+        auto* m = new mw_mra_s();
+        m->ctx = ctx;
+        m->n0 = min_scale;
+        for (int d = 0; d < 3; ++d) {
+            m->corner[d] = corner[d];
+            m->boxes[d] = boxes[d];
+        }
+        m->max_depth = max_depth;
+        int lb = 0;
+        while ((1 << lb) < maxb) ++lb;
+        m->depth_limit = std::min(max_depth, kKeyBits - lb);
+        m->basis.init(basis_type, order);
+        m->k = m->basis.k;
+        m->F = two_scale_filter(m->basis);
+        m->W = quadrature_matrix(m->basis);
+        const int k = m->k, K2 = 2 * k;
+        std::vector<double> FT(K2 * K2), PF(K2 * K2, 0.0);
+        for (int a = 0; a < K2; ++a)
+            for (int b = 0; b < K2; ++b) FT[a * K2 + b] = m->F[b * K2 + a];
+        for (int a = 0; a < K2; ++a)
+            for (int c = 0; c < 2; ++c)
+                for (int q = 0; q < k; ++q) {
+                    double s = 0.0;
+                    for (int j = 0; j < k; ++j) s += m->F[a * K2 + c * k + j] * m->W[j * k + q];
+                    PF[a * K2 + c * k + q] = s;
+                }
+        cudaStream_t s = ctx->stream;
+        m->d_F = (double*)dalloc(ctx, sizeof(double) * K2 * K2);
+        m->d_FT = (double*)dalloc(ctx, sizeof(double) * K2 * K2);
+        m->d_PF = (double*)dalloc(ctx, sizeof(double) * K2 * K2);
+        MWB_CUDA(cudaMemcpyAsync(m->d_F, m->F.data(), sizeof(double) * K2 * K2, cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(m->d_FT, FT.data(), sizeof(double) * K2 * K2, cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(m->d_PF, PF.data(), sizeof(double) * K2 * K2, cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaStreamSynchronize(s));
+        *out = m;
+    })
+}
+
+int mw_mra_destroy(mw_mra m) {
+    MW_TRY({
+        if (!m) return MW_OK;
+        cudaSetDevice(m->ctx->device);
+        dfree(m->ctx, m->d_F);
+        dfree(m->ctx, m->d_FT);
+        dfree(m->ctx, m->d_PF);
+        cudaStreamSynchronize(m->ctx->stream);
+        delete m;
+    })
+}
+
+int mw_mra_filter(mw_mra m, double* F) {
+    MW_TRY({
+        MW_ARG(m && F, "null pointer");
+        std::memcpy(F, m->F.data(), sizeof(double) * m->F.size());
+    })
+}
+
+int mw_mra_max_depth(mw_mra m, int* depth) {
+    MW_TRY({
+        MW_ARG(m && depth, "null pointer");
+        *depth = m->depth_limit;
+    })
+}
+
+int mw_tree_create(mw_mra m, mw_tree* out) {
+    MW_TRY({
+        MW_ARG(m && out, "null pointer");
+        MWB_CUDA(cudaSetDevice(m->ctx->device));
+        auto* t = new mw_tree_s();
+        t->mra = m;
+        *out = t;
+    })
+}
+
+int mw_tree_destroy(mw_tree t) {
+    MW_TRY({
+        if (t) delete t;
+    })
+}
+
+int mw_tree_nnodes(mw_tree t, int* n) {
+    MW_TRY({
+        MW_ARG(t && n, "null pointer");
+        *n = t->n;
+    })
+}
+
+int mw_tree_square_norm(mw_tree t, double* out) {
+    MW_TRY({
+        MW_ARG(t && out, "null pointer");
+        MWB_CUDA(cudaSetDevice(t->mra->ctx->device));
+        *out = t->n ? reduce_leaf_norm2(*t, t->mra->ctx->stream) : 0.0;
+    })
+}
+
+int mw_tree_upload(mw_tree t, int n, const int* depth, const long long* trans, const int* parent, const int* child0,
+                   const double* coef) {
+    MW_TRY({
+        MW_ARG(t && depth && trans && parent && child0 && coef, "null pointer");
+        MW_ARG(n > 0, "empty tree");
+        const Mra& m = *t->mra;
+        MWB_CUDA(cudaSetDevice(m.ctx->device));
+        cudaStream_t s = m.ctx->stream;
+        // validate and order by (depth, Morton): parents before children, siblings in child order
+        std::vector<uint64_t> key(n);
+        int maxd = 0;
+        for (int i = 0; i < n; ++i) {
+            MW_ARG(depth[i] >= 0 && depth[i] <= m.depth_limit, "node depth out of range");
+            for (int d = 0; d < 3; ++d)
+                MW_ARG(trans[3 * i + d] >= 0 && trans[3 * i + d] < ((long long)m.boxes[d] << depth[i]),
+                       "node translation outside the world");
+            key[i] = host_make_key(depth[i], trans[3 * i], trans[3 * i + 1], trans[3 * i + 2]);
+            maxd = std::max(maxd, depth[i]);
+        }
+        std::vector<int> ord(n);
+        std::iota(ord.begin(), ord.end(), 0);
+        std::sort(ord.begin(), ord.end(), [&](int a, int b) { return key[a] < key[b]; });
+        std::vector<int> pos(n);
+        for (int i = 0; i < n; ++i) pos[ord[i]] = i;
+        int nroot = (int)((long long)m.boxes[0] * m.boxes[1] * m.boxes[2]);
+        std::vector<uint64_t> k2(n);
+        std::vector<int> p2(n), c2(n);
+        std::vector<double> coef2((size_t)n * m.bsize());
+        std::vector<int> lb(maxd + 2, 0);
+        int roots = 0;
+        for (int i = 0; i < n; ++i) {
+            const int o = ord[i];
+            k2[i] = key[o];
+            p2[i] = parent[o] < 0 ? -1 : pos[parent[o]];
+            c2[i] = child0[o] < 0 ? -1 : pos[child0[o]];
+            if (depth[o] == 0) ++roots;
+            MW_ARG(parent[o] < n && child0[o] < n, "bad parent/child index");
+            std::memcpy(&coef2[(size_t)i * m.bsize()], coef + (size_t)o * m.bsize(), sizeof(double) * m.bsize());
+            lb[depth[o] + 1]++;
+        }
+        MW_ARG(roots == nroot, "tree must contain every root box");
+        for (int i = 0; i < n; ++i) {
+            if (c2[i] < 0) continue;
+            const int o = ord[i];
+            for (int c = 0; c < 8; ++c) {
+                const int ch = child0[o] + c;
+                MW_ARG(ch < n && pos[ch] == c2[i] + c && parent[ch] == o, "children must be 8 consecutive nodes");
+            }
+        }
+        for (int d = 1; d < (int)lb.size(); ++d) lb[d] += lb[d - 1];
+        t->n = 0;
+        tree_reserve(*t, n);
+        MWB_CUDA(cudaMemcpyAsync(t->key, k2.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(t->parent, p2.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(t->child0, c2.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(t->coef, coef2.data(), sizeof(double) * coef2.size(), cudaMemcpyHostToDevice, s));
+        t->n = n;
+        t->level_begin = lb;
+        launch_hash_reset(*t, s);
+        launch_hash_insert(*t, 0, n, s);
+        launch_node_norms(*t, 0, n, s);
+        MWB_CUDA(cudaStreamSynchronize(s));
+    })
+}
+
+int mw_tree_download(mw_tree t, int* depth, long long* trans, int* parent, int* child0, double* coef) {
+    MW_TRY({
+        MW_ARG(t, "null tree");
+        const int n = t->n;
+        if (n == 0) return MW_OK;
+        MWB_CUDA(cudaSetDevice(t->mra->ctx->device));
+        cudaStream_t s = t->mra->ctx->stream;
+        std::vector<uint64_t> key(n);
+        MWB_CUDA(cudaMemcpyAsync(key.data(), t->key, sizeof(uint64_t) * n, cudaMemcpyDeviceToHost, s));
+        if (parent) MWB_CUDA(cudaMemcpyAsync(parent, t->parent, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+        if (child0) MWB_CUDA(cudaMemcpyAsync(child0, t->child0, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+        if (coef)
+            MWB_CUDA(cudaMemcpyAsync(coef, t->coef, sizeof(double) * n * t->mra->bsize(), cudaMemcpyDeviceToHost, s));
+        MWB_CUDA(cudaStreamSynchronize(s));
+        for (int i = 0; i < n; ++i) {
+            long long tr[3];
+            host_key_trans(key[i], tr);
+            if (depth) depth[i] = (int)(key[i] >> 59);
+            if (trans)
+                for (int d = 0; d < 3; ++d) trans[3 * i + d] = tr[d];
+        }
+    })
+}
+
+int mw_tree_device_arrays(mw_tree t, void** coef, void** key, void** norm2) {
+    MW_TRY({
+        MW_ARG(t, "null tree");
+        if (coef) *coef = t->coef;
+        if (key) *key = t->key;
+        if (norm2) *norm2 = t->norm2;
+    })
+}
+
+int mw_tree_rescale(mw_tree t, double c) {
+    MW_TRY({
+        MW_ARG(t, "null tree");
+        MWB_CUDA(cudaSetDevice(t->mra->ctx->device));
+        launch_rescale(*t, c, t->mra->ctx->stream);
+        MWB_CUDA(cudaStreamSynchronize(t->mra->ctx->stream));
+    })
+}
+
+int mw_project(double prec, mw_tree t, int func_type, int nparams, const double* params) {
+    MW_TRY({
+        MW_ARG(t && params, "null pointer");
+        MWB_CUDA(cudaSetDevice(t->mra->ctx->device));
+        project(prec, *t, func_type, nparams, params);
+    })
+}
+
+int mw_dot(mw_tree a, mw_tree b, double* out) {
+    MW_TRY({
+        MW_ARG(a && b && out, "null pointer");
+        MW_ARG(a->mra == b->mra, "trees must share the world");
+        MWB_CUDA(cudaSetDevice(a->mra->ctx->device));
+        *out = launch_dot(*a, *b, a->mra->ctx->stream);
+    })
+}
+
+int mw_op_create_poisson(mw_mra m, double prec, mw_op* out) {
+    MW_TRY({
+        MW_ARG(m && out, "null pointer");
+        MWB_CUDA(cudaSetDevice(m->ctx->device));
+        auto* op = new mw_op_s();
+        try {
+            op_init(*op, m, 0.0, prec);
+        } catch (...) {
+            delete op;
+            throw;
+        }
+        *out = op;
+    })
+}
+
+int mw_op_create_helmholtz(mw_mra m, double mu, double prec, mw_op* out) {
+    MW_TRY({
+        MW_ARG(m && out, "null pointer");
+        MW_ARG(mu > 0.0, "mu must be positive");
+        MWB_CUDA(cudaSetDevice(m->ctx->device));
+        auto* op = new mw_op_s();
+        try {
+            op_init(*op, m, mu, prec);
+        } catch (...) {
+            delete op;
+            throw;
+        }
+        *out = op;
+    })
+}
+
+int mw_op_destroy(mw_op op) {
+    MW_TRY({
+        if (op) delete op;
+    })
+}
+
+int mw_op_nterms(mw_op op, int* n) {
+    MW_TRY({
+        MW_ARG(op && n, "null pointer");
+        *n = (int)op->terms.size();
+    })
+}
+
+int mw_op_terms(mw_op op, double* alpha, double* beta) {
+    MW_TRY({
+        MW_ARG(op && alpha && beta, "null pointer");
+        for (size_t i = 0; i < op->terms.size(); ++i) {
+            alpha[i] = op->terms[i].alpha;
+            beta[i] = op->terms[i].beta;
+        }
+    })
+}
+
+int mw_apply(double prec, mw_tree out, mw_op op, mw_tree inp, int flags) {
+    MW_TRY({
+        MW_ARG(out && op && inp, "null pointer");
+        MW_ARG(flags == MW_APPLY_FP64, "unknown apply flags");
+        MWB_CUDA(cudaSetDevice(inp->mra->ctx->device));
+        apply(prec, *out, *op, *inp);
+    })
+}
+
+int mw_apply_stats(mw_tree out, long long* stats) {
+    MW_TRY({
+        MW_ARG(out && stats, "null pointer");
+        for (int i = 0; i < 4; ++i) stats[i] = out->stats[i];
+    })
+}
+
+}  // extern "C"

@@ -1,0 +1,113 @@
+// mw_internal.hpp -- host-side objects behind the C-ABI handles (include/mwb200.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "mw_math.hpp"
+
+namespace mwb {
+
+// error carried to the C-ABI boundary (converted to a status code + mw_last_error text)
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define MWB_CUDA(call)                                                                           \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            throw ::mwb::Error(-2, std::string(#call) + ": " + cudaGetErrorString(e_) + " (" +    \
+                                       __FILE__ + ":" + std::to_string(__LINE__) + ")");          \
+    } while (0)
+
+constexpr int kKeyBits = 19;          // translation bits per dimension in a node key
+constexpr uint64_t kEmptyKey = ~0ull; // empty hash slot
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int num_sms = 0;
+};
+
+struct Mra {
+    Ctx* ctx = nullptr;
+    int n0 = 0;
+    int corner[3] = {0, 0, 0};
+    int boxes[3] = {1, 1, 1};
+    int max_depth = 0;      // as requested (sets the operators' r_min)
+    int depth_limit = 0;    // max_depth clamped to the key capacity
+    int k = 0;
+    ScalingBasis basis;
+    std::vector<double> F;  // (2k)^2 two-scale filter
+    std::vector<double> W;  // k x k projection quadrature matrix
+    double* d_F = nullptr;   // F
+    double* d_FT = nullptr;  // F^T
+    double* d_PF = nullptr;  // projection matrix F * blkdiag(W, W)
+    size_t bsize() const { return (size_t)8 * k * k * k; }
+};
+
+// Per-depth operator tables (device layout documented in mw_kernels.cuh)
+struct DeltaRec {
+    int d[3];
+    int t0, t1;
+    int pad;
+    double maxb;
+};
+struct TermRec {
+    int mx, my, mz, m;
+    double beta;
+    double bound;
+};
+
+struct OpDepth {
+    std::vector<double> mats;          // NS matrices, (2k)^2 each
+    std::vector<DeltaRec> deltas;      // sorted by maxb, descending
+    std::vector<TermRec> terms;
+    double* d_mats = nullptr;
+    DeltaRec* d_deltas = nullptr;
+    TermRec* d_terms = nullptr;
+};
+
+struct Op {
+    Mra* mra = nullptr;
+    double mu = 0.0, prec = 0.0, eps = 0.0;
+    std::vector<GaussTerm> terms;
+    std::unique_ptr<GaussianOperatorBuilder> builder;
+    double B0 = 0.0;
+    std::map<int, std::unique_ptr<OpDepth>> depths;
+    std::mutex mtx;
+    ~Op();
+};
+
+struct Tree {
+    Mra* mra = nullptr;
+    int n = 0, cap = 0;
+    uint64_t* key = nullptr;
+    int* parent = nullptr;
+    int* child0 = nullptr;
+    double* coef = nullptr;
+    double* norm2 = nullptr;   // squared norm of the whole block
+    double* wnorm2 = nullptr;  // squared norm of the wavelet part
+    uint64_t* hkey = nullptr;
+    int* hval = nullptr;
+    uint32_t hcap = 0;
+    std::vector<int> level_begin;  // level d = [level_begin[d], level_begin[d+1])
+    long long stats[4] = {0, 0, 0, 0};
+    ~Tree();
+    int levels() const { return (int)level_begin.size() - 1; }
+};
+
+// device memory from the stream-ordered pool
+void* dalloc(Ctx* ctx, size_t bytes);
+void dfree(Ctx* ctx, void* p);
+
+}  // namespace mwb

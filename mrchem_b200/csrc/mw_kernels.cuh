@@ -1,0 +1,64 @@
+// mw_kernels.cuh -- launchers of the sm_100a kernels (mw_kernels.cu), called by the host driver.
+#pragma once
+#include <cstdint>
+
+#include "mw_internal.hpp"
+
+namespace mwb {
+
+// analytic function for projection (device copy of the parameter block)
+struct FuncDesc {
+    int type;
+    int nterm;
+    const double* p;
+};
+
+// Transform modes of launch_transform_nodes
+enum TransformMode {
+    TM_PROJECT = 0,   // quadrature block of f at the node -> compressed block
+    TM_COMPRESS = 1,  // children's scaling parts -> compressed block of the parent
+    TM_SUMUP = 2,     // reconstruct parent block, add the child parts into the children's scaling parts
+};
+
+// Per-apply view of the input tree for the candidate and contraction kernels
+struct InView {
+    const uint64_t* hkey;
+    const int* hval;
+    uint32_t hcap;
+    const double* coef;
+    const double* norm2;
+};
+
+void launch_transform_nodes(Tree& t, int mode, const int* d_nodes, int nnodes, const FuncDesc* f,
+                            cudaStream_t s);
+void launch_node_norms(Tree& t, int begin, int end, cudaStream_t s);
+void launch_hash_reset(Tree& t, cudaStream_t s);
+void launch_hash_insert(Tree& t, int begin, int end, cudaStream_t s);
+// flags[i - begin] = sqrt(wnorm2[i]) > thr(depth) for i in [begin, end); returns number of splits
+// and writes the split list (tree indices) to d_list
+int launch_split(Tree& t, int begin, int end, int depth, double thr, int depth_limit, int* d_list,
+                 cudaStream_t s);
+// append 8 children for each node in d_list (n_split entries)
+void launch_make_children(Tree& t, const int* d_list, int nsplit, cudaStream_t s);
+// internal node list of [begin, end) (returns count)
+int launch_internal_list(Tree& t, int begin, int end, int* d_list, cudaStream_t s);
+// deterministic reductions: sum of norm2 over leaves (or over [begin,end) when all=true), max norm2
+double reduce_leaf_norm2(Tree& t, cudaStream_t s);
+double reduce_range_norm2(Tree& t, int begin, int end, cudaStream_t s);
+double reduce_max_norm2(Tree& t, cudaStream_t s);
+void launch_rescale(Tree& t, double c, cudaStream_t s);
+double launch_dot(Tree& a, Tree& b, cudaStream_t s);
+
+// apply pass over output level [obegin, oend) at `depth`
+struct ApplyPass {
+    int depth;
+    bool root;
+    double theta;
+    int nprefix;  // number of leading offset entries considered
+    const OpDepth* tab;
+    long long ext[3];
+    long long triples = 0, triples_gen = 0;
+};
+void run_apply_pass(Tree& out, int obegin, int oend, Tree& inp, ApplyPass& pass, cudaStream_t s);
+
+}  // namespace mwb

@@ -1,0 +1,298 @@
+"""Python mirror of the MRCPP operator-apply interface, bound to the C-ABI library ``libmwb200.so``.
+
+Names and argument meaning follow the objects the reference calls on this path:
+
+* ``MultiResolutionAnalysis(min_scale, corner, boxes, order, max_depth, basis)`` --
+  ``BoundingBox<3>`` + ``InterpolatingBasis``/``LegendreBasis`` + ``MultiResolutionAnalysis<3>``
+  (reference ``src/mrenv.cpp:52,64-72``);
+* ``FunctionTree(mra)`` -- ``FunctionTree<3>`` (``src/qmfunctions/QMFunction.cpp:68-77``);
+* ``PoissonOperator(mra, prec)`` / ``HelmholtzOperator(mra, mu, prec)``
+  (``src/SCFDriver.cpp:279``, ``src/scf_solver/HelmholtzVector.cpp:171``);
+* ``apply(prec, out, op, inp)`` (``src/scf_solver/HelmholtzVector.cpp:176``,
+  ``src/qmoperators/two_electron/CoulombPotential.cpp:85``);
+* ``project(prec, tree, f)`` and ``dot(a, b)``.
+
+Every call runs on the GPU through the C-ABI; there is no CPU path.  A non-zero status from the
+library raises :class:`MWError` (the reference aborts through ``MSG_FATAL`` instead).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmwb200.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_lp = ctypes.POINTER(ctypes.c_longlong)
+_vp = ctypes.c_void_p
+_vpp = ctypes.POINTER(ctypes.c_void_p)
+
+BASIS_INTERPOLATING = 0
+BASIS_LEGENDRE = 1
+FUNC_GAUSSIANS = 1
+FUNC_HYDROGEN_PRODUCTS = 2
+APPLY_FP64 = 0
+
+# every symbol include/mwb200.h declares: (name, restype, argtypes)
+SYMBOLS = [
+    ("mw_last_error", ctypes.c_char_p, []),
+    ("mw_version", ctypes.c_int, [_ip, _ip]),
+    ("mw_ctx_create", ctypes.c_int, [ctypes.c_int, _vp, _vpp]),
+    ("mw_ctx_destroy", ctypes.c_int, [_vp]),
+    ("mw_ctx_synchronize", ctypes.c_int, [_vp]),
+    ("mw_mra_create", ctypes.c_int, [_vp, ctypes.c_int, _ip, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vpp]),
+    ("mw_mra_destroy", ctypes.c_int, [_vp]),
+    ("mw_mra_filter", ctypes.c_int, [_vp, _dp]),
+    ("mw_mra_max_depth", ctypes.c_int, [_vp, _ip]),
+    ("mw_tree_create", ctypes.c_int, [_vp, _vpp]),
+    ("mw_tree_destroy", ctypes.c_int, [_vp]),
+    ("mw_tree_nnodes", ctypes.c_int, [_vp, _ip]),
+    ("mw_tree_square_norm", ctypes.c_int, [_vp, _dp]),
+    ("mw_tree_upload", ctypes.c_int, [_vp, ctypes.c_int, _ip, _lp, _ip, _ip, _dp]),
+    ("mw_tree_download", ctypes.c_int, [_vp, _ip, _lp, _ip, _ip, _dp]),
+    ("mw_tree_device_arrays", ctypes.c_int, [_vp, _vpp, _vpp, _vpp]),
+    ("mw_tree_rescale", ctypes.c_int, [_vp, ctypes.c_double]),
+    ("mw_project", ctypes.c_int, [ctypes.c_double, _vp, ctypes.c_int, ctypes.c_int, _dp]),
+    ("mw_dot", ctypes.c_int, [_vp, _vp, _dp]),
+    ("mw_op_create_poisson", ctypes.c_int, [_vp, ctypes.c_double, _vpp]),
+    ("mw_op_create_helmholtz", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _vpp]),
+    ("mw_op_destroy", ctypes.c_int, [_vp]),
+    ("mw_op_nterms", ctypes.c_int, [_vp, _ip]),
+    ("mw_op_terms", ctypes.c_int, [_vp, _dp, _dp]),
+    ("mw_apply", ctypes.c_int, [ctypes.c_double, _vp, _vp, _vp, ctypes.c_int]),
+    ("mw_apply_stats", ctypes.c_int, [_vp, _lp]),
+]
+
+_lib = None
+
+
+class MWError(RuntimeError):
+    """Error status returned by the C-ABI."""
+
+
+def load_library(path: str = LIB_PATH):
+    """Load ``libmwb200.so`` and bind every declared symbol; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"libmwb200.so not built ({path}); run __graft_entry__.build()")
+    L = ctypes.CDLL(path)
+    for name, res, args in SYMBOLS:
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(status):
+    if status != 0:
+        msg = _lib.mw_last_error().decode(errors="replace")
+        raise MWError(f"mwb200 error {status}: {msg}")
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+class Context:
+    """CUDA device + stream + memory pool of the library."""
+
+    _default = None
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        L = load_library()
+        h = ctypes.c_void_p()
+        _check(L.mw_ctx_create(int(device), stream, ctypes.byref(h)))
+        self._h = h
+        self.device = device
+
+    @classmethod
+    def default(cls):
+        if cls._default is None:
+            cls._default = Context(0)
+        return cls._default
+
+    def synchronize(self):
+        _check(_lib.mw_ctx_synchronize(self._h))
+
+
+class MultiResolutionAnalysis:
+    INTERPOLATING = BASIS_INTERPOLATING
+    LEGENDRE = BASIS_LEGENDRE
+
+    def __init__(self, min_scale, corner, boxes, order, max_depth, basis=BASIS_INTERPOLATING, ctx=None):
+        L = load_library()
+        self.ctx = ctx or Context.default()
+        self.min_scale = int(min_scale)
+        self.corner = tuple(int(c) for c in corner)
+        self.boxes = tuple(int(b) for b in boxes)
+        self.order = int(order)
+        self.k = self.order + 1
+        self.max_depth = int(max_depth)
+        self.basis = int(basis)
+        h = ctypes.c_void_p()
+        _check(L.mw_mra_create(self.ctx._h, self.min_scale, (ctypes.c_int * 3)(*self.corner),
+                               (ctypes.c_int * 3)(*self.boxes), self.basis, self.order, self.max_depth,
+                               ctypes.byref(h)))
+        self._h = h
+
+    def filter(self):
+        F = np.zeros((2 * self.k, 2 * self.k))
+        _check(_lib.mw_mra_filter(self._h, _d(F)))
+        return F
+
+    def depth_limit(self):
+        d = ctypes.c_int()
+        _check(_lib.mw_mra_max_depth(self._h, ctypes.byref(d)))
+        return d.value
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.mw_mra_destroy(self._h)
+            self._h = None
+
+
+class FunctionTree:
+    def __init__(self, mra: MultiResolutionAnalysis):
+        self.mra = mra
+        h = ctypes.c_void_p()
+        _check(load_library().mw_tree_create(mra._h, ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.mw_tree_destroy(self._h)
+            self._h = None
+
+    def nnodes(self):
+        n = ctypes.c_int()
+        _check(_lib.mw_tree_nnodes(self._h, ctypes.byref(n)))
+        return n.value
+
+    getNNodes = nnodes
+
+    def square_norm(self):
+        v = ctypes.c_double()
+        _check(_lib.mw_tree_square_norm(self._h, ctypes.byref(v)))
+        return v.value
+
+    getSquareNorm = square_norm
+
+    def rescale(self, c):
+        _check(_lib.mw_tree_rescale(self._h, float(c)))
+
+    def export(self, with_coefs=True):
+        n = self.nnodes()
+        k = self.mra.k
+        depth = np.zeros(n, np.int32)
+        trans = np.zeros((n, 3), np.int64)
+        parent = np.zeros(n, np.int32)
+        child0 = np.zeros(n, np.int32)
+        coef = np.zeros((n, 2 * k, 2 * k, 2 * k)) if with_coefs else None
+        _check(_lib.mw_tree_download(self._h, depth.ctypes.data_as(_ip), trans.ctypes.data_as(_lp),
+                                     parent.ctypes.data_as(_ip), child0.ctypes.data_as(_ip),
+                                     _d(coef) if with_coefs else None))
+        return dict(depth=depth, trans=trans, parent=parent, child0=child0, coef=coef)
+
+    def load(self, depth, trans, parent, child0, coef):
+        depth = np.ascontiguousarray(depth, np.int32)
+        trans = np.ascontiguousarray(trans, np.int64)
+        parent = np.ascontiguousarray(parent, np.int32)
+        child0 = np.ascontiguousarray(child0, np.int32)
+        coef = np.ascontiguousarray(coef, np.float64)
+        _check(_lib.mw_tree_upload(self._h, len(depth), depth.ctypes.data_as(_ip), trans.ctypes.data_as(_lp),
+                                   parent.ctypes.data_as(_ip), child0.ctypes.data_as(_ip), _d(coef)))
+
+    def device_arrays(self):
+        c, k, n = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        _check(_lib.mw_tree_device_arrays(self._h, ctypes.byref(c), ctypes.byref(k), ctypes.byref(n)))
+        return c.value, k.value, n.value
+
+
+def gauss_params(coefs, alphas, centers, powers=None):
+    """Parameter block of sum_g c_g (r-R_g)^p exp(-alpha_g |r-R_g|^2) (``GaussExp<3>`` analogue)."""
+    ng = len(coefs)
+    p = [float(ng)]
+    for g in range(ng):
+        pw = (0, 0, 0) if powers is None else powers[g]
+        p += [float(coefs[g]), float(alphas[g])] + [float(x) for x in centers[g]] + [float(x) for x in pw]
+    return FUNC_GAUSSIANS, np.array(p)
+
+
+def hydrogen_params(terms, Z=1.0, origin=(0.0, 0.0, 0.0)):
+    """sum_t c_t phi_a(r) phi_b(r) of hydrogen orbitals (reference ``HydrogenFunction``)."""
+    p = [float(len(terms))]
+    for (c, a, b) in terms:
+        b = b if b is not None else (0, 0, 0)
+        p += [float(c), *map(float, a), *map(float, b), float(Z), *map(float, origin)]
+    return FUNC_HYDROGEN_PRODUCTS, np.array(p)
+
+
+def project(prec, tree: FunctionTree, func):
+    ftype, params = func
+    params = np.ascontiguousarray(params, np.float64)
+    _check(_lib.mw_project(float(prec), tree._h, int(ftype), len(params), _d(params)))
+    return tree.nnodes()
+
+
+def dot(a: FunctionTree, b: FunctionTree):
+    v = ctypes.c_double()
+    _check(_lib.mw_dot(a._h, b._h, ctypes.byref(v)))
+    return v.value
+
+
+class ConvolutionOperator:
+    def __init__(self, mra, mu, prec):
+        self.mra = mra
+        self.mu = float(mu)
+        self.prec = float(prec)
+        h = ctypes.c_void_p()
+        L = load_library()
+        if self.mu == 0.0:
+            _check(L.mw_op_create_poisson(mra._h, self.prec, ctypes.byref(h)))
+        else:
+            _check(L.mw_op_create_helmholtz(mra._h, self.mu, self.prec, ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.mw_op_destroy(self._h)
+            self._h = None
+
+    def terms(self):
+        n = ctypes.c_int()
+        _check(_lib.mw_op_nterms(self._h, ctypes.byref(n)))
+        a = np.zeros(n.value)
+        b = np.zeros(n.value)
+        _check(_lib.mw_op_terms(self._h, _d(a), _d(b)))
+        return a, b
+
+
+class PoissonOperator(ConvolutionOperator):
+    """Kernel 1/|r|."""
+
+    def __init__(self, mra, prec):
+        super().__init__(mra, 0.0, prec)
+
+
+class HelmholtzOperator(ConvolutionOperator):
+    """Kernel exp(-mu|r|)/|r|."""
+
+    def __init__(self, mra, mu, prec):
+        if not mu > 0.0:
+            raise MWError("mu must be positive")
+        super().__init__(mra, mu, prec)
+
+
+def apply(prec, out: FunctionTree, op: ConvolutionOperator, inp: FunctionTree, flags=APPLY_FP64):
+    """out = op * inp (adaptive); returns (triples, triples_gen, passes, out_nodes)."""
+    _check(_lib.mw_apply(float(prec), out._h, op._h, inp._h, int(flags)))
+    st = np.zeros(4, np.int64)
+    _check(_lib.mw_apply_stats(out._h, st.ctypes.data_as(_lp)))
+    return tuple(int(x) for x in st)
