@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""Benchmark of the MW operator apply (batched Helmholtz, config 2).
+
+Workload (one step): 32 orbitals, each a normalised sum of 2-6 Gaussians (exponents log-U[0.5,200],
+centres on 8 seeded atom sites in a 6 Bohr box), projected at prec 1e-6 with interpolating order 9
+(k = 10) on the [-20,20]^3 world; one Helmholtz operator per orbital (mu ~ U[0.5,3]); the step
+applies all 32 operators (out_i = H_i phi_i, adaptive, prec 1e-6).  Inputs are resident in HBM
+when the timed region starts; their coefficient blocks (several GB per step) are larger than L2.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1: one process per GPU (torchrun); weak scaling, each rank applies its own 32-orbital batch.
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MW Poisson/Helmholtz apply time at 1e-6 rel. error: mixed+learned vs plain FP64 GPU"
+FP64_PEAK_NOMINAL = 37.0  # TFLOP/s, B200 datasheet FP64 (no measured FP64 peak on this pool)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="mw", choices=["mw", "reference"])
+    p.add_argument("--orbitals", type=int, default=32)
+    p.add_argument("--order", type=int, default=9)
+    p.add_argument("--prec", type=float, default=1e-6)
+    p.add_argument("--cpu-sample-seconds", type=float, default=12.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "_fallback": True}
+
+
+class Clocks:
+    """nvidia-smi sampling (200 ms) during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def workload(rank, n, seed=2):
+    from mrchem_b200 import workloads as W
+
+    return W.orbitals(n, seed=seed + 1000 * rank), W.helmholtz_mus(n, seed=seed + 1000 * rank)
+
+
+def flops_per_triple(k):
+    return 6 * (2 * k) ** 4
+
+
+# ----------------------------------------------------------------------------------------------
+# reference arm: the CPU restatement (MRCPP itself cannot be built here), all host threads
+# ----------------------------------------------------------------------------------------------
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from mrchem_b200 import workloads as W
+    from oracle import oracle as O
+
+    orbs, mus = workload(0, args.orbitals)
+    m = O.MultiResolutionAnalysis(W.WORLD["min_scale"], W.WORLD["corner"], W.WORLD["boxes"], args.order, 15)
+    n_use = min(4, args.orbitals)
+    trees, ops = [], []
+    for i in range(n_use):
+        t = O.FunctionTree(m)
+        O.project(args.prec, t, orbs[i])
+        trees.append(t)
+        ops.append(O.HelmholtzOperator(m, mus[i], args.prec))
+    outs = [O.FunctionTree(m) for _ in range(n_use)]
+
+    def step(s):
+        i = s % n_use
+        O.apply(args.prec, outs[i], ops[i], trees[i])
+
+    for i in range(n_use):  # operator tables are built on first use: build them all untimed
+        O.apply(args.prec, outs[i], ops[i], trees[i])
+    for s in range(args.warmup):
+        step(s)
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        step(args.warmup + s)
+    dt = time.perf_counter() - t0
+    cores = O.lib().oracle_num_threads()
+    val = args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": "applies/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "helmholtz_batch_32orb_k10_prec1e-6", "orbitals": args.orbitals,
+                   "order": args.order, "prec": args.prec, "step": "one orbital apply (rotating over the batch)"},
+        "cpu_baseline": {"value": val, "unit": "applies/s", "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} single-orbital Helmholtz applies (orbitals 0-{n_use - 1}); "
+                                   "FP64 CPU restatement (OpenMP), not MRCPP (not buildable here)"},
+        "e2e": {"value": val, "unit": "applies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------------------------------
+def run_gpu(args):
+    import torch
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from mrchem_b200 import mrcpp as G
+    from mrchem_b200 import workloads as W
+
+    stream = torch.cuda.Stream()
+    ctx = G.Context(local, stream=stream.cuda_stream)
+    m = G.MultiResolutionAnalysis(W.WORLD["min_scale"], W.WORLD["corner"], W.WORLD["boxes"], args.order, 15,
+                                  ctx=ctx)
+    orbs, mus = workload(rank, args.orbitals)
+    inps, ops, outs = [], [], []
+    for i in range(args.orbitals):
+        t = G.FunctionTree(m)
+        G.project(args.prec, t, orbs[i])
+        inps.append(t)
+        ops.append(G.HelmholtzOperator(m, mus[i], args.prec))
+        outs.append(G.FunctionTree(m))
+    in_bytes = sum(t.nnodes() for t in inps) * (2 * m.k) ** 3 * 8
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def step():
+        trip = 0
+        for i in range(args.orbitals):
+            st = G.apply(args.prec, outs[i], ops[i], inps[i])
+            trip += st[0]
+        return trip
+
+    for _ in range(args.warmup):
+        step()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    ctx.profile(True)
+    triples = 0
+    with Clocks(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            triples += step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    launches, apply_launches, apply_ms = ctx.profile_read()
+    ctx.profile(False)
+    clocks = clk.summary()
+    if world > 1:
+        tt = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        ms = float(tt.item())
+    total_applies = args.orbitals * args.steps * world
+    value = total_applies / (ms / 1e3)
+
+    # end to end through the public API from host buffers: upload, apply, download, every step
+    host = [t.export() for t in inps]
+    n_e2e = max(1, min(args.steps, 2))
+    e_in = [G.FunctionTree(m) for _ in range(args.orbitals)]
+    h2d = sum(h["coef"].nbytes + h["depth"].nbytes + h["trans"].nbytes + h["parent"].nbytes + h["child0"].nbytes
+              for h in host)
+    d2h = 0
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        d2h = 0
+        for i in range(args.orbitals):
+            h = host[i]
+            e_in[i].load(h["depth"], h["trans"], h["parent"], h["child0"], h["coef"])
+            G.apply(args.prec, outs[i], ops[i], e_in[i])
+            res = outs[i].export()
+            d2h += sum(v.nbytes for v in res.values() if v is not None)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        tt = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e_val = args.orbitals * n_e2e * world / e2e_s
+
+    peaks = measured_peaks()
+    k = m.k
+    flops = triples * flops_per_triple(k)
+    achieved = flops / (apply_ms / 1e3) / 1e12 if apply_ms > 0 else None
+    peak = float(peaks.get("bf16_tflops", 1590.0))
+    traffic = None
+    prof_file = os.path.join(ROOT, "profiles", "k_apply_fp64_traffic.json")
+    if os.path.exists(prof_file):
+        try:
+            traffic = json.load(open(prof_file)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args, inps, mus)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "applies/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "helmholtz_batch_32orb_k10_prec1e-6", "orbitals": args.orbitals,
+                       "order": args.order, "k": k, "prec": args.prec, "mu": "U[0.5,3]", "world": "[-20,20]^3",
+                       "path": "plain FP64 NS-form apply (CUDA cores)", "parallelism": f"replicas x{world}",
+                       "l2": f"inputs larger than L2 ({in_bytes / 1e9:.2f} GB of input blocks per step)"},
+            "e2e": {"value": e2e_val, "unit": "applies/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "tensor", "kernel": "k_apply_fp64", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if not peaks.get("_fallback")
+                         else "fallback", "fp64_peak_nominal": FP64_PEAK_NOMINAL,
+                         "frac_fp64_nominal": (achieved / FP64_PEAK_NOMINAL) if achieved else None,
+                         "flops_per_triple": flops_per_triple(k), "triples_per_step": triples // max(1, args.steps),
+                         "kernel_ms_per_step": apply_ms / args.steps, "kernel_launches": apply_launches},
+            "cpu_baseline": cpu,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+def cpu_baseline(args, inps, mus):
+    """Oracle (FP64 CPU restatement, OpenMP, all host threads) on a bounded sample of the batch."""
+    from mrchem_b200 import workloads as W
+    from oracle import oracle as O
+
+    m = O.MultiResolutionAnalysis(W.WORLD["min_scale"], W.WORLD["corner"], W.WORLD["boxes"], args.order, 15)
+    done, t_used = 0, 0.0
+    while done < len(inps) and t_used < args.cpu_sample_seconds:
+        ex = inps[done].export()
+        ti = O.FunctionTree(m)
+        ti.load(ex["depth"], ex["trans"], ex["parent"], ex["child0"], ex["coef"])
+        op = O.HelmholtzOperator(m, mus[done], args.prec)
+        to = O.FunctionTree(m)
+        O.apply(args.prec, to, op, ti)  # operator tables build lazily: warm them first
+        t0 = time.perf_counter()
+        O.apply(args.prec, to, op, ti)
+        t_used += time.perf_counter() - t0
+        done += 1
+    return {"value": done / t_used, "unit": "applies/s", "cores": O.lib().oracle_num_threads(), "kind": "port",
+            "sample": f"first {done} orbitals of the batch, one Helmholtz apply each ({t_used:.1f} s); "
+                      "FP64 CPU restatement (OpenMP), not MRCPP"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

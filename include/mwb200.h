@@ -41,6 +41,11 @@ int mw_version(int* major, int* minor);
 int mw_ctx_create(int device, void* stream, mw_ctx* out);
 int mw_ctx_destroy(mw_ctx ctx);
 int mw_ctx_synchronize(mw_ctx ctx);
+/* Benchmark counters (no reference counterpart: the reference times with mrcpp::Timer around whole
+ * calls, src/scf_solver/HelmholtzVector.cpp:68-82).  enable != 0 resets and starts them: number of
+ * kernels this library launched, and number and CUDA-event time (ms) of contraction-kernel launches. */
+int mw_ctx_profile(mw_ctx ctx, int enable);
+int mw_ctx_profile_read(mw_ctx ctx, long long* launches, long long* apply_launches, double* apply_ms);
 
 /* World and basis.  Replaces BoundingBox<3>(min_scale, corner, boxes) +
  * InterpolatingBasis(order) / LegendreBasis(order) + MultiResolutionAnalysis<3>(world, basis,

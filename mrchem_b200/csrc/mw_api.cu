@@ -441,7 +441,7 @@ static void apply(double prec, Tree& out, Op& op, Tree& inp) {
             ps.theta = kScreen * split_threshold(prec, g0, depth);
         }
         int np = 0;
-        while (np < (int)tab.deltas.size() && !(tab.deltas[np].maxb * nu_max < ps.theta)) ++np;
+        while (nu_max > 0.0 && np < (int)tab.deltas.size() && !(tab.deltas[np].maxb * nu_max < ps.theta)) ++np;
         ps.nprefix = np;
         for (int d = 0; d < 3; ++d) ps.ext[d] = (long long)m.boxes[d] << depth;
         run_apply_pass(out, b, e, inp, ps, s);
@@ -523,11 +523,37 @@ int mw_ctx_create(int device, void* stream, mw_ctx* out) {
     })
 }
 
+int mw_ctx_profile(mw_ctx ctx, int enable) {
+    MW_TRY({
+        MW_ARG(ctx, "null context");
+        MWB_CUDA(cudaSetDevice(ctx->device));
+        if (enable && !ctx->ev0) {
+            MWB_CUDA(cudaEventCreate(&ctx->ev0));
+            MWB_CUDA(cudaEventCreate(&ctx->ev1));
+        }
+        ctx->prof = enable != 0;
+        ctx->launches = 0;
+        ctx->apply_launches = 0;
+        ctx->apply_ms = 0.0;
+    })
+}
+
+int mw_ctx_profile_read(mw_ctx ctx, long long* launches, long long* apply_launches, double* apply_ms) {
+    MW_TRY({
+        MW_ARG(ctx && launches && apply_launches && apply_ms, "null pointer");
+        *launches = ctx->launches;
+        *apply_launches = ctx->apply_launches;
+        *apply_ms = ctx->apply_ms;
+    })
+}
+
 int mw_ctx_destroy(mw_ctx ctx) {
     MW_TRY({
         if (!ctx) return MW_OK;
         cudaSetDevice(ctx->device);
         cudaStreamSynchronize(ctx->stream);
+        if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+        if (ctx->ev1) cudaEventDestroy(ctx->ev1);
         if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
         delete ctx;
     })

@@ -36,6 +36,13 @@ struct Ctx {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int num_sms = 0;
+    // profiling counters (benchmarks): kernels of this library launched, and CUDA-event time of
+    // the contraction kernel when enabled
+    bool prof = false;
+    long long launches = 0;
+    long long apply_launches = 0;
+    double apply_ms = 0.0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
 struct Mra {

@@ -490,14 +490,16 @@ __global__ void k_candidates(CandArgs a, int fill) {
                 const uint64_t key = make_key(a.depth, ti[0], ti[1], ti[2]);
                 const int idx = hlookup(a.in.hkey, a.in.hval, a.in.hcap, key);
                 if (idx >= 0) {
-                    if (de.maxb * sqrt(a.in.norm2[idx]) >= a.theta) { ok = 1; src = idx; }
+                    const double nu = sqrt(a.in.norm2[idx]);
+                    if (nu > 0.0 && de.maxb * nu >= a.theta) { ok = 1; src = idx; }
                 } else {
                     for (int da = a.depth - 1; da >= 0 && leaf < 0; --da) {
                         const int sh = a.depth - da;
                         leaf = hlookup(a.in.hkey, a.in.hval, a.in.hcap,
                                        make_key(da, ti[0] >> sh, ti[1] >> sh, ti[2] >> sh));
                     }
-                    if (leaf >= 0 && de.maxb * sqrt(a.in.norm2[leaf]) >= a.theta) {
+                    const double nul = leaf >= 0 ? sqrt(a.in.norm2[leaf]) : 0.0;
+                    if (nul > 0.0 && de.maxb * nul >= a.theta) {
                         ok = 1;
                         gk = key;
                     }
@@ -813,7 +815,7 @@ __global__ void __launch_bounds__(ApplyCfg<K>::NT, 1) k_apply_fp64(ApplyArgs A) 
         const bool gen = src < 0;
         const double nu = gen ? sqrt(A.gnorm2[-src - 1]) : sqrt(A.in.norm2[src]);
         const DeltaRec de = A.deltas[e];
-        if (de.maxb * nu < A.theta) continue;
+        if (!(nu > 0.0) || de.maxb * nu < A.theta) continue;
         if (A.terms[de.t0].bound * nu < A.theta) continue;
         const double* blk = gen ? A.gblk + (size_t)(-src - 1) * K * K * K : A.in.coef + (size_t)src * G::BS;
         // stage the input block (full (2k)^3, or the k^3 scaling block of a generated node); the
@@ -879,6 +881,8 @@ __global__ void __launch_bounds__(ApplyCfg<K>::NT, 1) k_apply_fp64(ApplyArgs A) 
 // launchers
 // ---------------------------------------------------------------------------------------------
 
+static inline void count(Ctx* c, int n = 1) { c->launches += n; }
+
 #define MWB_DISPATCH_K(k, F)                                    \
     switch (k) {                                                \
         case 4: F(4); break;                                    \
@@ -925,6 +929,7 @@ void launch_transform_nodes(Tree& t, int mode, const int* d_nodes, int nnodes, c
     MWB_DISPATCH_K(m.k, L_TR)
 #undef L_TR
     MWB_CUDA(cudaGetLastError());
+    count(m.ctx);
 }
 
 void launch_node_norms(Tree& t, int begin, int end, cudaStream_t s) {
@@ -935,16 +940,19 @@ void launch_node_norms(Tree& t, int begin, int end, cudaStream_t s) {
     MWB_DISPATCH_K(t.mra->k, L_NN)
 #undef L_NN
     MWB_CUDA(cudaGetLastError());
+    count(t.mra->ctx);
 }
 
 void launch_hash_reset(Tree& t, cudaStream_t s) {
     k_hash_reset<<<std::min<uint32_t>((t.hcap + 255) / 256, 4096), 256, 0, s>>>(t.hkey, t.hval, t.hcap);
     MWB_CUDA(cudaGetLastError());
+    count(t.mra->ctx);
 }
 void launch_hash_insert(Tree& t, int begin, int end, cudaStream_t s) {
     if (end <= begin) return;
     k_hash_insert<<<(end - begin + 255) / 256, 256, 0, s>>>(t.hkey, t.hval, t.hcap, t.key, begin, end);
     MWB_CUDA(cudaGetLastError());
+    count(t.mra->ctx);
 }
 
 // flags -> exclusive scan -> list; returns the count (synchronises the stream)
@@ -957,6 +965,7 @@ static int compact_flags(Ctx* ctx, int* d_flags, int n, int begin, int* d_list, 
     MWB_CUDA(cub::DeviceScan::ExclusiveSum(d_tmp, tmp, d_flags, d_pos, n + 1, s));
     k_scatter_list<<<(n + 255) / 256, 256, 0, s>>>(d_flags, d_pos, begin, n, d_list);
     MWB_CUDA(cudaGetLastError());
+    count(ctx);
     int total = 0;
     MWB_CUDA(cudaMemcpyAsync(&total, d_pos + n, sizeof(int), cudaMemcpyDeviceToHost, s));
     MWB_CUDA(cudaStreamSynchronize(s));
@@ -975,6 +984,7 @@ int launch_split(Tree& t, int begin, int end, int depth, double thr, int depth_l
     MWB_CUDA(cudaMemsetAsync(d_flags, 0, sizeof(int) * (n + 1), s));
     k_split_flags<<<(n + 255) / 256, 256, 0, s>>>(t.wnorm2, t.key, begin, end, thr, depth_limit, d_flags);
     MWB_CUDA(cudaGetLastError());
+    count(ctx);
     int cnt = compact_flags(ctx, d_flags, n, begin, d_list, s);
     dfree(ctx, d_flags);
     return cnt;
@@ -988,6 +998,7 @@ int launch_internal_list(Tree& t, int begin, int end, int* d_list, cudaStream_t 
     MWB_CUDA(cudaMemsetAsync(d_flags, 0, sizeof(int) * (n + 1), s));
     k_internal_flags<<<(n + 255) / 256, 256, 0, s>>>(t.child0, begin, end, d_flags);
     MWB_CUDA(cudaGetLastError());
+    count(ctx);
     int cnt = compact_flags(ctx, d_flags, n, begin, d_list, s);
     dfree(ctx, d_flags);
     return cnt;
@@ -997,6 +1008,7 @@ void launch_make_children(Tree& t, const int* d_list, int nsplit, cudaStream_t s
     if (nsplit <= 0) return;
     k_make_children<<<(nsplit + 127) / 128, 128, 0, s>>>(view(t), d_list, nsplit, t.n);
     MWB_CUDA(cudaGetLastError());
+    count(t.mra->ctx);
 }
 
 static double reduce_impl(Tree& t, int begin, int end, int leaves, int mx, cudaStream_t s) {
@@ -1005,6 +1017,7 @@ static double reduce_impl(Tree& t, int begin, int end, int leaves, int mx, cudaS
     double* d = (double*)dalloc(ctx, sizeof(double));
     k_reduce_norm2<<<1, 1024, 0, s>>>(t.norm2, t.child0, begin, end, leaves, mx, d);
     MWB_CUDA(cudaGetLastError());
+    count(ctx);
     double h = 0.0;
     MWB_CUDA(cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, s));
     MWB_CUDA(cudaStreamSynchronize(s));
@@ -1021,6 +1034,7 @@ void launch_rescale(Tree& t, double c, cudaStream_t s) {
     k_rescale<<<64, 256, 0, s>>>(t.norm2, (size_t)t.n, c * c);
     k_rescale<<<64, 256, 0, s>>>(t.wnorm2, (size_t)t.n, c * c);
     MWB_CUDA(cudaGetLastError());
+    count(t.mra->ctx, 3);
 }
 
 double launch_dot(Tree& a, Tree& b, cudaStream_t s) {
@@ -1034,6 +1048,7 @@ double launch_dot(Tree& a, Tree& b, cudaStream_t s) {
 #undef L_DOT
     k_sum_array<<<1, 1024, 0, s>>>(part, a.n, d);
     MWB_CUDA(cudaGetLastError());
+    count(ctx, 2);
     double h = 0.0;
     MWB_CUDA(cudaMemcpyAsync(&h, d, sizeof(double), cudaMemcpyDeviceToHost, s));
     MWB_CUDA(cudaStreamSynchronize(s));
@@ -1069,6 +1084,7 @@ void run_apply_pass(Tree& out, int obegin, int oend, Tree& inp, ApplyPass& pass,
     const int cblocks = (nwork * 32 + 255) / 256;
     k_candidates<<<cblocks, 256, 0, s>>>(ca, 0);
     MWB_CUDA(cudaGetLastError());
+    count(ctx);
     size_t tmp = 0;
     MWB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, d_count, d_offs, nwork + 1, s));
     void* d_tmp = dalloc(ctx, tmp);
@@ -1092,6 +1108,7 @@ void run_apply_pass(Tree& out, int obegin, int oend, Tree& inp, ApplyPass& pass,
     if (ncand > 0) {
         k_candidates<<<cblocks, 256, 0, s>>>(ca, 1);
         MWB_CUDA(cudaGetLastError());
+        count(ctx);
     }
     int ngreq = 0;
     MWB_CUDA(cudaMemcpyAsync(&ngreq, d_ngreq, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1140,6 +1157,7 @@ void run_apply_pass(Tree& out, int obegin, int oend, Tree& inp, ApplyPass& pass,
         MWB_DISPATCH_K(K, L_GEN)
 #undef L_GEN
         MWB_CUDA(cudaGetLastError());
+        count(ctx, 4);
         dfree(ctx, d_sk);
         dfree(ctx, d_sl);
         dfree(ctx, d_flags);
@@ -1173,12 +1191,21 @@ void run_apply_pass(Tree& out, int obegin, int oend, Tree& inp, ApplyPass& pass,
                                       (int)smem));                                                    \
         k_apply_fp64<KK><<<nwork, ApplyCfg<KK>::NT, smem, s>>>(aa);                                   \
     }
+    if (ctx->prof) MWB_CUDA(cudaEventRecord(ctx->ev0, s));
     MWB_DISPATCH_K(K, L_AP)
 #undef L_AP
     MWB_CUDA(cudaGetLastError());
+    if (ctx->prof) MWB_CUDA(cudaEventRecord(ctx->ev1, s));
+    count(ctx);
+    ctx->apply_launches++;
     unsigned long long nt = 0;
     MWB_CUDA(cudaMemcpyAsync(&nt, d_ntrip, sizeof(nt), cudaMemcpyDeviceToHost, s));
     MWB_CUDA(cudaStreamSynchronize(s));
+    if (ctx->prof) {
+        float ms = 0.0f;
+        MWB_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        ctx->apply_ms += ms;
+    }
     pass.triples = (long long)nt;
     pass.triples_gen = 0;
 

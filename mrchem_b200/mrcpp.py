@@ -44,6 +44,8 @@ SYMBOLS = [
     ("mw_ctx_create", ctypes.c_int, [ctypes.c_int, _vp, _vpp]),
     ("mw_ctx_destroy", ctypes.c_int, [_vp]),
     ("mw_ctx_synchronize", ctypes.c_int, [_vp]),
+    ("mw_ctx_profile", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("mw_ctx_profile_read", ctypes.c_int, [_vp, _lp, _lp, _dp]),
     ("mw_mra_create", ctypes.c_int, [_vp, ctypes.c_int, _ip, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vpp]),
     ("mw_mra_destroy", ctypes.c_int, [_vp]),
     ("mw_mra_filter", ctypes.c_int, [_vp, _dp]),
@@ -120,6 +122,16 @@ class Context:
 
     def synchronize(self):
         _check(_lib.mw_ctx_synchronize(self._h))
+
+    def profile(self, enable=True):
+        """Reset and (de)activate the kernel counters."""
+        _check(_lib.mw_ctx_profile(self._h, int(enable)))
+
+    def profile_read(self):
+        """(kernels launched, contraction launches, contraction CUDA-event ms) since profile()."""
+        a, b, c = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_double()
+        _check(_lib.mw_ctx_profile_read(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
 
 
 class MultiResolutionAnalysis:

@@ -977,7 +977,7 @@ void apply(double prec, Tree& out, Operator& op, const Tree& inp, ApplyStats* st
         for (size_t q = 0; q < work.size(); ++q) {
             const Node& o = out.nodes[work[q]];
             for (size_t e = 0; e < dl.size(); ++e) {
-                if (dl[e].maxb * nu_max < theta) break;
+                if (!(nu_max > 0.0) || dl[e].maxb * nu_max < theta) break;
                 int64_t ti[3];
                 bool inside = true;
                 for (int d = 0; d < 3; ++d) {
@@ -987,7 +987,7 @@ void apply(double prec, Tree& out, Operator& op, const Tree& inp, ApplyStats* st
                 if (!inside) continue;
                 int idx = inp.find(depth, ti);
                 if (idx >= 0) {
-                    if (dl[e].maxb * inorm[idx] < theta) continue;
+                    if (!(inorm[idx] > 0.0) || dl[e].maxb * inorm[idx] < theta) continue;
                     cands[q].push_back({(int)e, idx});
                 } else {
                     int leaf = -1;
@@ -996,7 +996,7 @@ void apply(double prec, Tree& out, Operator& op, const Tree& inp, ApplyStats* st
                         leaf = inp.find(da, ta);
                     }
                     if (leaf < 0) continue;
-                    if (dl[e].maxb * inorm[leaf] < theta) continue;  // ||gen|| <= ||leaf||
+                    if (!(inorm[leaf] > 0.0) || dl[e].maxb * inorm[leaf] < theta) continue;  // ||gen|| <= ||leaf||
                     cands[q].push_back({(int)e, -1});
                     genreq[q].push_back({node_key(depth, ti), {leaf, {ti[0], ti[1], ti[2]}}});
                 }
@@ -1036,7 +1036,7 @@ void apply(double prec, Tree& out, Operator& op, const Tree& inp, ApplyStats* st
                 const bool gen = c.src < 0;
                 const double* blk = gen ? &gblk[(size_t)(-c.src - 1) * SS] : inp.nodes[c.src].c.data();
                 const double nu = gen ? gnorm[-c.src - 1] : inorm[c.src];
-                if (de.maxb * nu < theta) continue;
+                if (!(nu > 0.0) || de.maxb * nu < theta) continue;
                 if (!gen && !root) {
                     for (int z = 0; z < k; ++z)
                         for (int y = 0; y < k; ++y)

@@ -1,0 +1,268 @@
+"""GPU parity: the sm_100a path (through the C-ABI) against the FP64 CPU oracle on the same inputs.
+
+Bar: integer tree structure (node keys) identical; FP64 coefficients within 1e-10 of the largest
+coefficient (observed ~1e-13: only summation order differs).  Inputs are projected on the GPU and
+loaded unchanged into the oracle, so both sides apply to the identical input tree.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+from scipy.special import erf
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+WORLD = (-2, (-5, -5, -5), (10, 10, 10))
+COEF_TOL = 1e-10
+
+
+def keyed(ex):
+    return {(int(d), *map(int, t)): i for i, (d, t) in enumerate(zip(ex["depth"], ex["trans"]))}
+
+
+def assert_same_tree(eg, eo, tol=COEF_TOL):
+    kg, ko = keyed(eg), keyed(eo)
+    assert set(kg) == set(ko), f"structure differs: {len(kg)} vs {len(ko)} nodes"
+    scale = max(np.abs(eo["coef"]).max(), 1e-300)
+    diff = max(np.abs(eg["coef"][kg[q]] - eo["coef"][ko[q]]).max() for q in kg)
+    assert diff <= tol * scale, (diff, scale)
+    # parent / child links describe the same tree
+    for q, i in kg.items():
+        j = ko[q]
+        pg, po = eg["parent"][i], eo["parent"][j]
+        if pg < 0:
+            assert po < 0
+        else:
+            assert (int(eg["depth"][pg]), *map(int, eg["trans"][pg])) == (int(eo["depth"][po]), *map(int, eo["trans"][po]))
+        assert (eg["child0"][i] < 0) == (eo["child0"][j] < 0)
+    return diff / scale
+
+
+def to_oracle(O, mo, tree_g):
+    ex = tree_g.export()
+    t = O.FunctionTree(mo)
+    t.load(ex["depth"], ex["trans"], ex["parent"], ex["child0"], ex["coef"])
+    return t
+
+
+def pair(G, O, order, max_depth=14, basis=0, world=WORLD):
+    return (G.MultiResolutionAnalysis(*world, order, max_depth, basis=basis),
+            O.MultiResolutionAnalysis(*world, order, max_depth, basis=basis))
+
+
+def two_gaussians(G):
+    return G.gauss_params([(10 / np.pi) ** 1.5, 0.5 * (30 / np.pi) ** 1.5], [10.0, 30.0],
+                          [(0.1, -0.2, 0.3), (-0.5, 0.4, 0.0)])
+
+
+@pytest.mark.parametrize("order,prec,basis", [(5, 1e-3, 0), (7, 1e-5, 0), (9, 1e-6, 0), (7, 1e-5, 1)])
+def test_projection_parity(gpu_mod, oracle_mod, order, prec, basis):
+    G, O = gpu_mod, oracle_mod
+    mg, mo = pair(G, O, order, basis=basis)
+    assert np.abs(mg.filter() - mo.filter()).max() < 1e-10
+    f = two_gaussians(G)
+    tg = G.FunctionTree(mg)
+    G.project(prec, tg, f)
+    to = O.FunctionTree(mo)
+    O.project(prec, to, f)
+    assert_same_tree(tg.export(), to.export())
+    assert abs(tg.square_norm() - to.square_norm()) < 1e-12 * to.square_norm()
+
+
+@pytest.mark.parametrize("order,prec,mu", [(5, 1e-3, 0.0), (5, 1e-3, 1.3), (7, 1e-5, 0.0), (7, 1e-5, 2.0),
+                                           (9, 1e-6, 0.0), (9, 1e-6, 0.8)])
+def test_apply_parity(gpu_mod, oracle_mod, order, prec, mu):
+    G, O = gpu_mod, oracle_mod
+    mg, mo = pair(G, O, order)
+    inp = G.FunctionTree(mg)
+    G.project(prec, inp, two_gaussians(G))
+    inp_o = to_oracle(O, mo, inp)
+    out = G.FunctionTree(mg)
+    sg = G.apply(prec, out, G.ConvolutionOperator(mg, mu, prec), inp)
+    out_o = O.FunctionTree(mo)
+    so = O.apply(prec, out_o, O.ConvolutionOperator(mo, mu, prec), inp_o)
+    assert sg[0] == so[0], "contracted triple counts differ"
+    assert sg[2] == so[2], "refinement pass counts differ"
+    assert_same_tree(out.export(), out_o.export())
+    assert abs(G.dot(out, inp) - O.dot(out_o, inp_o)) < 1e-11 * abs(O.dot(out_o, inp_o))
+
+
+def test_apply_matches_analytic_potential(gpu_mod, oracle_mod):
+    """Poisson of a normalised Gaussian is erf(sqrt(a) r)/r (config-1 accuracy level)."""
+    G, O = gpu_mod, oracle_mod
+    prec = 1e-5
+    mg, mo = pair(G, O, 7)
+    alpha, c = 25.0, np.array([0.3, 0.1, -0.2])
+    inp = G.FunctionTree(mg)
+    G.project(prec, inp, G.gauss_params([(alpha / np.pi) ** 1.5], [alpha], [c]))
+    out = G.FunctionTree(mg)
+    G.apply(prec, out, G.PoissonOperator(mg, prec), inp)
+    ev = to_oracle(O, mo, out)
+    rng = np.random.default_rng(3)
+    err = 0.0
+    for _ in range(300):
+        r = c + rng.uniform(-5, 5, 3)
+        d = np.linalg.norm(r - c)
+        err = max(err, abs(ev.evalf(r) - erf(np.sqrt(alpha) * d) / d))
+    assert err < 2e-5 * 2 * np.sqrt(alpha / np.pi)
+
+
+def test_config1_poisson(gpu_mod, oracle_mod):
+    """Config 1 as specified: order 7, prec 1e-5, 3 unit Gaussians (seed 1); parity + analytic."""
+    from mrchem_b200 import workloads as W
+
+    G, O = gpu_mod, oracle_mod
+    prec = 1e-5
+    mg, mo = pair(G, O, 7, max_depth=15)
+    f, meta = W.poisson_density(seed=1)
+    inp = G.FunctionTree(mg)
+    G.project(prec, inp, f)
+    out = G.FunctionTree(mg)
+    G.apply(prec, out, G.PoissonOperator(mg, prec), inp)
+    out_o = O.FunctionTree(mo)
+    O.apply(prec, out_o, O.PoissonOperator(mo, prec), to_oracle(O, mo, inp))
+    assert_same_tree(out.export(), out_o.export())
+    rng = np.random.default_rng(5)
+    err, vmax = 0.0, 0.0
+    for _ in range(200):
+        r = rng.uniform(-6, 6, 3)
+        v = sum(erf(np.sqrt(a) * np.linalg.norm(r - c)) / np.linalg.norm(r - c)
+                for a, c in zip(meta["alphas"], meta["centers"]))
+        err = max(err, abs(out_o.evalf(r) - v))
+        vmax = max(vmax, v)
+    assert err < 3e-5 * vmax
+
+
+def test_config2_orbitals_helmholtz_subset(gpu_mod, oracle_mod):
+    """Two orbitals of config 2 (order 9, prec 1e-6, Helmholtz mu from the seeded draw)."""
+    from mrchem_b200 import workloads as W
+
+    G, O = gpu_mod, oracle_mod
+    prec = 1e-6
+    mg, mo = pair(G, O, 9, max_depth=15)
+    orbs = W.orbitals(32, seed=2)
+    mus = W.helmholtz_mus(32, seed=2)
+    for i in (0, 7):
+        inp = G.FunctionTree(mg)
+        G.project(prec, inp, orbs[i])
+        assert abs(inp.square_norm() - 1.0) < 1e-5
+        out = G.FunctionTree(mg)
+        G.apply(prec, out, G.HelmholtzOperator(mg, mus[i], prec), inp)
+        out_o = O.FunctionTree(mo)
+        O.apply(prec, out_o, O.HelmholtzOperator(mo, mus[i], prec), to_oracle(O, mo, inp))
+        assert_same_tree(out.export(), out_o.export())
+
+
+def test_hydrogen_coulomb_kat(gpu_mod, oracle_mod):
+    """Reference KAT quantities (tests/qmoperators/coulomb_operator.cpp) through the GPU path."""
+    G = gpu_mod
+    kat = json.load(open(os.path.join(HERE, "golden", "reference_kats.json")))
+    w = kat["world"]
+    m = G.MultiResolutionAnalysis(w["min_scale"], w["corner"], w["boxes"], 7, w["max_depth"])
+    orbs = [tuple(o) for o in kat["orbitals"]]
+    prec = 1e-5
+    rho = G.FunctionTree(m)
+    G.project(prec, rho, G.hydrogen_params([(2.0, o, o) for o in orbs]))
+    V = G.FunctionTree(m)
+    G.apply(prec / np.sqrt(rho.square_norm()), V, G.PoissonOperator(m, prec), rho)
+    for key, expr in kat["analytic_E_P"].items():
+        i, j = map(int, key.split(","))
+        d = G.FunctionTree(m)
+        G.project(1e-7, d, G.hydrogen_params([(1.0, orbs[i], orbs[j])]))
+        val = G.dot(d, V)
+        exact = eval(expr)
+        assert abs(val - exact) / exact < 1e-4
+
+
+def test_upload_download_roundtrip(gpu_mod, oracle_mod):
+    G, O = gpu_mod, oracle_mod
+    mg, mo = pair(G, O, 7)
+    to = O.FunctionTree(mo)
+    O.project(1e-4, to, two_gaussians(G))
+    eo = to.export()
+    tg = G.FunctionTree(mg)
+    tg.load(eo["depth"], eo["trans"], eo["parent"], eo["child0"], eo["coef"])
+    eg = tg.export()
+    assert_same_tree(eg, eo, tol=0.0)
+    assert abs(tg.square_norm() - to.square_norm()) < 1e-13 * to.square_norm()
+
+
+def test_rescale_and_dot(gpu_mod, oracle_mod):
+    G, O = gpu_mod, oracle_mod
+    mg, mo = pair(G, O, 5)
+    a = G.FunctionTree(mg)
+    G.project(1e-3, a, two_gaussians(G))
+    b = G.FunctionTree(mg)
+    G.project(1e-3, b, G.gauss_params([1.0], [2.0], [(0.2, 0.0, 0.0)]))
+    d0 = G.dot(a, b)
+    assert abs(d0 - O.dot(to_oracle(O, mo, a), to_oracle(O, mo, b))) < 1e-12 * abs(d0)
+    n0 = a.square_norm()
+    a.rescale(-1.0 / (2 * np.pi))  # HelmholtzVector.cpp:81
+    assert abs(a.square_norm() - n0 / (4 * np.pi ** 2)) < 1e-12 * n0
+    assert abs(G.dot(a, b) + d0 / (2 * np.pi)) < 1e-12 * abs(d0)
+
+
+def test_zero_function(gpu_mod):
+    G = gpu_mod
+    m = G.MultiResolutionAnalysis(*WORLD, 5, 10)
+    z = G.FunctionTree(m)
+    G.project(1e-3, z, G.gauss_params([0.0], [1.0], [(0.0, 0.0, 0.0)]))
+    assert z.nnodes() == 1000 and z.square_norm() == 0.0
+    out = G.FunctionTree(m)
+    G.apply(1e-3, out, G.PoissonOperator(m, 1e-3), z)
+    assert out.nnodes() == 1000 and out.square_norm() == 0.0
+
+
+def test_depth_limit(gpu_mod, oracle_mod):
+    G, O = gpu_mod, oracle_mod
+    mg, mo = pair(G, O, 5, max_depth=2)
+    f = G.gauss_params([(200 / np.pi) ** 1.5], [200.0], [(0.05, 0.05, 0.05)])
+    tg = G.FunctionTree(mg)
+    G.project(1e-6, tg, f)
+    assert tg.export()["depth"].max() == 2
+    to = O.FunctionTree(mo)
+    O.project(1e-6, to, f)
+    assert_same_tree(tg.export(), to.export())
+    out = G.FunctionTree(mg)
+    G.apply(1e-6, out, G.PoissonOperator(mg, 1e-6), tg)
+    out_o = O.FunctionTree(mo)
+    O.apply(1e-6, out_o, O.PoissonOperator(mo, 1e-6), to_oracle(O, mo, tg))
+    assert_same_tree(out.export(), out_o.export())
+
+
+def test_single_root_world(gpu_mod, oracle_mod):
+    G, O = gpu_mod, oracle_mod
+    world = (0, (-1, -1, -1), (1, 1, 1))  # one root box [-1, 0)^3 ... edge 1
+    mg, mo = pair(G, O, 5, max_depth=8, world=world)
+    f = G.gauss_params([1.0], [20.0], [(-0.5, -0.5, -0.5)])
+    tg = G.FunctionTree(mg)
+    G.project(1e-4, tg, f)
+    out = G.FunctionTree(mg)
+    G.apply(1e-4, out, G.HelmholtzOperator(mg, 1.0, 1e-4), tg)
+    out_o = O.FunctionTree(mo)
+    O.apply(1e-4, out_o, O.HelmholtzOperator(mo, 1.0, 1e-4), to_oracle(O, mo, tg))
+    assert_same_tree(out.export(), out_o.export())
+
+
+def test_errors_are_reported(gpu_mod):
+    G = gpu_mod
+    with pytest.raises(G.MWError):
+        G.MultiResolutionAnalysis(*WORLD, 15, 10)  # order out of range
+    m1 = G.MultiResolutionAnalysis(*WORLD, 5, 10)
+    m2 = G.MultiResolutionAnalysis(*WORLD, 5, 10)
+    a = G.FunctionTree(m1)
+    G.project(1e-3, a, G.gauss_params([1.0], [1.0], [(0.0, 0.0, 0.0)]))
+    with pytest.raises(G.MWError):
+        G.apply(1e-3, G.FunctionTree(m2), G.PoissonOperator(m1, 1e-3), a)  # different worlds
+    with pytest.raises(G.MWError):
+        G.apply(1e-3, G.FunctionTree(m1), G.PoissonOperator(m1, 1e-3), G.FunctionTree(m1))  # empty input
+    with pytest.raises(G.MWError):
+        G.HelmholtzOperator(m1, -1.0, 1e-3)
+    with pytest.raises(G.MWError):
+        G.project(1e-3, a, (7, np.array([1.0])))  # unknown function type
+    # the context still works after the errors
+    b = G.FunctionTree(m1)
+    G.project(1e-3, b, G.gauss_params([1.0], [1.0], [(0.0, 0.0, 0.0)]))
+    assert b.square_norm() > 0
