@@ -87,6 +87,20 @@ int mw_project(double prec, mw_tree tree, int func_type, int nparams, const doub
  * tests/qmoperators/coulomb_operator.cpp:90). */
 int mw_dot(mw_tree a, mw_tree b, double* out);
 
+/* Allocation-free inner product <a|b>.  No counterpart in the reference: it serves callers that
+ * cannot allocate device memory when they need the result -- a thread recording a CUDA graph
+ * (allocation is not capturable), code under a fixed, pre-reserved memory budget, or a host whose
+ * device memory pool belongs to another framework.  Same result as mw_dot (which allocates two
+ * small scratch buffers per call), computed with a fixed scratch array compiled into the library:
+ * 8 MiB per GPU that loads the library, held until process exit.
+ *   - `a` may have at most 1048576 (2^20) nodes; larger trees return MW_ERR_CAPACITY.
+ *   - The first call on a device looks up the array's device address; make that first call before
+ *     any stream capture on that device.
+ *   - Every call shares the one array: calls that overlap on the GPU (other streams, other threads)
+ *     race and must be serialised by the caller.
+ *   - `out` is a host pointer; the call returns after the result is written. */
+int mw_nalloc_dot(mw_tree a, mw_tree b, double* out);
+
 /* Convolution operators.  Replace mrcpp::PoissonOperator(MRA, prec) (reference src/SCFDriver.cpp:279,
  * tests/qmoperators/coulomb_operator.cpp:84) and mrcpp::HelmholtzOperator(MRA, mu, prec)
  * (reference src/scf_solver/HelmholtzVector.cpp:171).  Kernels 1/|r| and exp(-mu|r|)/|r|. */

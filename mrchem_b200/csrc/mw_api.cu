@@ -18,6 +18,9 @@ void host_key_trans(uint64_t k, long long t[3]);
 
 static thread_local std::string g_err;
 
+// lets other translation units of the C-ABI report an error through mw_last_error()
+void set_last_error(const std::string& msg) { g_err = msg; }
+
 void* dalloc(Ctx* ctx, size_t bytes) {
     void* p = nullptr;
     if (bytes == 0) bytes = 16;

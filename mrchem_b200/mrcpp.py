@@ -60,6 +60,7 @@ SYMBOLS = [
     ("mw_tree_rescale", ctypes.c_int, [_vp, ctypes.c_double]),
     ("mw_project", ctypes.c_int, [ctypes.c_double, _vp, ctypes.c_int, ctypes.c_int, _dp]),
     ("mw_dot", ctypes.c_int, [_vp, _vp, _dp]),
+    ("mw_nalloc_dot", ctypes.c_int, [_vp, _vp, _dp]),
     ("mw_op_create_poisson", ctypes.c_int, [_vp, ctypes.c_double, _vpp]),
     ("mw_op_create_helmholtz", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _vpp]),
     ("mw_op_destroy", ctypes.c_int, [_vp]),
@@ -256,6 +257,14 @@ def project(prec, tree: FunctionTree, func):
 def dot(a: FunctionTree, b: FunctionTree):
     v = ctypes.c_double()
     _check(_lib.mw_dot(a._h, b._h, ctypes.byref(v)))
+    return v.value
+
+
+def nalloc_dot(a: FunctionTree, b: FunctionTree):
+    """<a|b> without any device allocation (for callers that cannot allocate, e.g. while recording a
+    CUDA graph); at most 2^20 nodes in `a`; concurrent calls on one GPU must be serialised."""
+    v = ctypes.c_double()
+    _check(_lib.mw_nalloc_dot(a._h, b._h, ctypes.byref(v)))
     return v.value
 
 

@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
     for name in sorted(declared_symbols()):
         assert hasattr(lib, name), name
     bound = {s[0] for s in mrcpp.SYMBOLS}
-    assert declared_symbols() <= bound | {n for n in declared_symbols() if n.startswith("mw_nalloc")}
+    assert declared_symbols() <= bound
 
 
 def test_library_rejects_bad_arguments_without_gpu():
