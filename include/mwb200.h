@@ -115,8 +115,14 @@ int mw_op_terms(mw_op op, double* alpha, double* beta);
  * src/qmoperators/two_electron/ExchangePotential.cpp:137,259,318.  `out` is overwritten and left
  * compressed with valid norms. */
 int mw_apply(double prec, mw_tree out, mw_op op, mw_tree inp, int flags);
-/* statistics of the last apply into `out`: [0] contracted (out node, in node, term) triples,
- * [1] of which with a generated input node, [2] refinement passes, [3] output nodes */
+/* Batched apply: out[i] = ops[i] * inp[i] for i < n (n <= 128), all on one world; the refinement
+ * passes of the whole batch run together (one launch per stage and depth).  Same result per tree as
+ * n separate mw_apply calls.  Replaces the per-orbital loop of reference
+ * src/scf_solver/HelmholtzVector.cpp:129-135,168-184 (one HelmholtzOperator and one apply per orbital). */
+int mw_apply_batched(int n, double prec, mw_tree* out, mw_op* ops, mw_tree* inp, int flags);
+/* statistics of the last apply into `out`: [0] contracted (out node, in node, term) triples of this
+ * tree (-1 after a batched apply of more than one tree), [1] triples of the whole batch,
+ * [2] refinement passes, [3] output nodes */
 int mw_apply_stats(mw_tree out, long long* stats);
 
 #ifdef __cplusplus

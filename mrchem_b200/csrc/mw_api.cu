@@ -415,52 +415,103 @@ static void op_init(Op& op, Mra* m, double mu, double prec) {
 // apply
 // ---------------------------------------------------------------------------------------------
 
-static void apply(double prec, Tree& out, Op& op, Tree& inp) {
-    if (out.mra != inp.mra || op.mra != inp.mra) throw Error(MW_ERR_ARG, "trees and operator must share the world");
-    if (&out == &inp) throw Error(MW_ERR_ARG, "in-place apply is not supported");
-    if (inp.n == 0) throw Error(MW_ERR_STATE, "input tree is empty");
-    const Mra& m = *inp.mra;
-    Ctx* ctx = m.ctx;
+static void tree_add_children(Tree& t, const std::vector<int>& list) {
+    const int ns = (int)list.size();
+    if (ns == 0) return;
+    Ctx* ctx = t.mra->ctx;
     cudaStream_t s = ctx->stream;
-    tree_make_roots(out);
-    const double fnorm = std::sqrt(reduce_leaf_norm2(inp, s));
-    const double nu_max = std::sqrt(reduce_max_norm2(inp, s));
-    double g0 = 0.0;
-    long long trip = 0;
-    int passes = 0;
-    for (int depth = 0;; ++depth) {
-        const int b = out.level_begin[depth], e = out.level_begin[depth + 1];
-        if (e <= b) break;
-        ++passes;
-        const OpDepth& tab = op_depth(op, depth);
-        ApplyPass ps;
-        ps.depth = depth;
-        ps.root = depth == 0;
-        ps.tab = &tab;
-        if (ps.root) {
-            const double nu0 = tab.deltas.empty() ? 0.0 : tab.deltas.front().maxb;
-            ps.theta = kScreen * prec * fnorm * nu0;
-        } else {
-            ps.theta = kScreen * split_threshold(prec, g0, depth);
-        }
-        int np = 0;
-        while (nu_max > 0.0 && np < (int)tab.deltas.size() && !(tab.deltas[np].maxb * nu_max < ps.theta)) ++np;
-        ps.nprefix = np;
-        for (int d = 0; d < 3; ++d) ps.ext[d] = (long long)m.boxes[d] << depth;
-        run_apply_pass(out, b, e, inp, ps, s);
-        trip += ps.triples;
-        if (ps.root) g0 = std::sqrt(reduce_range_norm2(out, b, e, s));
-        if (!(prec > 0.0) || !(g0 > 0.0)) break;
-        if (tree_refine_last_level(out, split_threshold(prec, g0, depth)) == 0) break;
-    }
-    tree_sumup_top_down(out);
-    tree_compress_bottom_up(out);
-    launch_node_norms(out, 0, out.n, s);
+    tree_reserve(t, t.n + 8 * ns);
+    int* d_list = (int*)dalloc(ctx, sizeof(int) * ns);
+    MWB_CUDA(cudaMemcpyAsync(d_list, list.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
+    launch_make_children(t, d_list, ns, s);
+    launch_hash_insert(t, t.n, t.n + 8 * ns, s);
     MWB_CUDA(cudaStreamSynchronize(s));
-    out.stats[0] = trip;
-    out.stats[1] = 0;
-    out.stats[2] = passes;
-    out.stats[3] = out.n;
+    dfree(ctx, d_list);
+    t.n += 8 * ns;
+    t.level_begin.push_back(t.n);
+}
+
+// Adaptive NS-form apply of a batch: out[i] = op[i] * inp[i], all trees on one world.  The passes
+// run in lock-step over the batch (one launch per stage for all trees of a depth).
+static void apply_batched(double prec, int n, Tree** out, Op** op, Tree** inp) {
+    if (n <= 0) throw Error(MW_ERR_ARG, "empty batch");
+    if (n > 128) throw Error(MW_ERR_ARG, "at most 128 trees per batch");
+    const Mra* m = inp[0]->mra;
+    for (int i = 0; i < n; ++i) {
+        if (!out[i] || !op[i] || !inp[i]) throw Error(MW_ERR_ARG, "null tree or operator");
+        if (out[i]->mra != m || inp[i]->mra != m || op[i]->mra != m)
+            throw Error(MW_ERR_ARG, "trees and operators must share the world");
+        if (inp[i]->n == 0) throw Error(MW_ERR_STATE, "input tree is empty");
+        for (int j = 0; j < n; ++j)
+            if (out[i] == inp[j] || (j != i && out[i] == out[j]))
+                throw Error(MW_ERR_ARG, "output trees must be distinct from each other and from the inputs");
+    }
+    Ctx* ctx = m->ctx;
+    cudaStream_t s = ctx->stream;
+    std::vector<double> fnorm(n), nu_max(n), g0(n, 0.0);
+    long long total_trip = 0;
+    std::vector<int> passes(n, 0);
+    std::vector<bool> active(n, true);
+    for (int i = 0; i < n; ++i) {
+        tree_make_roots(*out[i]);
+        fnorm[i] = std::sqrt(reduce_leaf_norm2(*inp[i], s));
+        nu_max[i] = std::sqrt(reduce_max_norm2(*inp[i], s));
+    }
+    for (int depth = 0;; ++depth) {
+        BatchPass bp;
+        bp.depth = depth;
+        std::vector<int> idx;
+        for (int i = 0; i < n; ++i) {
+            if (!active[i] || out[i]->levels() <= depth) continue;
+            const int b = out[i]->level_begin[depth], e = out[i]->level_begin[depth + 1];
+            if (e <= b) continue;
+            BatchTree bt;
+            bt.out = out[i];
+            bt.inp = inp[i];
+            bt.tab = &op_depth(*op[i], depth);
+            bt.obegin = b;
+            bt.oend = e;
+            bt.prec = prec;
+            bt.g0 = g0[i];
+            if (depth == 0) {
+                const double nu0 = bt.tab->deltas.empty() ? 0.0 : bt.tab->deltas.front().maxb;
+                bt.theta = kScreen * prec * fnorm[i] * nu0;
+            } else {
+                bt.theta = kScreen * split_threshold(prec, g0[i], depth);
+            }
+            int np = 0;
+            while (nu_max[i] > 0.0 && np < (int)bt.tab->deltas.size() && !(bt.tab->deltas[np].maxb * nu_max[i] < bt.theta))
+                ++np;
+            bt.nprefix = np;
+            bp.trees.push_back(bt);
+            idx.push_back(i);
+        }
+        if (bp.trees.empty()) break;
+        run_batch_pass(bp, s);
+        for (size_t q = 0; q < idx.size(); ++q) {
+            const int i = idx[q];
+            ++passes[i];
+            if (depth == 0) g0[i] = bp.trees[q].g0;
+            if (!(prec > 0.0) || !(g0[i] > 0.0) || bp.split_lists[q].empty()) {
+                active[i] = false;
+                continue;
+            }
+            tree_add_children(*out[i], bp.split_lists[q]);
+        }
+        total_trip += bp.triples;
+    }
+    for (int i = 0; i < n; ++i) {
+        tree_sumup_top_down(*out[i]);
+        tree_compress_bottom_up(*out[i]);
+        launch_node_norms(*out[i], 0, out[i]->n, s);
+    }
+    MWB_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < n; ++i) {
+        out[i]->stats[0] = (n == 1) ? total_trip : -1;
+        out[i]->stats[1] = total_trip;
+        out[i]->stats[2] = passes[i];
+        out[i]->stats[3] = out[i]->n;
+    }
 }
 
 }  // namespace mwb
@@ -861,7 +912,27 @@ int mw_apply(double prec, mw_tree out, mw_op op, mw_tree inp, int flags) {
         MW_ARG(out && op && inp, "null pointer");
         MW_ARG(flags == MW_APPLY_FP64, "unknown apply flags");
         MWB_CUDA(cudaSetDevice(inp->mra->ctx->device));
-        apply(prec, *out, *op, *inp);
+        Tree* o = out;
+        Op* p = op;
+        Tree* i = inp;
+        apply_batched(prec, 1, &o, &p, &i);
+    })
+}
+
+int mw_apply_batched(int n, double prec, mw_tree* out, mw_op* ops, mw_tree* inp, int flags) {
+    MW_TRY({
+        MW_ARG(n > 0 && out && ops && inp, "null pointer or empty batch");
+        MW_ARG(flags == MW_APPLY_FP64, "unknown apply flags");
+        MW_ARG(inp[0], "null input tree");
+        MWB_CUDA(cudaSetDevice(inp[0]->mra->ctx->device));
+        std::vector<Tree*> o(n), i(n);
+        std::vector<Op*> p(n);
+        for (int q = 0; q < n; ++q) {
+            o[q] = out[q];
+            p[q] = ops[q];
+            i[q] = inp[q];
+        }
+        apply_batched(prec, n, o.data(), p.data(), i.data());
     })
 }
 

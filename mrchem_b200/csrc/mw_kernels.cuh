@@ -1,6 +1,7 @@
 // mw_kernels.cuh -- launchers of the sm_100a kernels (mw_kernels.cu), called by the host driver.
 #pragma once
 #include <cstdint>
+#include <vector>
 
 #include "mw_internal.hpp"
 
@@ -49,16 +50,24 @@ double reduce_max_norm2(Tree& t, cudaStream_t s);
 void launch_rescale(Tree& t, double c, cudaStream_t s);
 double launch_dot(Tree& a, Tree& b, cudaStream_t s);
 
-// apply pass over output level [obegin, oend) at `depth`
-struct ApplyPass {
-    int depth;
-    bool root;
-    double theta;
-    int nprefix;  // number of leading offset entries considered
-    const OpDepth* tab;
-    long long ext[3];
-    long long triples = 0, triples_gen = 0;
+// one refinement pass of a batched apply (mw_apply.cu)
+struct BatchTree {
+    Tree* out = nullptr;
+    Tree* inp = nullptr;
+    const OpDepth* tab = nullptr;
+    int obegin = 0, oend = 0;  // output nodes of this depth
+    int nprefix = 0;           // leading offset entries that can pass the screening
+    double theta = 0.0;        // screening threshold
+    double prec = 0.0;
+    double g0 = 0.0;           // root-level output norm (set by the root pass)
 };
-void run_apply_pass(Tree& out, int obegin, int oend, Tree& inp, ApplyPass& pass, cudaStream_t s);
+struct BatchPass {
+    int depth = 0;
+    std::vector<BatchTree> trees;
+    long long triples = 0;
+    int nitems = 0, nchunks = 0, nslots = 0;
+    std::vector<std::vector<int>> split_lists;  // per tree: nodes to split (level order)
+};
+void run_batch_pass(BatchPass& bp, cudaStream_t s);
 
 }  // namespace mwb

@@ -67,6 +67,7 @@ SYMBOLS = [
     ("mw_op_nterms", ctypes.c_int, [_vp, _ip]),
     ("mw_op_terms", ctypes.c_int, [_vp, _dp, _dp]),
     ("mw_apply", ctypes.c_int, [ctypes.c_double, _vp, _vp, _vp, ctypes.c_int]),
+    ("mw_apply_batched", ctypes.c_int, [ctypes.c_int, ctypes.c_double, _vpp, _vpp, _vpp, ctypes.c_int]),
     ("mw_apply_stats", ctypes.c_int, [_vp, _lp]),
 ]
 
@@ -309,6 +310,19 @@ class HelmholtzOperator(ConvolutionOperator):
         if not mu > 0.0:
             raise MWError("mu must be positive")
         super().__init__(mra, mu, prec)
+
+
+def apply_batched(prec, outs, ops, inps, flags=APPLY_FP64):
+    """outs[i] = ops[i] * inps[i] for the whole batch in lock-step passes; returns the batch's
+    contracted triple count."""
+    n = len(outs)
+    if not (len(ops) == n and len(inps) == n):
+        raise MWError("batch lists must have equal length")
+    arr = lambda objs: (ctypes.c_void_p * n)(*[o._h.value for o in objs])
+    _check(_lib.mw_apply_batched(n, float(prec), arr(outs), arr(ops), arr(inps), int(flags)))
+    st = np.zeros(4, np.int64)
+    _check(_lib.mw_apply_stats(outs[0]._h, st.ctypes.data_as(_lp)))
+    return int(st[1])
 
 
 def apply(prec, out: FunctionTree, op: ConvolutionOperator, inp: FunctionTree, flags=APPLY_FP64):

@@ -89,6 +89,32 @@ def test_apply_parity(gpu_mod, oracle_mod, order, prec, mu):
     assert abs(G.dot(out, inp) - O.dot(out_o, inp_o)) < 1e-11 * abs(O.dot(out_o, inp_o))
 
 
+def test_batched_apply_equals_single_applies(gpu_mod):
+    """mw_apply_batched over several trees/operators gives exactly the single-apply results."""
+    from mrchem_b200 import workloads as W
+
+    G = gpu_mod
+    prec = 1e-5
+    m = G.MultiResolutionAnalysis(*WORLD, 7, 14)
+    orbs = W.orbitals(5, seed=11)
+    mus = W.helmholtz_mus(5, seed=11)
+    inps, ops = [], []
+    for f, mu in zip(orbs, mus):
+        t = G.FunctionTree(m)
+        G.project(prec, t, f)
+        inps.append(t)
+        ops.append(G.HelmholtzOperator(m, mu, prec))
+    ops[2] = G.PoissonOperator(m, prec)  # mixed operator kinds in one batch
+    outs_b = [G.FunctionTree(m) for _ in inps]
+    total = G.apply_batched(prec, outs_b, ops, inps)
+    singles = 0
+    for i in range(len(inps)):
+        o = G.FunctionTree(m)
+        singles += G.apply(prec, o, ops[i], inps[i])[0]
+        assert_same_tree(outs_b[i].export(), o.export(), tol=0.0)
+    assert total == singles
+
+
 def test_apply_matches_analytic_potential(gpu_mod, oracle_mod):
     """Poisson of a normalised Gaussian is erf(sqrt(a) r)/r (config-1 accuracy level)."""
     G, O = gpu_mod, oracle_mod
