@@ -30,6 +30,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "MW Poisson/Helmholtz apply time at 1e-6 rel. error: mixed+learned vs plain FP64 GPU"
 FP64_PEAK_NOMINAL = 37.0  # TFLOP/s, B200 datasheet FP64 (no measured FP64 peak on this pool)
+FP32_PEAK_NOMINAL = 74.4  # TFLOP/s, 148 SMs x 128 FP32 lanes x 2 x 1.965 GHz
 
 
 def parse():
@@ -201,32 +202,43 @@ def run_gpu(args):
         if world > 1:
             torch.distributed.barrier()
 
-    def step():
-        return G.apply_batched(args.prec, outs, ops, inps)
-
-    for _ in range(args.warmup):
-        step()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    barrier()
-    torch.cuda.synchronize()
-    ctx.profile(True)
-    triples = 0
-    with Clocks(local) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            triples += step()
-        ev1.record(stream)
+    def timed(flags, outs_):
+        """W untimed + K timed steps of the batched apply with the given precision flag."""
+        for _ in range(args.warmup):
+            G.apply_batched(args.prec, outs_, ops, inps, flags)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        barrier()
         torch.cuda.synchronize()
-    barrier()
-    ms = ev0.elapsed_time(ev1)
-    launches, apply_launches, apply_ms = ctx.profile_read()
-    ctx.profile(False)
-    clocks = clk.summary()
-    if world > 1:
-        tt = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        ms = float(tt.item())
+        ctx.profile(True)
+        trip = 0
+        with Clocks(local) as clk:
+            ev0.record(stream)
+            for _ in range(args.steps):
+                trip += G.apply_batched(args.prec, outs_, ops, inps, flags)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        barrier()
+        ms_ = ev0.elapsed_time(ev1)
+        prof = ctx.profile_read()
+        ctx.profile(False)
+        if world > 1:
+            tt = torch.tensor([ms_], device=f"cuda:{local}", dtype=torch.float64)
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+            ms_ = float(tt.item())
+        return ms_, trip, prof, clk.summary()
+
+    # plain FP64 (the reference method on the GPU) and the mixed path (FP32 products, FP64
+    # accumulation), same inputs, same operators
+    ms64, trip64, prof64, _ = timed(G.APPLY_FP64, outs)
+    outs32 = [G.FunctionTree(m) for _ in range(args.orbitals)]
+    ms, triples, prof32, clocks = timed(G.APPLY_FP32, outs32)
+    launches, apply_launches, apply_ms = prof32
+    # error of the mixed result against the FP64 one: ||g32 - g64|| / ||g64|| per orbital
+    rel_err = 0.0
+    for a, b in zip(outs32, outs):
+        na, nb, ab = a.square_norm(), b.square_norm(), G.dot(a, b)
+        rel_err = max(rel_err, np.sqrt(max(na + nb - 2 * ab, 0.0) / nb))
     total_applies = args.orbitals * args.steps * world
     value = total_applies / (ms / 1e3)
 
@@ -245,9 +257,9 @@ def run_gpu(args):
         for i in range(args.orbitals):
             h = host[i]
             e_in[i].load(h["depth"], h["trans"], h["parent"], h["child0"], h["coef"])
-        G.apply_batched(args.prec, outs, ops, e_in)
+        G.apply_batched(args.prec, outs32, ops, e_in, G.APPLY_FP32)
         for i in range(args.orbitals):
-            res = outs[i].export()
+            res = outs32[i].export()
             d2h += sum(v.nbytes for v in res.values() if v is not None)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
@@ -278,18 +290,23 @@ def run_gpu(args):
         line = {
             "metric": METRIC, "value": value, "unit": "applies/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f32 products, f64 accumulation", "data": "synthetic",
             "config": {"workload": "helmholtz_batch_32orb_k10_prec1e-6", "orbitals": args.orbitals,
                        "order": args.order, "k": k, "prec": args.prec, "mu": "U[0.5,3]", "world": "[-20,20]^3",
-                       "path": "plain FP64 NS-form apply (CUDA cores), batched passes", "parallelism": f"replicas x{world}",
+                       "path": "mixed: FP32 products, FP64 accumulation; batched passes", "parallelism": f"replicas x{world}",
                        "l2": f"inputs larger than L2 ({in_bytes / 1e9:.2f} GB of input blocks per step)"},
             "e2e": {"value": e2e_val, "unit": "applies/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "roofline": {"bound": "tensor", "kernel": "k_apply_fp64", "achieved": achieved, "peak": peak,
+            "plain_fp64": {"value": args.orbitals * args.steps * world / (ms64 / 1e3), "unit": "applies/s",
+                           "ms_per_step": ms64 / args.steps, "kernel_ms_per_step": prof64[2] / args.steps,
+                           "triples_per_step": trip64 // max(1, args.steps)},
+            "speedup_vs_plain_fp64": ms64 / ms,
+            "rel_error_vs_fp64": rel_err,
+            "roofline": {"bound": "tensor", "kernel": "k_bapply<10,float>", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if not peaks.get("_fallback")
-                         else "fallback", "fp64_peak_nominal": FP64_PEAK_NOMINAL,
-                         "frac_fp64_nominal": (achieved / FP64_PEAK_NOMINAL) if achieved else None,
+                         else "fallback", "fp32_simt_peak_nominal": FP32_PEAK_NOMINAL,
+                         "frac_fp32_simt_nominal": (achieved / FP32_PEAK_NOMINAL) if achieved else None,
                          "flops_per_triple": flops_per_triple(k), "triples_per_step": triples // max(1, args.steps),
                          "kernel_ms_per_step": apply_ms / args.steps, "kernel_launches": apply_launches},
             "cpu_baseline": cpu,

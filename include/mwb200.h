@@ -31,8 +31,9 @@ typedef struct mw_op_s* mw_op;     /* separated-Gaussian convolution operator, d
 enum { MW_OK = 0, MW_ERR_ARG = -1, MW_ERR_CUDA = -2, MW_ERR_STATE = -3, MW_ERR_CAPACITY = -4 };
 enum { MW_BASIS_INTERPOLATING = 0, MW_BASIS_LEGENDRE = 1 };
 enum { MW_FUNC_GAUSSIANS = 1, MW_FUNC_HYDROGEN_PRODUCTS = 2 };
-/* apply flags */
-enum { MW_APPLY_FP64 = 0 };
+/* apply flags: FP64 products (the plain apply), or FP32 products with every term's contribution
+ * accumulated in FP64 (mixed precision); norms, screening and refinement are FP64 in both */
+enum { MW_APPLY_FP64 = 0, MW_APPLY_FP32 = 1 };
 
 const char* mw_last_error(void);
 int mw_version(int* major, int* minor);

@@ -215,6 +215,7 @@ Op::~Op() {
     cudaSetDevice(c->device);
     for (auto& kv : depths) {
         dfree(c, kv.second->d_mats);
+        dfree(c, kv.second->d_mats32);
         dfree(c, kv.second->d_deltas);
         dfree(c, kv.second->d_terms);
     }
@@ -377,8 +378,12 @@ static const OpDepth& op_depth(Op& op, int depth) {
     od->d_mats = (double*)dalloc(ctx, sizeof(double) * std::max<size_t>(1, od->mats.size()));
     od->d_deltas = (DeltaRec*)dalloc(ctx, sizeof(DeltaRec) * std::max<size_t>(1, od->deltas.size()));
     od->d_terms = (TermRec*)dalloc(ctx, sizeof(TermRec) * std::max<size_t>(1, od->terms.size()));
-    if (!od->mats.empty())
+    od->d_mats32 = (float*)dalloc(ctx, sizeof(float) * std::max<size_t>(1, od->mats.size()));
+    std::vector<float> m32(od->mats.begin(), od->mats.end());
+    if (!od->mats.empty()) {
         MWB_CUDA(cudaMemcpyAsync(od->d_mats, od->mats.data(), sizeof(double) * od->mats.size(), cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(od->d_mats32, m32.data(), sizeof(float) * m32.size(), cudaMemcpyHostToDevice, s));
+    }
     if (!od->deltas.empty())
         MWB_CUDA(cudaMemcpyAsync(od->d_deltas, od->deltas.data(), sizeof(DeltaRec) * od->deltas.size(), cudaMemcpyHostToDevice, s));
     if (!od->terms.empty())
@@ -433,7 +438,7 @@ static void tree_add_children(Tree& t, const std::vector<int>& list) {
 
 // Adaptive NS-form apply of a batch: out[i] = op[i] * inp[i], all trees on one world.  The passes
 // run in lock-step over the batch (one launch per stage for all trees of a depth).
-static void apply_batched(double prec, int n, Tree** out, Op** op, Tree** inp) {
+static void apply_batched(double prec, int n, Tree** out, Op** op, Tree** inp, int precision) {
     if (n <= 0) throw Error(MW_ERR_ARG, "empty batch");
     if (n > 128) throw Error(MW_ERR_ARG, "at most 128 trees per batch");
     const Mra* m = inp[0]->mra;
@@ -460,6 +465,7 @@ static void apply_batched(double prec, int n, Tree** out, Op** op, Tree** inp) {
     for (int depth = 0;; ++depth) {
         BatchPass bp;
         bp.depth = depth;
+        bp.precision = precision;
         std::vector<int> idx;
         for (int i = 0; i < n; ++i) {
             if (!active[i] || out[i]->levels() <= depth) continue;
@@ -910,19 +916,19 @@ int mw_op_terms(mw_op op, double* alpha, double* beta) {
 int mw_apply(double prec, mw_tree out, mw_op op, mw_tree inp, int flags) {
     MW_TRY({
         MW_ARG(out && op && inp, "null pointer");
-        MW_ARG(flags == MW_APPLY_FP64, "unknown apply flags");
+        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32, "unknown apply flags");
         MWB_CUDA(cudaSetDevice(inp->mra->ctx->device));
         Tree* o = out;
         Op* p = op;
         Tree* i = inp;
-        apply_batched(prec, 1, &o, &p, &i);
+        apply_batched(prec, 1, &o, &p, &i, flags);
     })
 }
 
 int mw_apply_batched(int n, double prec, mw_tree* out, mw_op* ops, mw_tree* inp, int flags) {
     MW_TRY({
         MW_ARG(n > 0 && out && ops && inp, "null pointer or empty batch");
-        MW_ARG(flags == MW_APPLY_FP64, "unknown apply flags");
+        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32, "unknown apply flags");
         MW_ARG(inp[0], "null input tree");
         MWB_CUDA(cudaSetDevice(inp[0]->mra->ctx->device));
         std::vector<Tree*> o(n), i(n);
@@ -932,7 +938,7 @@ int mw_apply_batched(int n, double prec, mw_tree* out, mw_op* ops, mw_tree* inp,
             p[q] = ops[q];
             i[q] = inp[q];
         }
-        apply_batched(prec, n, o.data(), p.data(), i.data());
+        apply_batched(prec, n, o.data(), p.data(), i.data(), flags);
     })
 }
 

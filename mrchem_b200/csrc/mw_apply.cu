@@ -34,6 +34,7 @@ struct BTree {
     const DeltaRec* deltas;
     const TermRec* terms;
     const double* mats;
+    const float* mats32;
     int nprefix;
     int root;
     double theta;
@@ -273,171 +274,211 @@ __global__ void k_multi_slots(const int* __restrict__ nchunk, int nitems, int* n
 }
 
 // ---------------------------------------------------------------------------------------------
-// 5. FP64 contraction (one CTA per chunk)
+// 5. contraction (one CTA per chunk), templated on the product type R:
+//    R = double: the plain FP64 apply; R = float: FP32 products with FP64 accumulation of every
+//    term's contribution (the mixed path).  Per term, three in-place pencil transforms:
+//      out += beta (NS_z (x) NS_y (x) NS_x) in       out_sss -= beta (T_z (x) T_y (x) T_x) in_sss
+//    (the second only at depth > 0: the s->s block belongs to coarser scales).
+//    Each thread owns two pencils per step, so every operator element read from shared memory (as a
+//    16-byte vector) feeds two FMA chains; the per-term matrices are double-buffered.
 // ---------------------------------------------------------------------------------------------
-template <int K>
-struct ApplyCfg {
+template <typename R> struct VecT;
+template <> struct VecT<double> { using T = double2; static constexpr int V = 2; };
+template <> struct VecT<float> { using T = float4; static constexpr int V = 4; };
+
+template <int K, typename R>
+struct ACfg {
     static constexpr int K2 = 2 * K;
     static constexpr int NP = K2 * K2;
-    static constexpr bool STAGE = K2 <= 20;       // input block staged in shared memory
-    static constexpr int PPT = K2 <= 20 ? 1 : 2;   // z-pencils (accumulators) per thread
-    static constexpr int NT = ((NP + PPT - 1) / PPT + 31) / 32 * 32;
-    static constexpr int XS = STAGE ? Geo<K>::VOL : K * K * K;
-    static constexpr size_t SMEM = sizeof(double) * (size_t)(XS + Geo<K>::VOL + 3 * NP + K * K * K + 64);
+    static constexpr int LDM = (K2 + 3) / 4 * 4;          // padded operator row (16-byte vectors)
+    static constexpr int MS = K2 * LDM;                     // one operator matrix
+    static constexpr int P = K2 + 1;
+    static constexpr int VOL = P * K2 * K2;                 // padded (2k)^3 tensor
+    static constexpr bool STAGE = sizeof(R) * 2 * (size_t)VOL + sizeof(R) * 6 * MS <= 200 * 1024;
+    static constexpr int XS = STAGE ? VOL : K * K * K;
+    static constexpr int US = K * K * K;
+    static constexpr int NT = ((NP / 2) + 31) / 32 * 32;    // two z-pencils per thread
+    static constexpr size_t SMEM = sizeof(R) * (size_t)(XS + VOL + 6 * MS + US) + 64 * sizeof(double) + 64;
+    __device__ static inline int at(int a, int b, int c) { return a + P * (b + K2 * c); }
 };
 
-template <int K, bool GEN>
-__device__ __forceinline__ double xin(const double* X, const double* __restrict__ blk, int a, int b, int c) {
-    using C = ApplyCfg<K>;
-    if (C::STAGE) return X[Geo<K>::at(a, b, c)];
-    if (GEN) return X[a + K * (b + K * c)];
-    return __ldg(&blk[a + 2 * K * (b + 2 * K * c)]);
-}
+// round n up to the vector width
+template <typename R> __host__ __device__ constexpr int vround(int n) { return (n + VecT<R>::V - 1) / VecT<R>::V * VecT<R>::V; }
 
-// x-step: T[:, b, c] = M_x X[:, b, c] (GEN: k scaling inputs, b, c < k), and for depth > 0 the
-// scaling-only chain U = T_x X_sss
-template <int K, bool GEN>
-__device__ __forceinline__ void step_x(const double* __restrict__ Mx, const double* X, const double* __restrict__ blk,
-                                       double* T, double* U, bool root) {
-    using G = Geo<K>;
-    constexpr int K2 = G::K2;
-    constexpr int NIN = GEN ? K : K2;
-    constexpr int UX = GEN ? K : K2;
-    for (int p = threadIdx.x; p < UX * UX; p += blockDim.x) {
-        const int b = p % UX, c = p / UX;
-        double x[NIN];
+// out0[o] = sum_i M[o][i] x0[i], out1[o] = sum_i M[o][i] x1[i] for o < NOUT, i < NIN (x padded with
+// zeros up to a multiple of the vector width)
+template <typename R, int NIN, int LDM>
+__device__ __forceinline__ void dot2(const R* __restrict__ Mrow, const R (&x0)[vround<R>(NIN)],
+                                     const R (&x1)[vround<R>(NIN)], R& s0, R& s1) {
+    using V = VecT<R>;
+    s0 = R(0);
+    s1 = R(0);
 #pragma unroll
-        for (int i = 0; i < NIN; ++i) x[i] = xin<K, GEN>(X, blk, i, b, c);
-#pragma unroll 2
-        for (int o = 0; o < K2; ++o) {
-            double s = 0.0;
-#pragma unroll
-            for (int i = 0; i < NIN; ++i) s = fma(Mx[o * K2 + i], x[i], s);
-            T[G::at(o, b, c)] = s;
+    for (int i = 0; i < vround<R>(NIN); i += V::V) {
+        const typename V::T m = *reinterpret_cast<const typename V::T*>(Mrow + i);
+        if constexpr (V::V == 2) {
+            s0 = fma(m.x, x0[i], s0); s1 = fma(m.x, x1[i], s1);
+            s0 = fma(m.y, x0[i + 1], s0); s1 = fma(m.y, x1[i + 1], s1);
+        } else {
+            s0 = fmaf(m.x, x0[i], s0); s1 = fmaf(m.x, x1[i], s1);
+            s0 = fmaf(m.y, x0[i + 1], s0); s1 = fmaf(m.y, x1[i + 1], s1);
+            s0 = fmaf(m.z, x0[i + 2], s0); s1 = fmaf(m.z, x1[i + 2], s1);
+            s0 = fmaf(m.w, x0[i + 3], s0); s1 = fmaf(m.w, x1[i + 3], s1);
         }
     }
-    if (!root) {
-        for (int p = threadIdx.x; p < K * K; p += blockDim.x) {
-            const int b = p % K, c = p / K;
-            double x[K];
+}
+
+// generic pencil step over a padded shared tensor: for the pencils q of the step (two per
+// thread iteration), y[o] = sum_i M[o][i] x[i], i < NIN, o < NOUT, in place (pencils are owned).
+// base(q) / stride describe where a pencil lives.
+template <int K, typename R, int NIN, int NOUT, int NPEN, typename BaseF>
+__device__ __forceinline__ void pencil_step(const R* __restrict__ M, R* A, int stride, BaseF base) {
+    using C = ACfg<K, R>;
+    constexpr int NV = vround<R>(NIN);
+    for (int q = 2 * threadIdx.x; q < NPEN; q += 2 * blockDim.x) {
+        const bool two = q + 1 < NPEN;
+        const int b0 = base(q), b1 = two ? base(q + 1) : b0;
+        R x0[NV], x1[NV];
 #pragma unroll
-            for (int i = 0; i < K; ++i) x[i] = xin<K, GEN>(X, blk, i, b, c);
+        for (int i = 0; i < NV; ++i) {
+            x0[i] = i < NIN ? A[b0 + i * stride] : R(0);
+            x1[i] = i < NIN ? A[b1 + i * stride] : R(0);
+        }
 #pragma unroll 2
-            for (int o = 0; o < K; ++o) {
-                double s = 0.0;
+        for (int o = 0; o < NOUT; ++o) {
+            R s0, s1;
+            dot2<R, NIN, C::LDM>(M + o * C::LDM, x0, x1, s0, s1);
+            A[b0 + o * stride] = s0;
+            if (two) A[b1 + o * stride] = s1;
+        }
+    }
+}
+
+template <int K, typename R, bool GEN>
+__device__ __forceinline__ void chain_xy(const R* Mx, const R* My, R* X, R* T, R* U, bool root, const double* blk,
+                                         bool xfrom_global) {
+    using C = ACfg<K, R>;
+    constexpr int K2 = C::K2;
+    constexpr int NIN = GEN ? K : K2;
+    (void)blk;
+    (void)xfrom_global;
+    // x: T[:, b, c] = Mx X[:, b, c]   (pencils (b, c); GEN: b, c < k, inputs a < k)
+    {
+        constexpr int UX = GEN ? K : K2;
+        constexpr int NV = vround<R>(NIN);
+        for (int q = 2 * threadIdx.x; q < UX * UX; q += 2 * blockDim.x) {
+            const bool two = q + 1 < UX * UX;
+            const int bq0 = q % UX, cq0 = q / UX, bq1 = (q + 1) % UX, cq1 = (q + 1) / UX;
+            R x0[NV], x1[NV];
 #pragma unroll
-                for (int i = 0; i < K; ++i) s = fma(Mx[o * K2 + i], x[i], s);
-                U[o + K * (b + K * c)] = s;
+            for (int i = 0; i < NV; ++i) {
+                if (i < NIN) {
+                    if (C::STAGE) {
+                        x0[i] = X[C::at(i, bq0, cq0)];
+                        x1[i] = two ? X[C::at(i, bq1, cq1)] : R(0);
+                    } else if (GEN) {
+                        x0[i] = X[i + K * (bq0 + K * cq0)];
+                        x1[i] = two ? X[i + K * (bq1 + K * cq1)] : R(0);
+                    } else {
+                        x0[i] = (R)__ldg(&blk[i + K2 * (bq0 + K2 * cq0)]);
+                        x1[i] = two ? (R)__ldg(&blk[i + K2 * (bq1 + K2 * cq1)]) : R(0);
+                    }
+                } else {
+                    x0[i] = R(0);
+                    x1[i] = R(0);
+                }
             }
-        }
-    }
-}
-
-template <int K, bool GEN>
-__device__ __forceinline__ void step_y(const double* __restrict__ My, double* T, double* U, bool root) {
-    using G = Geo<K>;
-    constexpr int K2 = G::K2;
-    constexpr int NIN = GEN ? K : K2;
-    constexpr int NC = GEN ? K : K2;
-    for (int p = threadIdx.x; p < K2 * NC; p += blockDim.x) {
-        const int a = p % K2, c = p / K2;
-        double x[NIN];
-#pragma unroll
-        for (int i = 0; i < NIN; ++i) x[i] = T[G::at(a, i, c)];
 #pragma unroll 2
-        for (int o = 0; o < K2; ++o) {
-            double s = 0.0;
-#pragma unroll
-            for (int i = 0; i < NIN; ++i) s = fma(My[o * K2 + i], x[i], s);
-            T[G::at(a, o, c)] = s;
-        }
-    }
-    if (!root) {
-        for (int p = threadIdx.x; p < K * K; p += blockDim.x) {
-            const int a = p % K, c = p / K;
-            double x[K];
-#pragma unroll
-            for (int i = 0; i < K; ++i) x[i] = U[a + K * (i + K * c)];
-#pragma unroll 2
-            for (int o = 0; o < K; ++o) {
-                double s = 0.0;
-#pragma unroll
-                for (int i = 0; i < K; ++i) s = fma(My[o * K2 + i], x[i], s);
-                U[a + K * (o + K * c)] = s;
-            }
-        }
-    }
-}
-
-template <int K, bool GEN>
-__device__ __forceinline__ void step_z(const double* __restrict__ Mz, const double* T, const double* U, bool root,
-                                       double beta, double (&acc)[ApplyCfg<K>::PPT][2 * K]) {
-    using G = Geo<K>;
-    using C = ApplyCfg<K>;
-    constexpr int K2 = G::K2;
-    constexpr int NIN = GEN ? K : K2;
-#pragma unroll
-    for (int j = 0; j < C::PPT; ++j) {
-        const int p = threadIdx.x + j * C::NT;
-        if (p < C::NP) {
-            const int a = p % K2, b = p / K2;
-            double x[NIN];
-#pragma unroll
-            for (int i = 0; i < NIN; ++i) x[i] = T[G::at(a, b, i)];
-#pragma unroll
             for (int o = 0; o < K2; ++o) {
-                double s = 0.0;
-#pragma unroll
-                for (int i = 0; i < NIN; ++i) s = fma(Mz[o * K2 + i], x[i], s);
-                acc[j][o] = fma(beta, s, acc[j][o]);
+                R s0, s1;
+                dot2<R, NIN, C::LDM>(Mx + o * C::LDM, x0, x1, s0, s1);
+                T[C::at(o, bq0, cq0)] = s0;
+                if (two) T[C::at(o, bq1, cq1)] = s1;
             }
-            if (!root && a < K && b < K) {
-                double u[K];
+        }
+        if (!root) {
+            constexpr int KV = vround<R>(K);
+            for (int q = 2 * threadIdx.x; q < K * K; q += 2 * blockDim.x) {
+                const bool two = q + 1 < K * K;
+                const int bq0 = q % K, cq0 = q / K, bq1 = (q + 1) % K, cq1 = (q + 1) / K;
+                R x0[KV], x1[KV];
 #pragma unroll
-                for (int i = 0; i < K; ++i) u[i] = U[a + K * (b + K * i)];
-#pragma unroll
+                for (int i = 0; i < KV; ++i) {
+                    if (i < K) {
+                        if (C::STAGE) {
+                            x0[i] = X[C::at(i, bq0, cq0)];
+                            x1[i] = two ? X[C::at(i, bq1, cq1)] : R(0);
+                        } else if (GEN) {
+                            x0[i] = X[i + K * (bq0 + K * cq0)];
+                            x1[i] = two ? X[i + K * (bq1 + K * cq1)] : R(0);
+                        } else {
+                            x0[i] = (R)__ldg(&blk[i + K2 * (bq0 + K2 * cq0)]);
+                            x1[i] = two ? (R)__ldg(&blk[i + K2 * (bq1 + K2 * cq1)]) : R(0);
+                        }
+                    } else {
+                        x0[i] = R(0);
+                        x1[i] = R(0);
+                    }
+                }
+#pragma unroll 2
                 for (int o = 0; o < K; ++o) {
-                    double s = 0.0;
-#pragma unroll
-                    for (int i = 0; i < K; ++i) s = fma(Mz[o * K2 + i], u[i], s);
-                    acc[j][o] = fma(-beta, s, acc[j][o]);
+                    R s0, s1;
+                    dot2<R, K, C::LDM>(Mx + o * C::LDM, x0, x1, s0, s1);
+                    U[o + K * (bq0 + K * cq0)] = s0;
+                    if (two) U[o + K * (bq1 + K * cq1)] = s1;
                 }
             }
         }
     }
+    __syncthreads();
+    // y (in place): pencils (a, c), GEN: planes c < k, inputs b < k
+    {
+        constexpr int NC = GEN ? K : K2;
+        pencil_step<K, R, NIN, K2, K2 * NC>(My, T, C::P, [](int q) { return ACfg<K, R>::at(q % (2 * K), 0, q / (2 * K)); });
+        if (!root)
+            pencil_step<K, R, K, K, K * K>(My, U, K, [](int q) { return (q % K) + K * K * (q / K); });
+    }
 }
 
-// For every term of every candidate of the chunk:
-//   out += beta (NS_z (x) NS_y (x) NS_x) in        (three in-place pencil transforms)
-//   out_sss -= beta (T_z (x) T_y (x) T_x) in_sss   (depth > 0: the s->s block belongs to coarser scales)
-template <int K>
-__global__ void __launch_bounds__(ApplyCfg<K>::NT, 1)
-    k_bapply_fp64(const Chunk* __restrict__ chunks, const Item* __restrict__ items, const BTree* __restrict__ trees,
-                  const int* __restrict__ cdelta, const int* __restrict__ csrc, const double* __restrict__ gblk,
-                  const double* __restrict__ gnorm2, double* partials, unsigned long long* ntrip_out) {
-    using G = Geo<K>;
-    using C = ApplyCfg<K>;
-    constexpr int K2 = G::K2;
-    extern __shared__ double sm[];
-    double* X = sm;
-    double* T = X + C::XS;
-    double* Mx = T + G::VOL;
-    double* My = Mx + C::NP;
-    double* Mz = My + C::NP;
-    double* U = Mz + C::NP;
-    double* red = U + K * K * K;
+template <int K, typename R>
+__global__ void __launch_bounds__(ACfg<K, R>::NT, 1)
+    k_bapply(const Chunk* __restrict__ chunks, const Item* __restrict__ items, const BTree* __restrict__ trees,
+             const int* __restrict__ cdelta, const int* __restrict__ csrc, const double* __restrict__ gblk,
+             const double* __restrict__ gnorm2, double* partials, unsigned long long* ntrip_out) {
+    using C = ACfg<K, R>;
+    constexpr int K2 = C::K2;
+    constexpr int BS = K2 * K2 * K2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    R* X = reinterpret_cast<R*>(smraw);
+    R* T = X + C::XS;
+    R* Mb = T + C::VOL;  // [2][3][MS]
+    R* U = Mb + 6 * C::MS;
+    double* red = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(U + C::US) + 15) & ~uintptr_t(15));
     const Chunk ch = chunks[blockIdx.x];
     const Item it = items[ch.item];
     const BTree& TR = trees[it.tree];
+    const R* mats = reinterpret_cast<const R*>(sizeof(R) == 8 ? (const void*)TR.mats : (const void*)TR.mats32);
     const bool root = TR.root != 0;
     const double theta = TR.theta;
     const int tid = threadIdx.x;
-    double acc[C::PPT][K2];
+    double acc[2][K2];
 #pragma unroll
-    for (int j = 0; j < C::PPT; ++j)
+    for (int j = 0; j < 2; ++j)
 #pragma unroll
         for (int c = 0; c < K2; ++c) acc[j][c] = 0.0;
+    // the thread's two z-pencils (a, b)
+    const int pz0 = 2 * tid, pz1 = 2 * tid + 1;
+    const bool own0 = pz0 < C::NP, own1 = pz1 < C::NP;
+    const int za0 = pz0 % K2, zb0 = pz0 / K2, za1 = pz1 % K2, zb1 = pz1 / K2;
     unsigned long long ntrip = 0;
+    auto load_mats = [&](int buf, const TermRec& tr) {
+        R* dst = Mb + buf * 3 * C::MS;
+        for (int i = tid; i < 3 * C::MS; i += blockDim.x) {
+            const int w = i / C::MS, r = (i % C::MS) / C::LDM, cc = (i % C::MS) % C::LDM;
+            const int mi = w == 0 ? tr.mx : (w == 1 ? tr.my : tr.mz);
+            dst[i] = cc < K2 ? mats[(size_t)mi * C::NP + r * K2 + cc] : R(0);
+        }
+    };
     for (int ci = ch.c0; ci < ch.c1; ++ci) {
         const int src = csrc[ci];
         const bool gen = src < 0;
@@ -445,44 +486,82 @@ __global__ void __launch_bounds__(ApplyCfg<K>::NT, 1)
         const DeltaRec de = TR.deltas[cdelta[ci]];
         if (!(nu > 0.0) || de.maxb * nu < theta) continue;
         if (TR.terms[de.t0].bound * nu < theta) continue;
-        const double* blk = gen ? gblk + (size_t)(-src - 1) * K * K * K : TR.in.coef + (size_t)src * G::BS;
+        const double* blk = gen ? gblk + (size_t)(-src - 1) * K * K * K : TR.in.coef + (size_t)src * BS;
         __syncthreads();  // previous candidate's users of X/T/U/M are done
         if (gen) {
             for (int e2 = tid; e2 < K * K * K; e2 += blockDim.x) {
                 const int a = e2 % K, b = (e2 / K) % K, c = e2 / (K * K);
-                if (C::STAGE) X[G::at(a, b, c)] = blk[e2]; else X[e2] = blk[e2];
+                if (C::STAGE) X[C::at(a, b, c)] = (R)blk[e2]; else X[e2] = (R)blk[e2];
             }
         } else if (C::STAGE) {
-            for (int e2 = tid; e2 < G::BS; e2 += blockDim.x) {
+            for (int e2 = tid; e2 < BS; e2 += blockDim.x) {
                 const int a = e2 % K2, b = (e2 / K2) % K2, c = e2 / (K2 * K2);
-                X[G::at(a, b, c)] = blk[e2];
+                X[C::at(a, b, c)] = (R)blk[e2];
             }
         }
+        load_mats(0, TR.terms[de.t0]);
+        int buf = 0;
         for (int ti = de.t0; ti < de.t1; ++ti) {
             const TermRec tr = TR.terms[ti];
             if (tr.bound * nu < theta) break;
+            const R* Mx = Mb + buf * 3 * C::MS;
+            const R* My = Mx + C::MS;
+            const R* Mz = My + C::MS;
+            __syncthreads();  // X, this term's matrices and the previous z-step are complete
+            if (gen) chain_xy<K, R, true>(Mx, My, X, T, U, root, blk, !C::STAGE);
+            else chain_xy<K, R, false>(Mx, My, X, T, U, root, blk, !C::STAGE);
             __syncthreads();
-            for (int i = tid; i < C::NP; i += blockDim.x) {
-                Mx[i] = TR.mats[(size_t)tr.mx * C::NP + i];
-                My[i] = TR.mats[(size_t)tr.my * C::NP + i];
-                Mz[i] = TR.mats[(size_t)tr.mz * C::NP + i];
+            // prefetch the next term's matrices into the other buffer while doing z
+            if (ti + 1 < de.t1 && !(TR.terms[ti + 1].bound * nu < theta)) load_mats(buf ^ 1, TR.terms[ti + 1]);
+            // z: acc[(a, b)][c'] += beta sum_c Mz[c'][c] T[a, b, c]
+            {
+                constexpr int NIN = K2;
+                const int nin = gen ? K : K2;
+                constexpr int NV = vround<R>(NIN);
+                R x0[NV], x1[NV];
+#pragma unroll
+                for (int i = 0; i < NV; ++i) {
+                    x0[i] = (own0 && i < nin) ? T[C::at(za0, zb0, i)] : R(0);
+                    x1[i] = (own1 && i < nin) ? T[C::at(za1, zb1, i)] : R(0);
+                }
+#pragma unroll
+                for (int o = 0; o < K2; ++o) {
+                    R s0, s1;
+                    dot2<R, NIN, C::LDM>(Mz + o * C::LDM, x0, x1, s0, s1);
+                    acc[0][o] = fma(tr.beta, (double)s0, acc[0][o]);
+                    acc[1][o] = fma(tr.beta, (double)s1, acc[1][o]);
+                }
+                if (!root) {
+                    constexpr int KV = vround<R>(K);
+                    const bool u0 = own0 && za0 < K && zb0 < K, u1 = own1 && za1 < K && zb1 < K;
+                    if (u0 || u1) {
+                        R y0[KV], y1[KV];
+#pragma unroll
+                        for (int i = 0; i < KV; ++i) {
+                            y0[i] = (u0 && i < K) ? U[za0 + K * (zb0 + K * i)] : R(0);
+                            y1[i] = (u1 && i < K) ? U[za1 + K * (zb1 + K * i)] : R(0);
+                        }
+#pragma unroll
+                        for (int o = 0; o < K; ++o) {
+                            R s0, s1;
+                            dot2<R, K, C::LDM>(Mz + o * C::LDM, y0, y1, s0, s1);
+                            if (u0) acc[0][o] = fma(-tr.beta, (double)s0, acc[0][o]);
+                            if (u1) acc[1][o] = fma(-tr.beta, (double)s1, acc[1][o]);
+                        }
+                    }
+                }
             }
-            __syncthreads();
-            if (gen) step_x<K, true>(Mx, X, blk, T, U, root); else step_x<K, false>(Mx, X, blk, T, U, root);
-            __syncthreads();
-            if (gen) step_y<K, true>(My, T, U, root); else step_y<K, false>(My, T, U, root);
-            __syncthreads();
-            if (gen) step_z<K, true>(Mz, T, U, root, tr.beta, acc); else step_z<K, false>(Mz, T, U, root, tr.beta, acc);
+            buf ^= 1;
             ++ntrip;
         }
     }
-    double* dst = ch.slot < 0 ? TR.ocoef + (size_t)it.node * G::BS : partials + (size_t)ch.slot * G::BS;
+    double* dst = ch.slot < 0 ? TR.ocoef + (size_t)it.node * BS : partials + (size_t)ch.slot * BS;
     double n2 = 0.0, w2 = 0.0;
 #pragma unroll
-    for (int j = 0; j < C::PPT; ++j) {
-        const int p = tid + j * C::NT;
-        if (p < C::NP) {
-            const int a = p % K2, b = p / K2;
+    for (int j = 0; j < 2; ++j) {
+        const bool own = j == 0 ? own0 : own1;
+        const int a = j == 0 ? za0 : za1, b = j == 0 ? zb0 : zb1;
+        if (own) {
 #pragma unroll
             for (int c = 0; c < K2; ++c) {
                 const double v = acc[j][c];
@@ -634,6 +713,7 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         d.deltas = b.tab->d_deltas;
         d.terms = b.tab->d_terms;
         d.mats = b.tab->d_mats;
+        d.mats32 = b.tab->d_mats32;
         d.nprefix = b.nprefix;
         d.root = bp.depth == 0;
         d.theta = b.theta;
@@ -749,12 +829,21 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     unsigned long long* d_ntrip_tot = (unsigned long long*)dalloc(ctx, sizeof(unsigned long long));
     MWB_CUDA(cudaMemsetAsync(d_ntrip_tot, 0, sizeof(unsigned long long), s));
     if (ctx->prof) MWB_CUDA(cudaEventRecord(ctx->ev0, s));
-#define L_AP(KK)                                                                                            \
-    {                                                                                                       \
-        size_t smem = ApplyCfg<KK>::SMEM;                                                                   \
-        MWB_CUDA(cudaFuncSetAttribute(k_bapply_fp64<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-        k_bapply_fp64<KK><<<nchunks, ApplyCfg<KK>::NT, smem, s>>>(d_chunks, d_items, d_trees, d_cdelta, d_csrc,  \
-                                                                   d_gblk, d_gnorm2, d_partials, d_ntrip_tot);  \
+#define L_AP(KK)                                                                                             \
+    {                                                                                                        \
+        if (bp.precision == 1) {                                                                             \
+            size_t smem = ACfg<KK, float>::SMEM;                                                             \
+            MWB_CUDA(cudaFuncSetAttribute(k_bapply<KK, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+            k_bapply<KK, float><<<nchunks, ACfg<KK, float>::NT, smem, s>>>(d_chunks, d_items, d_trees, d_cdelta,  \
+                                                                            d_csrc, d_gblk, d_gnorm2, d_partials, \
+                                                                            d_ntrip_tot);                         \
+        } else {                                                                                             \
+            size_t smem = ACfg<KK, double>::SMEM;                                                            \
+            MWB_CUDA(cudaFuncSetAttribute(k_bapply<KK, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+            k_bapply<KK, double><<<nchunks, ACfg<KK, double>::NT, smem, s>>>(d_chunks, d_items, d_trees, d_cdelta, \
+                                                                              d_csrc, d_gblk, d_gnorm2, d_partials, \
+                                                                              d_ntrip_tot);                        \
+        }                                                                                                    \
     }
     MWB_DISPATCH_K(K, L_AP)
 #undef L_AP

@@ -80,6 +80,7 @@ struct OpDepth {
     std::vector<DeltaRec> deltas;      // sorted by maxb, descending
     std::vector<TermRec> terms;
     double* d_mats = nullptr;
+    float* d_mats32 = nullptr;  // FP32 copy of d_mats (mixed-precision apply)
     DeltaRec* d_deltas = nullptr;
     TermRec* d_terms = nullptr;
 };

@@ -63,6 +63,7 @@ struct BatchTree {
 };
 struct BatchPass {
     int depth = 0;
+    int precision = 0;  // 0: FP64 products, 1: FP32 products with FP64 accumulation
     std::vector<BatchTree> trees;
     long long triples = 0;
     int nitems = 0, nchunks = 0, nslots = 0;

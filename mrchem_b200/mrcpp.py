@@ -36,6 +36,7 @@ BASIS_LEGENDRE = 1
 FUNC_GAUSSIANS = 1
 FUNC_HYDROGEN_PRODUCTS = 2
 APPLY_FP64 = 0
+APPLY_FP32 = 1
 
 # every symbol include/mwb200.h declares: (name, restype, argtypes)
 SYMBOLS = [

@@ -897,6 +897,8 @@ struct ApplyStats {
     long long triples_gen = 0;   // of which with a generated (scaling-only) input node
     int passes = 0;
     double g0 = 0.0;
+    long long lines_yz = 0;      // distinct (output node, term, dy, dz) among the triples
+    long long lines_z = 0;       // distinct (output node, term, dz)
 };
 
 // s-only block of the generated input node (depth, t) below the leaf `leaf` (k^3 values)
@@ -953,7 +955,7 @@ void apply(double prec, Tree& out, Operator& op, const Tree& inp, ApplyStats* st
     std::vector<int> work(out.nodes.size());
     for (size_t i = 0; i < work.size(); ++i) work[i] = (int)i;
     double g0 = 0.0;
-    long long n_trip = 0, n_gen = 0;
+    long long n_trip = 0, n_gen = 0, n_lyz = 0, n_lz = 0;
     int passes = 0;
     for (int depth = 0; !work.empty(); ++depth) {
         ++passes;
@@ -1025,12 +1027,13 @@ void apply(double prec, Tree& out, Operator& op, const Tree& inp, ApplyStats* st
                 if (c.src < 0) c.src = -(genid[genreq[q][gi++].first] + 1);
         }
         // Phase B: contractions
-        std::vector<long long> trip(work.size(), 0), tripg(work.size(), 0);
+        std::vector<long long> trip(work.size(), 0), tripg(work.size(), 0), lyz(work.size(), 0), lz(work.size(), 0);
 #pragma omp parallel for schedule(dynamic, 1)
         for (size_t q = 0; q < work.size(); ++q) {
             Node& o = out.nodes[work[q]];
             std::vector<double> acc(BS, 0.0), t1(BS), t2(BS), t3(BS);
             std::vector<double> s_in(SS), u1(SS), u2(SS), u3(SS);
+            std::vector<std::array<int, 3>> seen_yz, seen_z;
             for (const Cand& c : cands[q]) {
                 const DeltaEntry& de = dl[c.delta];
                 const bool gen = c.src < 0;
@@ -1073,13 +1076,21 @@ void apply(double prec, Tree& out, Operator& op, const Tree& inp, ApplyStats* st
                     }
                     ++trip[q];
                     if (gen) ++tripg[q];
+                    seen_yz.push_back({m, de.d[1], de.d[2]});
+                    seen_z.push_back({m, 0, de.d[2]});
                 }
             }
             o.c = acc;
+            std::sort(seen_yz.begin(), seen_yz.end());
+            std::sort(seen_z.begin(), seen_z.end());
+            lyz[q] = std::unique(seen_yz.begin(), seen_yz.end()) - seen_yz.begin();
+            lz[q] = std::unique(seen_z.begin(), seen_z.end()) - seen_z.begin();
         }
         for (size_t q = 0; q < work.size(); ++q) {
             n_trip += trip[q];
             n_gen += tripg[q];
+            n_lyz += lyz[q];
+            n_lz += lz[q];
         }
         if (root) {
             double s = 0.0;
@@ -1123,6 +1134,8 @@ void apply(double prec, Tree& out, Operator& op, const Tree& inp, ApplyStats* st
         stats->triples_gen = n_gen;
         stats->passes = passes;
         stats->g0 = g0;
+        stats->lines_yz = n_lyz;
+        stats->lines_z = n_lz;
     }
 }
 
@@ -1342,6 +1355,8 @@ int oracle_apply(double prec, void* out, void* op, void* inp, long long* stats) 
         stats[0] = st.triples;
         stats[1] = st.triples_gen;
         stats[2] = st.passes;
+        stats[3] = st.lines_yz;
+        stats[4] = st.lines_z;
     }
     return (int)((Tree*)out)->nodes.size();
 }

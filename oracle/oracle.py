@@ -223,6 +223,13 @@ class HelmholtzOperator(ConvolutionOperator):
 
 def apply(prec, out: FunctionTree, op: ConvolutionOperator, inp: FunctionTree):
     """Adaptive NS-form apply; returns (triples, triples_with_generated_input, passes)."""
-    st = np.zeros(4, np.int64)
+    st = np.zeros(8, np.int64)
     lib().oracle_apply(float(prec), out._h, op._h, inp._h, st.ctypes.data_as(_lp))
     return int(st[0]), int(st[1]), int(st[2])
+
+
+def apply_line_stats(prec, out, op, inp):
+    """(triples, distinct (node, term, dy, dz) lines, distinct (node, term, dz) planes) of an apply."""
+    st = np.zeros(8, np.int64)
+    lib().oracle_apply(float(prec), out._h, op._h, inp._h, st.ctypes.data_as(_lp))
+    return int(st[0]), int(st[3]), int(st[4])

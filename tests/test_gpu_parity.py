@@ -115,6 +115,24 @@ def test_batched_apply_equals_single_applies(gpu_mod):
     assert total == singles
 
 
+@pytest.mark.parametrize("order,prec,mu", [(7, 1e-5, 0.0), (9, 1e-6, 1.1)])
+def test_mixed_precision_apply_error(gpu_mod, order, prec, mu):
+    """FP32 products with FP64 accumulation: relative L2 error vs the FP64 apply stays below
+    prec / 10 (1e-7 at prec 1e-6); tree structure is the FP64 one up to borderline nodes."""
+    G = gpu_mod
+    m = G.MultiResolutionAnalysis(*WORLD, order, 14)
+    inp = G.FunctionTree(m)
+    G.project(prec, inp, two_gaussians(G))
+    op = G.ConvolutionOperator(m, mu, prec)
+    o64, o32 = G.FunctionTree(m), G.FunctionTree(m)
+    G.apply(prec, o64, op, inp, G.APPLY_FP64)
+    G.apply(prec, o32, op, inp, G.APPLY_FP32)
+    a, b = o32.square_norm(), o64.square_norm()
+    err = np.sqrt(max(a + b - 2 * G.dot(o32, o64), 0.0) / b)
+    assert err < 0.1 * prec, err
+    assert abs(o32.nnodes() - o64.nnodes()) <= 0.02 * o64.nnodes()
+
+
 def test_apply_matches_analytic_potential(gpu_mod, oracle_mod):
     """Poisson of a normalised Gaussian is erf(sqrt(a) r)/r (config-1 accuracy level)."""
     G, O = gpu_mod, oracle_mod
