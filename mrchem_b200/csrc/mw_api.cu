@@ -216,6 +216,8 @@ Op::~Op() {
     for (auto& kv : depths) {
         dfree(c, kv.second->d_mats);
         dfree(c, kv.second->d_mats32);
+        dfree(c, kv.second->d_matsb);
+        dfree(c, kv.second->d_matsb32);
         dfree(c, kv.second->d_deltas);
         dfree(c, kv.second->d_terms);
     }
@@ -379,10 +381,21 @@ static const OpDepth& op_depth(Op& op, int depth) {
     od->d_deltas = (DeltaRec*)dalloc(ctx, sizeof(DeltaRec) * std::max<size_t>(1, od->deltas.size()));
     od->d_terms = (TermRec*)dalloc(ctx, sizeof(TermRec) * std::max<size_t>(1, od->terms.size()));
     od->d_mats32 = (float*)dalloc(ctx, sizeof(float) * std::max<size_t>(1, od->mats.size()));
+    od->d_matsb = (double*)dalloc(ctx, sizeof(double) * std::max<size_t>(1, od->mats.size()));
+    od->d_matsb32 = (float*)dalloc(ctx, sizeof(float) * std::max<size_t>(1, od->mats.size()));
     std::vector<float> m32(od->mats.begin(), od->mats.end());
+    std::vector<double> mb(od->mats.size());
+    for (size_t mi = 0; mi < bs.size(); ++mi) {
+        if (!bs[mi].active) continue;
+        const size_t b0 = (size_t)base[mi] * K2 * K2, n = (size_t)(2 * bs[mi].L + 1) * K2 * K2;
+        for (size_t q = 0; q < n; ++q) mb[b0 + q] = op.terms[mi].beta * od->mats[b0 + q];
+    }
+    std::vector<float> mb32(mb.begin(), mb.end());
     if (!od->mats.empty()) {
         MWB_CUDA(cudaMemcpyAsync(od->d_mats, od->mats.data(), sizeof(double) * od->mats.size(), cudaMemcpyHostToDevice, s));
         MWB_CUDA(cudaMemcpyAsync(od->d_mats32, m32.data(), sizeof(float) * m32.size(), cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(od->d_matsb, mb.data(), sizeof(double) * mb.size(), cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(od->d_matsb32, mb32.data(), sizeof(float) * mb32.size(), cudaMemcpyHostToDevice, s));
     }
     if (!od->deltas.empty())
         MWB_CUDA(cudaMemcpyAsync(od->d_deltas, od->deltas.data(), sizeof(DeltaRec) * od->deltas.size(), cudaMemcpyHostToDevice, s));

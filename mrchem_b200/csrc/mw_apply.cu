@@ -35,6 +35,8 @@ struct BTree {
     const TermRec* terms;
     const double* mats;
     const float* mats32;
+    const double* matsb;    // beta-scaled copies (z-step operators)
+    const float* matsb32;
     int nprefix;
     int root;
     double theta;
@@ -714,6 +716,8 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         d.terms = b.tab->d_terms;
         d.mats = b.tab->d_mats;
         d.mats32 = b.tab->d_mats32;
+        d.matsb = b.tab->d_matsb;
+        d.matsb32 = b.tab->d_matsb32;
         d.nprefix = b.nprefix;
         d.root = bp.depth == 0;
         d.theta = b.theta;

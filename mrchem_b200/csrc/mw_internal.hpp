@@ -81,6 +81,8 @@ struct OpDepth {
     std::vector<TermRec> terms;
     double* d_mats = nullptr;
     float* d_mats32 = nullptr;  // FP32 copy of d_mats (mixed-precision apply)
+    double* d_matsb = nullptr;  // each matrix scaled by its term's beta (z-step operators)
+    float* d_matsb32 = nullptr;
     DeltaRec* d_deltas = nullptr;
     TermRec* d_terms = nullptr;
 };
