@@ -27,6 +27,7 @@ typedef struct mw_ctx_s* mw_ctx;   /* device + stream + memory pool */
 typedef struct mw_mra_s* mw_mra;   /* world, basis, filters (host and device copies) */
 typedef struct mw_tree_s* mw_tree; /* one function: device SoA node arrays + hash index */
 typedef struct mw_op_s* mw_op;     /* separated-Gaussian convolution operator, device tables */
+typedef struct mw_mlp_s* mw_mlp;   /* learned output-tree proposal network (FP32 MLP on the device) */
 
 enum { MW_OK = 0, MW_ERR_ARG = -1, MW_ERR_CUDA = -2, MW_ERR_STATE = -3, MW_ERR_CAPACITY = -4 };
 enum { MW_BASIS_INTERPOLATING = 0, MW_BASIS_LEGENDRE = 1 };
@@ -125,6 +126,36 @@ int mw_apply_batched(int n, double prec, mw_tree* out, mw_op* ops, mw_tree* inp,
  * tree (-1 after a batched apply of more than one tree), [1] triples of the whole batch,
  * [2] refinement passes, [3] output nodes */
 int mw_apply_stats(mw_tree out, long long* stats);
+
+/* Learned output-tree proposal.  No counterpart in the reference: MRCPP refines the output tree
+ * pass by pass (the plain path above).  A small FP32 MLP predicts which output nodes the wavelet-norm
+ * check will split, from 64 features per node (level, position, block and wavelet norms of the 27
+ * input neighbours relative to the split threshold, operator and precision scales).  It is trained
+ * on the device (forward, backward and Adam kernels of this library) from plain applies. */
+int mw_mlp_create(mw_ctx ctx, int hidden_layers, int width, unsigned seed, mw_mlp* out);
+int mw_mlp_destroy(mw_mlp mlp);
+int mw_mlp_nparams(mw_mlp mlp, long long* n, int* nfeatures);
+/* parameters, layer by layer: W (out x in, row-major) then b; host buffers of mw_mlp_nparams floats */
+int mw_mlp_get_params(mw_mlp mlp, float* p);
+int mw_mlp_set_params(mw_mlp mlp, const float* p);
+/* logits of n feature rows (host, n x nfeatures) */
+int mw_mlp_forward(mw_mlp mlp, int n, const float* x, float* logits);
+/* class-weighted binary cross-entropy of n rows and its gradient w.r.t. all parameters (host) */
+int mw_mlp_gradient(mw_mlp mlp, int n, const float* x, const float* y, const float* w, double* loss, float* grad);
+/* append the features and split labels of the non-root nodes of `out`, the result of a plain apply of
+ * `op` to `inp`, to the network's training set (kept on the device) */
+int mw_mlp_collect(mw_mlp mlp, mw_tree out, mw_op op, mw_tree inp);
+int mw_mlp_dataset(mw_mlp mlp, int* n, int* npositive);
+int mw_mlp_dataset_get(mw_mlp mlp, float* x, float* y);
+/* Adam on the training set (class-balanced weights); returns the last epoch's mean loss */
+int mw_mlp_train(mw_mlp mlp, int epochs, int batch, float lr, unsigned seed, double* loss);
+/* Learned apply: exact root pass, proposal of the deeper tree (nodes with sigmoid(logit) > tau
+ * split), one pass over all proposed nodes, then the plain criterion on every computed node: extra
+ * nodes are pruned and missed splits refined, so the output equals mw_apply_batched's.  stats (may be
+ * NULL): [0] triples, [1] passes, [2] proposed nodes, [3] pruned nodes, [4] refined misses,
+ * [5] output nodes. */
+int mw_apply_learned(int n, double prec, mw_tree* out, mw_op* ops, mw_tree* inp, int flags, mw_mlp mlp, float tau,
+                     long long* stats);
 
 #ifdef __cplusplus
 }

@@ -7,14 +7,14 @@
 #include <numeric>
 #include <string>
 #include <tuple>
+#include <unordered_map>
 
 #include "../../include/mwb200.h"
 #include "mw_kernels.cuh"
+#include "mw_learned.cuh"
 
 namespace mwb {
 
-uint64_t host_make_key(int depth, long long tx, long long ty, long long tz);
-void host_key_trans(uint64_t k, long long t[3]);
 
 static thread_local std::string g_err;
 
@@ -477,7 +477,6 @@ static void apply_batched(double prec, int n, Tree** out, Op** op, Tree** inp, i
     }
     for (int depth = 0;; ++depth) {
         BatchPass bp;
-        bp.depth = depth;
         bp.precision = precision;
         std::vector<int> idx;
         for (int i = 0; i < n; ++i) {
@@ -492,6 +491,7 @@ static void apply_batched(double prec, int n, Tree** out, Op** op, Tree** inp, i
             bt.oend = e;
             bt.prec = prec;
             bt.g0 = g0[i];
+            bt.depth = depth;
             if (depth == 0) {
                 const double nu0 = bt.tab->deltas.empty() ? 0.0 : bt.tab->deltas.front().maxb;
                 bt.theta = kScreen * prec * fnorm[i] * nu0;
@@ -526,11 +526,273 @@ static void apply_batched(double prec, int n, Tree** out, Op** op, Tree** inp, i
     }
     MWB_CUDA(cudaStreamSynchronize(s));
     for (int i = 0; i < n; ++i) {
+        out[i]->g0 = g0[i];
+        out[i]->prec = prec;
         out[i]->stats[0] = (n == 1) ? total_trip : -1;
         out[i]->stats[1] = total_trip;
         out[i]->stats[2] = passes[i];
         out[i]->stats[3] = out[i]->n;
     }
+}
+
+// run passes over explicit (tree, depth, node range) entries, at most 128 entries per launch set
+struct Entry {
+    int tree, depth, begin, end;
+};
+static long long run_entries(double prec, int precision, const std::vector<Entry>& ents, Tree** out, Op** op,
+                             Tree** inp, const std::vector<double>& fnorm, const std::vector<double>& nu_max,
+                             const std::vector<double>& g0) {
+    long long trip = 0;
+    cudaStream_t s = out[0]->mra->ctx->stream;
+    for (size_t e0 = 0; e0 < ents.size(); e0 += 128) {
+        BatchPass bp;
+        bp.precision = precision;
+        for (size_t e = e0; e < std::min(ents.size(), e0 + 128); ++e) {
+            const Entry& en = ents[e];
+            const int i = en.tree;
+            BatchTree bt;
+            bt.out = out[i];
+            bt.inp = inp[i];
+            bt.tab = &op_depth(*op[i], en.depth);
+            bt.obegin = en.begin;
+            bt.oend = en.end;
+            bt.prec = prec;
+            bt.g0 = g0[i];
+            bt.depth = en.depth;
+            if (en.depth == 0) {
+                const double nu0 = bt.tab->deltas.empty() ? 0.0 : bt.tab->deltas.front().maxb;
+                bt.theta = kScreen * prec * fnorm[i] * nu0;
+            } else {
+                bt.theta = kScreen * split_threshold(prec, g0[i], en.depth);
+            }
+            int np = 0;
+            while (nu_max[i] > 0.0 && np < (int)bt.tab->deltas.size() && !(bt.tab->deltas[np].maxb * nu_max[i] < bt.theta))
+                ++np;
+            bt.nprefix = np;
+            bp.trees.push_back(bt);
+        }
+        run_batch_pass(bp, s);
+        trip += bp.triples;
+    }
+    return trip;
+}
+
+// Learned apply: exact root pass, network proposal of the deeper tree, one pass over all proposed
+// nodes, then the plain criterion on every computed node (prune extras, refine misses).  The output
+// equals apply_batched's.  stats: [0] triples, [1] passes, [2] proposed nodes, [3] pruned,
+// [4] missed (refined) splits, [5] output nodes
+static void apply_learned(double prec, int n, Tree** out, Op** op, Tree** inp, int precision, Mlp& M, float tau,
+                          long long* stats) {
+    if (n <= 0 || n > 128) throw Error(MW_ERR_ARG, "batch size must be in [1, 128]");
+    const Mra* m = inp[0]->mra;
+    for (int i = 0; i < n; ++i) {
+        if (!out[i] || !op[i] || !inp[i]) throw Error(MW_ERR_ARG, "null tree or operator");
+        if (out[i]->mra != m || inp[i]->mra != m || op[i]->mra != m)
+            throw Error(MW_ERR_ARG, "trees and operators must share the world");
+        if (inp[i]->n == 0) throw Error(MW_ERR_STATE, "input tree is empty");
+        for (int j = 0; j < n; ++j)
+            if (out[i] == inp[j] || (j != i && out[i] == out[j]))
+                throw Error(MW_ERR_ARG, "output trees must be distinct from each other and from the inputs");
+    }
+    if (!(prec > 0.0)) throw Error(MW_ERR_ARG, "the learned apply needs prec > 0");
+    Ctx* ctx = m->ctx;
+    cudaStream_t s = ctx->stream;
+    const float logit_tau = std::log(tau / (1.0f - tau));
+    std::vector<double> fnorm(n), nu_max(n), g0(n, 0.0);
+    long long trip = 0, proposed = 0, pruned = 0, missed = 0;
+    int passes = 0;
+    std::vector<Entry> ents;
+    for (int i = 0; i < n; ++i) {
+        tree_make_roots(*out[i]);
+        fnorm[i] = std::sqrt(reduce_leaf_norm2(*inp[i], s));
+        nu_max[i] = std::sqrt(reduce_max_norm2(*inp[i], s));
+        ents.push_back(Entry{i, 0, 0, out[i]->n});
+    }
+    // exact root pass (sets g0)
+    {
+        BatchPass bp;
+        bp.precision = precision;
+        for (const Entry& en : ents) {
+            const int i = en.tree;
+            BatchTree bt;
+            bt.out = out[i];
+            bt.inp = inp[i];
+            bt.tab = &op_depth(*op[i], 0);
+            bt.obegin = en.begin;
+            bt.oend = en.end;
+            bt.prec = prec;
+            bt.depth = 0;
+            const double nu0 = bt.tab->deltas.empty() ? 0.0 : bt.tab->deltas.front().maxb;
+            bt.theta = kScreen * prec * fnorm[i] * nu0;
+            int np = 0;
+            while (nu_max[i] > 0.0 && np < (int)bt.tab->deltas.size() && !(bt.tab->deltas[np].maxb * nu_max[i] < bt.theta))
+                ++np;
+            bt.nprefix = np;
+            bp.trees.push_back(bt);
+        }
+        run_batch_pass(bp, s);
+        trip += bp.triples;
+        ++passes;
+        for (int i = 0; i < n; ++i) {
+            g0[i] = bp.trees[i].g0;
+            if (g0[i] > 0.0) tree_add_children(*out[i], bp.split_lists[i]);
+        }
+    }
+    // proposal: level by level, the network decides which nodes will split
+    std::vector<double*> rootw(n, nullptr);
+    for (int i = 0; i < n; ++i) rootw[i] = root_wnorms(*out[i]);
+    std::vector<FeatCtx> fc(n);
+    for (int i = 0; i < n; ++i) fc[i] = FeatCtx{out[i], inp[i], op[i], prec, g0[i], rootw[i]};
+    std::vector<long long> budget_used(n, 0);
+    for (int depth = 1;; ++depth) {
+        std::vector<int2> items;
+        for (int i = 0; i < n; ++i) {
+            if (out[i]->levels() <= depth || depth >= m->depth_limit) continue;
+            for (int q = out[i]->level_begin[depth]; q < out[i]->level_begin[depth + 1]; ++q) items.push_back(int2{i, q});
+        }
+        if (items.empty()) break;
+        float* d_F = features(ctx, fc, items, s);
+        std::vector<float> z = mlp_logits(M, d_F, (int)items.size(), s);
+        dfree(ctx, d_F);
+        std::vector<std::vector<int>> lists(n);
+        for (size_t q = 0; q < items.size(); ++q)
+            if (z[q] > logit_tau) lists[items[q].x].push_back(items[q].y);
+        bool any = false;
+        for (int i = 0; i < n; ++i) {
+            // proposal budget: twice the input tree; what lies beyond is left to the exact refinement
+            const long long room = 2LL * inp[i]->n - budget_used[i];
+            if ((long long)lists[i].size() * 8 > room) lists[i].resize(std::max(0LL, room / 8));
+            budget_used[i] += 8LL * (long long)lists[i].size();
+        }
+        for (int i = 0; i < n; ++i)
+            if (!lists[i].empty()) {
+                tree_add_children(*out[i], lists[i]);
+                proposed += 8 * (long long)lists[i].size();
+                any = true;
+            }
+        if (!any) break;
+    }
+    // compute every node below the root level in one pass set
+    ents.clear();
+    for (int i = 0; i < n; ++i)
+        for (int d = 1; d < out[i]->levels(); ++d)
+            if (out[i]->level_begin[d + 1] > out[i]->level_begin[d])
+                ents.push_back(Entry{i, d, out[i]->level_begin[d], out[i]->level_begin[d + 1]});
+    if (!ents.empty()) {
+        trip += run_entries(prec, precision, ents, out, op, inp, fnorm, nu_max, g0);
+        ++passes;
+    }
+    // exact criterion on every computed node, top-down; prune extras, refine misses
+    for (int iter = 0;; ++iter) {
+        std::vector<Entry> next;
+        for (int i = 0; i < n; ++i) {
+            Tree& t = *out[i];
+            const int nn = t.n;
+            std::vector<double> w2(nn);
+            std::vector<int> c0(nn);
+            std::vector<uint64_t> key(nn);
+            MWB_CUDA(cudaMemcpyAsync(w2.data(), t.wnorm2, sizeof(double) * nn, cudaMemcpyDeviceToHost, s));
+            MWB_CUDA(cudaMemcpyAsync(c0.data(), t.child0, sizeof(int) * nn, cudaMemcpyDeviceToHost, s));
+            MWB_CUDA(cudaMemcpyAsync(key.data(), t.key, sizeof(uint64_t) * nn, cudaMemcpyDeviceToHost, s));
+            MWB_CUDA(cudaStreamSynchronize(s));
+            std::vector<char> keep(nn, 0);
+            std::vector<uint64_t> miss;
+            std::vector<int> stack;
+            for (int q = 0; q < t.level_begin[1]; ++q) stack.push_back(q);
+            while (!stack.empty()) {
+                const int q = stack.back();
+                stack.pop_back();
+                keep[q] = 1;
+                const int d = (int)(key[q] >> 59);
+                const bool split = d < m->depth_limit && std::sqrt(w2[q]) > split_threshold(prec, g0[i], d);
+                if (split) {
+                    if (c0[q] >= 0)
+                        for (int c = 0; c < 8; ++c) stack.push_back(c0[q] + c);
+                    else
+                        miss.push_back(key[q]);
+                }
+            }
+            long long nk = 0;
+            for (char k : keep) nk += k;
+            if (nk < nn) {
+                pruned += nn - nk;
+                tree_rebuild(t, keep);
+            } else if (iter > 0) {
+                tree_rebuild(t, keep);  // restore (depth, Morton) order after appended refinements
+            }
+            if (!miss.empty()) {
+                missed += (long long)miss.size();
+                std::sort(miss.begin(), miss.end());  // depth-major: children come out grouped by depth
+                std::vector<uint64_t> k2(t.n);
+                MWB_CUDA(cudaMemcpyAsync(k2.data(), t.key, sizeof(uint64_t) * t.n, cudaMemcpyDeviceToHost, s));
+                MWB_CUDA(cudaStreamSynchronize(s));
+                std::unordered_map<uint64_t, int> pos;
+                for (int q = 0; q < t.n; ++q) pos[k2[q]] = q;
+                std::vector<int> list;
+                for (uint64_t k : miss) list.push_back(pos.at(k));
+                const int base = t.n;
+                tree_add_children(t, list);
+                // one entry per depth of the appended children
+                int b = base;
+                for (size_t q = 0; q < miss.size();) {
+                    const int d = (int)(miss[q] >> 59) + 1;
+                    size_t r = q;
+                    while (r < miss.size() && (int)(miss[r] >> 59) + 1 == d) ++r;
+                    next.push_back(Entry{i, d, b, b + 8 * (int)(r - q)});
+                    b += 8 * (int)(r - q);
+                    q = r;
+                }
+            }
+        }
+        if (next.empty()) break;
+        trip += run_entries(prec, precision, next, out, op, inp, fnorm, nu_max, g0);
+        ++passes;
+    }
+    for (int i = 0; i < n; ++i) {
+        dfree(ctx, rootw[i]);
+        tree_sumup_top_down(*out[i]);
+        tree_compress_bottom_up(*out[i]);
+        launch_node_norms(*out[i], 0, out[i]->n, s);
+        out[i]->g0 = g0[i];
+        out[i]->prec = prec;
+        out[i]->stats[0] = n == 1 ? trip : -1;
+        out[i]->stats[1] = trip;
+        out[i]->stats[2] = passes;
+        out[i]->stats[3] = out[i]->n;
+    }
+    MWB_CUDA(cudaStreamSynchronize(s));
+    if (stats) {
+        long long nout = 0;
+        for (int i = 0; i < n; ++i) nout += out[i]->n;
+        stats[0] = trip;
+        stats[1] = passes;
+        stats[2] = proposed;
+        stats[3] = pruned;
+        stats[4] = missed;
+        stats[5] = nout;
+    }
+}
+
+// features and labels (split or not) of the non-root nodes of an applied output tree
+static void collect_training(Mlp& M, Tree& out, Op& op, Tree& inp) {
+    if (out.n == 0 || out.levels() < 2) return;
+    Ctx* ctx = out.mra->ctx;
+    cudaStream_t s = ctx->stream;
+    double* rw = root_wnorms(out);
+    std::vector<FeatCtx> fc{FeatCtx{&out, &inp, &op, out.prec, out.g0, rw}};
+    std::vector<int2> items;
+    std::vector<int> c0(out.n);
+    MWB_CUDA(cudaMemcpyAsync(c0.data(), out.child0, sizeof(int) * out.n, cudaMemcpyDeviceToHost, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
+    std::vector<float> y;
+    for (int q = out.level_begin[1]; q < out.n; ++q) {
+        items.push_back(int2{0, q});
+        y.push_back(c0[q] >= 0 ? 1.0f : 0.0f);
+    }
+    float* d_F = features(ctx, fc, items, s);
+    mlp_append(M, d_F, y, s);
+    dfree(ctx, d_F);
+    dfree(ctx, rw);
 }
 
 }  // namespace mwb
@@ -544,6 +806,7 @@ struct mw_ctx_s : Ctx {};
 struct mw_mra_s : Mra {};
 struct mw_tree_s : Tree {};
 struct mw_op_s : Op {};
+struct mw_mlp_s : Mlp {};
 
 #define MW_TRY(...)                                        \
     try {                                                  \
@@ -959,6 +1222,146 @@ int mw_apply_stats(mw_tree out, long long* stats) {
     MW_TRY({
         MW_ARG(out && stats, "null pointer");
         for (int i = 0; i < 4; ++i) stats[i] = out->stats[i];
+    })
+}
+
+int mw_mlp_create(mw_ctx ctx, int hidden_layers, int width, unsigned seed, mw_mlp* out) {
+    MW_TRY({
+        MW_ARG(ctx && out, "null pointer");
+        MW_ARG(hidden_layers >= 1 && hidden_layers <= 8 && width >= 8 && width <= 512, "bad network shape");
+        MWB_CUDA(cudaSetDevice(ctx->device));
+        auto* M = new mw_mlp_s();
+        mlp_init(*M, ctx, hidden_layers, width, seed);
+        *out = M;
+    })
+}
+
+int mw_mlp_destroy(mw_mlp mlp) {
+    MW_TRY({
+        if (mlp) delete mlp;
+    })
+}
+
+int mw_mlp_nparams(mw_mlp mlp, long long* n, int* nfeatures) {
+    MW_TRY({
+        MW_ARG(mlp && n && nfeatures, "null pointer");
+        *n = (long long)mlp->nparam;
+        *nfeatures = kNF;
+    })
+}
+
+int mw_mlp_get_params(mw_mlp mlp, float* p) {
+    MW_TRY({
+        MW_ARG(mlp && p, "null pointer");
+        MWB_CUDA(cudaSetDevice(mlp->ctx->device));
+        MWB_CUDA(cudaMemcpyAsync(p, mlp->d_p, sizeof(float) * mlp->nparam, cudaMemcpyDeviceToHost, mlp->ctx->stream));
+        MWB_CUDA(cudaStreamSynchronize(mlp->ctx->stream));
+    })
+}
+
+int mw_mlp_set_params(mw_mlp mlp, const float* p) {
+    MW_TRY({
+        MW_ARG(mlp && p, "null pointer");
+        MWB_CUDA(cudaSetDevice(mlp->ctx->device));
+        MWB_CUDA(cudaMemcpyAsync(mlp->d_p, p, sizeof(float) * mlp->nparam, cudaMemcpyHostToDevice, mlp->ctx->stream));
+        MWB_CUDA(cudaStreamSynchronize(mlp->ctx->stream));
+    })
+}
+
+int mw_mlp_forward(mw_mlp mlp, int n, const float* x, float* logits) {
+    MW_TRY({
+        MW_ARG(mlp && x && logits && n > 0, "null pointer or empty input");
+        Ctx* ctx = mlp->ctx;
+        MWB_CUDA(cudaSetDevice(ctx->device));
+        float* d_X = (float*)dalloc(ctx, sizeof(float) * (size_t)n * kNF);
+        MWB_CUDA(cudaMemcpyAsync(d_X, x, sizeof(float) * (size_t)n * kNF, cudaMemcpyHostToDevice, ctx->stream));
+        std::vector<float> z = mlp_logits(*mlp, d_X, n, ctx->stream);
+        std::copy(z.begin(), z.end(), logits);
+        dfree(ctx, d_X);
+        MWB_CUDA(cudaStreamSynchronize(ctx->stream));
+    })
+}
+
+int mw_mlp_gradient(mw_mlp mlp, int n, const float* x, const float* y, const float* w, double* loss, float* grad) {
+    MW_TRY({
+        MW_ARG(mlp && x && y && w && loss && grad && n > 0, "null pointer or empty input");
+        Ctx* ctx = mlp->ctx;
+        cudaStream_t s = ctx->stream;
+        MWB_CUDA(cudaSetDevice(ctx->device));
+        float* d_X = (float*)dalloc(ctx, sizeof(float) * (size_t)n * kNF);
+        float* d_y = (float*)dalloc(ctx, sizeof(float) * n);
+        float* d_w = (float*)dalloc(ctx, sizeof(float) * n);
+        MWB_CUDA(cudaMemcpyAsync(d_X, x, sizeof(float) * (size_t)n * kNF, cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(d_y, y, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(d_w, w, sizeof(float) * n, cudaMemcpyHostToDevice, s));
+        std::vector<float*> acts;
+        mlp_forward(*mlp, d_X, n, acts, s);
+        *loss = mlp_backward(*mlp, acts, d_y, d_w, n, s);
+        free_acts(*mlp, acts);
+        MWB_CUDA(cudaMemcpyAsync(grad, mlp->d_g, sizeof(float) * mlp->nparam, cudaMemcpyDeviceToHost, s));
+        MWB_CUDA(cudaStreamSynchronize(s));
+        for (float* q : {d_X, d_y, d_w}) dfree(ctx, q);
+    })
+}
+
+int mw_mlp_collect(mw_mlp mlp, mw_tree out, mw_op op, mw_tree inp) {
+    MW_TRY({
+        MW_ARG(mlp && out && op && inp, "null pointer");
+        MW_ARG(out->g0 > 0.0 && out->prec > 0.0, "output tree has no apply to learn from");
+        MWB_CUDA(cudaSetDevice(mlp->ctx->device));
+        collect_training(*mlp, *out, *op, *inp);
+    })
+}
+
+int mw_mlp_dataset(mw_mlp mlp, int* n, int* npos) {
+    MW_TRY({
+        MW_ARG(mlp && n && npos, "null pointer");
+        *n = mlp->n_data;
+        std::vector<float> y(mlp->n_data);
+        if (mlp->n_data) {
+            MWB_CUDA(cudaMemcpyAsync(y.data(), mlp->d_y, sizeof(float) * y.size(), cudaMemcpyDeviceToHost, mlp->ctx->stream));
+            MWB_CUDA(cudaStreamSynchronize(mlp->ctx->stream));
+        }
+        int p = 0;
+        for (float v : y) p += v > 0.5f;
+        *npos = p;
+    })
+}
+
+int mw_mlp_dataset_get(mw_mlp mlp, float* x, float* y) {
+    MW_TRY({
+        MW_ARG(mlp && x && y, "null pointer");
+        cudaStream_t s = mlp->ctx->stream;
+        MWB_CUDA(cudaMemcpyAsync(x, mlp->d_X, sizeof(float) * (size_t)mlp->n_data * kNF, cudaMemcpyDeviceToHost, s));
+        MWB_CUDA(cudaMemcpyAsync(y, mlp->d_y, sizeof(float) * mlp->n_data, cudaMemcpyDeviceToHost, s));
+        MWB_CUDA(cudaStreamSynchronize(s));
+    })
+}
+
+int mw_mlp_train(mw_mlp mlp, int epochs, int batch, float lr, unsigned seed, double* loss) {
+    MW_TRY({
+        MW_ARG(mlp && loss && epochs > 0 && batch > 0 && lr > 0.0f, "bad training arguments");
+        MWB_CUDA(cudaSetDevice(mlp->ctx->device));
+        *loss = mlp_train(*mlp, epochs, batch, lr, seed);
+    })
+}
+
+int mw_apply_learned(int n, double prec, mw_tree* out, mw_op* ops, mw_tree* inp, int flags, mw_mlp mlp, float tau,
+                     long long* stats) {
+    MW_TRY({
+        MW_ARG(n > 0 && out && ops && inp && mlp, "null pointer or empty batch");
+        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32, "unknown apply flags");
+        MW_ARG(tau > 0.0f && tau < 1.0f, "tau must be in (0, 1)");
+        MW_ARG(inp[0], "null input tree");
+        MWB_CUDA(cudaSetDevice(inp[0]->mra->ctx->device));
+        std::vector<Tree*> o(n), i(n);
+        std::vector<Op*> p(n);
+        for (int q = 0; q < n; ++q) {
+            o[q] = out[q];
+            p[q] = ops[q];
+            i[q] = inp[q];
+        }
+        apply_learned(prec, n, o.data(), p.data(), i.data(), flags, *mlp, tau, stats);
     })
 }
 

@@ -41,6 +41,9 @@ struct BTree {
     int root;
     double theta;
     double thr;  // split threshold of this pass
+    int depth;   // depth of this entry's output nodes
+    int depth_limit;
+    long long ext[3];
 };
 
 struct Item {
@@ -57,15 +60,16 @@ struct Chunk {
 // ---------------------------------------------------------------------------------------------
 // 1. candidates
 // ---------------------------------------------------------------------------------------------
-__global__ void k_bcand(const Item* __restrict__ items, int nitems, const BTree* __restrict__ trees, int depth,
-                        long long e0, long long e1, long long e2, int fill, int* count, const int* offs, int* cdelta,
-                        int* csrc, uint64_t* greq_key, int* greq_leaf, int* ngreq) {
+__global__ void k_bcand(const Item* __restrict__ items, int nitems, const BTree* __restrict__ trees, int fill,
+                        int* count, const int* offs, int* cdelta, int* csrc, uint64_t* greq_key, int* greq_leaf,
+                        int* ngreq) {
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
     const int lane = threadIdx.x & 31;
     if (w >= nitems) return;
     const Item it = items[w];
     const BTree& T = trees[it.tree];
-    const long long ext[3] = {e0, e1, e2};
+    const int depth = T.depth;
+    const long long ext[3] = {T.ext[0], T.ext[1], T.ext[2]};
     long long to[3];
     key_trans(T.okey[it.node], to);
     int kept = 0;
@@ -96,7 +100,7 @@ __global__ void k_bcand(const Item* __restrict__ items, int nitems, const BTree*
                     const double nul = leaf >= 0 ? sqrt(T.in.norm2[leaf]) : 0.0;
                     if (nul > 0.0 && de.maxb * nul >= T.theta) {
                         ok = 1;
-                        // tree index in the (per-pass constant) depth bits: unique across the batch
+                        // entry index in place of the depth bits (an entry has one depth): unique
                         gk = ((uint64_t)it.tree << 57) | (key & ((1ull << 57) - 1));
                     }
                 }
@@ -156,7 +160,7 @@ __global__ void k_bresolve_gen(int* csrc, int ncand, const uint64_t* __restrict_
 // ---------------------------------------------------------------------------------------------
 template <int K>
 __global__ void __launch_bounds__(256) k_bgenerate(const uint64_t* __restrict__ ukey, const int* __restrict__ uleaf,
-                                                   const BTree* __restrict__ trees, int depth,
+                                                   const BTree* __restrict__ trees,
                                                    const double* __restrict__ FT, double* gblk, double* gnorm2) {
     using G = Geo<K>;
     extern __shared__ double sm[];
@@ -167,6 +171,7 @@ __global__ void __launch_bounds__(256) k_bgenerate(const uint64_t* __restrict__ 
     const int g = blockIdx.x;
     const uint64_t gkey = ukey[g];
     const BTree& T = trees[(int)(gkey >> 57)];
+    const int depth = T.depth;
     const int leaf = uleaf[g];
     for (int i = threadIdx.x; i < G::K2 * G::K2; i += blockDim.x) M[i] = FT[i];
     for (int e = threadIdx.x; e < G::BS; e += blockDim.x) {
@@ -632,13 +637,13 @@ __global__ void k_tree_item_norm2(const Item* __restrict__ items, const int* __r
     block_sum2(s, d, red);
     if (threadIdx.x == 0) out[t] = s;
 }
-__global__ void k_bsplit_flags(const Item* __restrict__ items, int nitems, const BTree* __restrict__ trees, int depth,
-                               int depth_limit, int* flags) {
+__global__ void k_bsplit_flags(const Item* __restrict__ items, int nitems, const BTree* __restrict__ trees,
+                               int* flags) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nitems) return;
     const Item it = items[i];
     const BTree& T = trees[it.tree];
-    flags[i] = (depth < depth_limit && sqrt(T.ownorm2[it.node]) > T.thr) ? 1 : 0;
+    flags[i] = (T.depth < T.depth_limit && sqrt(T.ownorm2[it.node]) > T.thr) ? 1 : 0;
 }
 __global__ void k_bsplit_list(const int* __restrict__ flags, const int* __restrict__ pos, const Item* __restrict__ items,
                               int n, int* list) {
@@ -719,9 +724,12 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         d.matsb = b.tab->d_matsb;
         d.matsb32 = b.tab->d_matsb32;
         d.nprefix = b.nprefix;
-        d.root = bp.depth == 0;
+        d.root = b.depth == 0;
         d.theta = b.theta;
         d.thr = 0.0;
+        d.depth = b.depth;
+        d.depth_limit = m.depth_limit;
+        for (int q = 0; q < 3; ++q) d.ext[q] = (long long)m.boxes[q] << b.depth;
     }
     item_off[nt] = (int)items.size();
     const int ni = (int)items.size();
@@ -737,11 +745,9 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     int* d_ngreq = (int*)dalloc(ctx, sizeof(int));
     MWB_CUDA(cudaMemsetAsync(d_count, 0, sizeof(int) * (ni + 1), s));
     MWB_CUDA(cudaMemsetAsync(d_ngreq, 0, sizeof(int), s));
-    const long long e0 = (long long)m.boxes[0] << bp.depth, e1 = (long long)m.boxes[1] << bp.depth,
-                    e2 = (long long)m.boxes[2] << bp.depth;
     const int cblocks = (ni * 32 + 255) / 256;
-    k_bcand<<<cblocks, 256, 0, s>>>(d_items, ni, d_trees, bp.depth, e0, e1, e2, 0, d_count, nullptr, nullptr, nullptr,
-                                    nullptr, nullptr, nullptr);
+    k_bcand<<<cblocks, 256, 0, s>>>(d_items, ni, d_trees, 0, d_count, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                    nullptr);
     MWB_CUDA(cudaGetLastError());
     count(ctx);
     const int ncand = scan_total(ctx, d_count, d_offs, ni);
@@ -751,8 +757,8 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     uint64_t* d_greq_key = (uint64_t*)dalloc(ctx, sizeof(uint64_t) * ncap);
     int* d_greq_leaf = (int*)dalloc(ctx, sizeof(int) * ncap);
     if (ncand > 0) {
-        k_bcand<<<cblocks, 256, 0, s>>>(d_items, ni, d_trees, bp.depth, e0, e1, e2, 1, d_count, d_offs, d_cdelta, d_csrc,
-                                        d_greq_key, d_greq_leaf, d_ngreq);
+        k_bcand<<<cblocks, 256, 0, s>>>(d_items, ni, d_trees, 1, d_count, d_offs, d_cdelta, d_csrc, d_greq_key,
+                                        d_greq_leaf, d_ngreq);
         MWB_CUDA(cudaGetLastError());
         count(ctx);
     }
@@ -790,7 +796,7 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     {                                                                                                     \
         size_t smem = sizeof(double) * (Geo<KK>::VOL + 4 * KK * KK + KK * KK * KK + 64);                 \
         MWB_CUDA(cudaFuncSetAttribute(k_bgenerate<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-        k_bgenerate<KK><<<nu, 256, smem, s>>>(d_ukey, d_uleaf, d_trees, bp.depth, m.d_FT, d_gblk, d_gnorm2); \
+        k_bgenerate<KK><<<nu, 256, smem, s>>>(d_ukey, d_uleaf, d_trees, m.d_FT, d_gblk, d_gnorm2);            \
     }
         MWB_DISPATCH_K(K, L_GEN)
 #undef L_GEN
@@ -882,26 +888,29 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     }
     bp.triples = (long long)ntot;
 
-    // 6. root norms (g0 per tree) when needed, then split lists per tree
-    if (bp.depth == 0) {
+    // 6. root norms (g0 per root entry), then split lists per entry
+    bool any_root = false;
+    for (int t = 0; t < nt; ++t) any_root |= bp.trees[t].depth == 0;
+    if (any_root) {
         double* d_g = (double*)dalloc(ctx, sizeof(double) * nt);
         k_tree_item_norm2<<<nt, 256, 0, s>>>(d_items, d_item_off, d_trees, d_g);
         count(ctx);
         std::vector<double> g(nt);
         MWB_CUDA(cudaMemcpyAsync(g.data(), d_g, sizeof(double) * nt, cudaMemcpyDeviceToHost, s));
         MWB_CUDA(cudaStreamSynchronize(s));
-        for (int t = 0; t < nt; ++t) bp.trees[t].g0 = std::sqrt(g[t]);
+        for (int t = 0; t < nt; ++t)
+            if (bp.trees[t].depth == 0) bp.trees[t].g0 = std::sqrt(g[t]);
         dfree(ctx, d_g);
     }
     for (int t = 0; t < nt; ++t) {
         const BatchTree& b = bp.trees[t];
-        bt[t].thr = (b.prec > 0.0 && b.g0 > 0.0) ? b.prec * b.g0 * std::pow(2.0, -0.5 * bp.depth) : INFINITY;
+        bt[t].thr = (b.prec > 0.0 && b.g0 > 0.0) ? b.prec * b.g0 * std::pow(2.0, -0.5 * b.depth) : INFINITY;
     }
     MWB_CUDA(cudaMemcpyAsync(d_trees, bt.data(), sizeof(BTree) * nt, cudaMemcpyHostToDevice, s));
     int* d_sflags = (int*)dalloc(ctx, sizeof(int) * (ni + 1));
     int* d_spos = (int*)dalloc(ctx, sizeof(int) * (ni + 1));
     MWB_CUDA(cudaMemsetAsync(d_sflags, 0, sizeof(int) * (ni + 1), s));
-    k_bsplit_flags<<<(ni + 255) / 256, 256, 0, s>>>(d_items, ni, d_trees, bp.depth, m.depth_limit, d_sflags);
+    k_bsplit_flags<<<(ni + 255) / 256, 256, 0, s>>>(d_items, ni, d_trees, d_sflags);
     count(ctx);
     const int nsplit = scan_total(ctx, d_sflags, d_spos, ni);
     bp.split_lists.assign(nt, {});

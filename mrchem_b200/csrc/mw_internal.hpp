@@ -111,7 +111,9 @@ struct Tree {
     int* hval = nullptr;
     uint32_t hcap = 0;
     std::vector<int> level_begin;  // level d = [level_begin[d], level_begin[d+1])
-    long long stats[4] = {0, 0, 0, 0};
+    long long stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double g0 = 0.0;      // root-level norm of the last apply into this tree (sets its thresholds)
+    double prec = 0.0;    // precision of the last apply into this tree
     ~Tree();
     int levels() const { return (int)level_begin.size() - 1; }
 };

@@ -60,14 +60,16 @@ struct BatchTree {
     double theta = 0.0;        // screening threshold
     double prec = 0.0;
     double g0 = 0.0;           // root-level output norm (set by the root pass)
+    int depth = 0;             // depth of these output nodes
 };
 struct BatchPass {
-    int depth = 0;
     int precision = 0;  // 0: FP64 products, 1: FP32 products with FP64 accumulation
     std::vector<BatchTree> trees;
     long long triples = 0;
     int nitems = 0, nchunks = 0, nslots = 0;
-    std::vector<std::vector<int>> split_lists;  // per tree: nodes to split (level order)
+    std::vector<std::vector<int>> split_lists;  // per entry: nodes to split (level order)
+    // per item of the pass (entries in order, nodes in order): 1 if the node splits
+    std::vector<int> split_flags;
 };
 void run_batch_pass(BatchPass& bp, cudaStream_t s);
 

@@ -1,0 +1,542 @@
+// mw_learned.cu -- learned output-tree proposal for the adaptive apply.
+//
+// A small MLP (FP32, 3 hidden layers of 128 by default) predicts, for a candidate output node, whether
+// the plain wavelet-norm check will split it.  Its 64 features are: level, position, the block and
+// wavelet norms of the 27 input neighbours at the node's depth (relative to the split threshold),
+// and operator / precision scales.  It is trained on the GPU by the kernels below (forward, backward,
+// Adam) from labels produced by plain applies.
+//
+// The learned apply (apply_learned) runs the exact root pass, proposes the whole deeper tree with
+// the network, computes every proposed node in one batched pass, then applies the plain criterion
+// top-down to every computed node: proposed nodes the criterion would not have created are pruned,
+// and nodes the criterion splits but the network did not are refined with further passes.  The
+// result is the plain apply's tree (node keys and coefficients) exactly.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <numeric>
+#include <random>
+#include <unordered_map>
+
+#include "../../include/mwb200.h"
+#include "mw_device.cuh"
+#include "mw_kernels.cuh"
+#include "mw_learned.cuh"
+
+namespace mwb {
+
+void set_last_error(const std::string& msg);
+
+// ---------------------------------------------------------------------------------------------
+// features
+// ---------------------------------------------------------------------------------------------
+struct FeatTree {
+    const uint64_t* okey;   // output tree keys
+    const uint64_t* ikey;   // input tree keys
+    const double* inorm2;   // input block norms^2
+    const double* iwnorm2;  // input wavelet norms^2
+    const uint64_t* hkey;
+    const int* hval;
+    uint32_t hcap;
+    const double* root_w;   // output root-node wavelet norms^2 (exact pass), indexed by root order
+    int n0;
+    int boxes[3];
+    double thr0;            // split threshold at depth 0 (prec * g0)
+    double mu, prec;
+};
+
+__device__ inline float lg(double v) { return (float)(log10(v + 1e-30) * 0.1); }
+
+// one thread per (entry, node): writes kNF features
+__global__ void k_features(const int2* __restrict__ items, int n, const FeatTree* __restrict__ trees,
+                           const int* __restrict__ root_index, float* F) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int2 it = items[i];
+    const FeatTree& T = trees[it.x];
+    const uint64_t key = T.okey[it.y];
+    const int d = key_depth(key);
+    long long t[3];
+    key_trans(key, t);
+    const double thr = T.thr0 * pow(2.0, -0.5 * d);
+    float* f = F + (size_t)i * kNF;
+    f[0] = d / 16.0f;
+    for (int q = 0; q < 3; ++q) f[1 + q] = (float)(2.0 * (t[q] + 0.5) / ((double)T.boxes[q] * (1ll << d)) - 1.0);
+    int p = 4;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                const long long u[3] = {t[0] + dx, t[1] + dy, t[2] + dz};
+                bool inside = true;
+                for (int q = 0; q < 3; ++q) inside &= u[q] >= 0 && u[q] < ((long long)T.boxes[q] << d);
+                float fb = -3.0f, fw = -3.0f;
+                if (inside) {
+                    int idx = hlookup(T.hkey, T.hval, T.hcap, make_key(d, u[0], u[1], u[2]));
+                    if (idx >= 0) {
+                        fb = lg(sqrt(T.inorm2[idx]) / thr);
+                        fw = lg(sqrt(T.iwnorm2[idx]) / thr);
+                    } else {
+                        for (int da = d - 1; da >= 0 && idx < 0; --da) {
+                            const int sh = d - da;
+                            idx = hlookup(T.hkey, T.hval, T.hcap, make_key(da, u[0] >> sh, u[1] >> sh, u[2] >> sh));
+                            if (idx >= 0) fb = lg(sqrt(T.inorm2[idx]) * pow(2.0, -1.5 * sh) / thr);
+                        }
+                    }
+                }
+                f[p++] = fb;
+                f[p++] = fw;
+            }
+    f[58] = (float)log10(T.mu + 1e-3);
+    f[59] = (float)(log10(T.prec) * 0.1);
+    const double edge = ldexp(1.0, -(T.n0 + d));
+    f[60] = (float)log10(edge);
+    f[61] = (float)log10(T.mu * edge + 1e-3);
+    f[62] = lg(thr);
+    const int r = root_index ? root_index[i] : -1;
+    f[63] = r >= 0 ? lg(sqrt(T.root_w[r]) / T.thr0) : 0.0f;
+}
+
+// ---------------------------------------------------------------------------------------------
+// MLP kernels (FP32)
+// ---------------------------------------------------------------------------------------------
+// Y[n][o] = act(sum_i X[n][i] W[o][i] + b[o]); 16x16 tiles
+__global__ void k_lin_fwd(const float* __restrict__ X, const float* __restrict__ W, const float* __restrict__ b, float* Y,
+                          int N, int in, int out, int relu) {
+    __shared__ float xs[16][17], ws[16][17];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int n = blockIdx.x * 16 + ty, o = blockIdx.y * 16 + tx;
+    float acc = 0.0f;
+    for (int k0 = 0; k0 < in; k0 += 16) {
+        xs[ty][tx] = (n < N && k0 + tx < in) ? X[(size_t)n * in + k0 + tx] : 0.0f;
+        const int ow = blockIdx.y * 16 + ty;
+        ws[ty][tx] = (ow < out && k0 + tx < in) ? W[(size_t)ow * in + k0 + tx] : 0.0f;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 16; ++k) acc = fmaf(xs[ty][k], ws[tx][k], acc);
+        __syncthreads();
+    }
+    if (n < N && o < out) {
+        float v = acc + b[o];
+        Y[(size_t)n * out + o] = (relu && v < 0.0f) ? 0.0f : v;
+    }
+}
+// dX[n][i] = sum_o dY[n][o] W[o][i] (dY already masked by the activation)
+__global__ void k_lin_bwd_x(const float* __restrict__ dY, const float* __restrict__ W, float* dX, int N, int in, int out) {
+    __shared__ float ds[16][17], ws[16][17];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int n = blockIdx.x * 16 + ty, i = blockIdx.y * 16 + tx;
+    float acc = 0.0f;
+    for (int o0 = 0; o0 < out; o0 += 16) {
+        ds[ty][tx] = (n < N && o0 + tx < out) ? dY[(size_t)n * out + o0 + tx] : 0.0f;
+        ws[ty][tx] = (o0 + ty < out && i < in) ? W[(size_t)(o0 + ty) * in + i] : 0.0f;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 16; ++k) acc = fmaf(ds[ty][k], ws[k][tx], acc);
+        __syncthreads();
+    }
+    if (n < N && i < in) dX[(size_t)n * in + i] = acc;
+}
+// dW[o][i] = sum_n dY[n][o] X[n][i]; db[o] = sum_n dY[n][o] (one block per 16x16 tile, fixed order)
+__global__ void k_lin_bwd_w(const float* __restrict__ dY, const float* __restrict__ X, float* dW, float* db, int N,
+                            int in, int out) {
+    __shared__ float ds[16][17], xs[16][17];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int o = blockIdx.y * 16 + ty, i = blockIdx.x * 16 + tx;
+    float acc = 0.0f, accb = 0.0f;
+    for (int n0 = 0; n0 < N; n0 += 16) {
+        ds[ty][tx] = (n0 + tx < N && blockIdx.y * 16 + ty < out) ? dY[(size_t)(n0 + tx) * out + blockIdx.y * 16 + ty] : 0.0f;
+        xs[ty][tx] = (n0 + ty < N && i < in) ? X[(size_t)(n0 + ty) * in + i] : 0.0f;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            acc = fmaf(ds[ty][k], xs[k][tx], acc);
+            accb += ds[ty][k];
+        }
+        __syncthreads();
+    }
+    if (o < out && i < in) dW[(size_t)o * in + i] = acc;
+    if (o < out && blockIdx.x == 0 && tx == 0) db[o] = accb;
+}
+__global__ void k_relu_mask(float* dY, const float* __restrict__ Y, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        if (Y[i] <= 0.0f) dY[i] = 0.0f;
+}
+// weighted BCE with logits: loss_i = w_i (softplus(z) - y z); dz_i = w_i (sigmoid(z) - y) / N
+__global__ void k_bce(const float* __restrict__ z, const float* __restrict__ y, const float* __restrict__ w, int N,
+                      float* dz, float* loss_part) {
+    __shared__ float red[32];
+    float l = 0.0f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const float zi = z[i];
+        const float sp = zi > 0.0f ? zi + log1pf(expf(-zi)) : log1pf(expf(zi));
+        l += w[i] * (sp - y[i] * zi);
+        const float sg = 1.0f / (1.0f + expf(-zi));
+        dz[i] = w[i] * (sg - y[i]) / (float)N;
+    }
+    for (int o = 16; o; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = l;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        l = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0f;
+        for (int o = 16; o; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+        if (threadIdx.x == 0) loss_part[blockIdx.x] = l;
+    }
+}
+__global__ void k_adam(float* p, const float* __restrict__ g, float* m, float* v, int n, float lr, float b1, float b2,
+                       float eps, float c1, float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    m[i] = b1 * m[i] + (1.0f - b1) * gi;
+    v[i] = b2 * v[i] + (1.0f - b2) * gi * gi;
+    p[i] -= lr * (m[i] / c1) / (sqrtf(v[i] / c2) + eps);
+}
+__global__ void k_gather_rows(const float* __restrict__ src, const int* __restrict__ idx, int n, int w, float* dst) {
+    const int i = blockIdx.x;
+    if (i >= n) return;
+    for (int j = threadIdx.x; j < w; j += blockDim.x) dst[(size_t)i * w + j] = src[(size_t)idx[i] * w + j];
+}
+
+// ---------------------------------------------------------------------------------------------
+// MLP object
+// ---------------------------------------------------------------------------------------------
+Mlp::~Mlp() {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    for (float* q : {d_p, d_m, d_v, d_g, d_X, d_y}) dfree(ctx, q);
+    cudaStreamSynchronize(ctx->stream);
+}
+
+void mlp_init(Mlp& M, Ctx* ctx, int nhidden, int width, unsigned seed) {
+    M.ctx = ctx;
+    M.nhidden = nhidden;
+    M.width = width;
+    M.dims = {kNF};
+    for (int l = 0; l < nhidden; ++l) M.dims.push_back(width);
+    M.dims.push_back(1);
+    M.nparam = 0;
+    for (size_t l = 0; l + 1 < M.dims.size(); ++l) {
+        M.woff.push_back(M.nparam);
+        M.nparam += (size_t)M.dims[l] * M.dims[l + 1];
+        M.boff.push_back(M.nparam);
+        M.nparam += M.dims[l + 1];
+    }
+    std::vector<float> p(M.nparam, 0.0f);
+    std::mt19937 rng(seed);
+    for (size_t l = 0; l + 1 < M.dims.size(); ++l) {
+        std::normal_distribution<float> nd(0.0f, std::sqrt(2.0f / M.dims[l]));  // He initialisation
+        for (size_t q = 0; q < (size_t)M.dims[l] * M.dims[l + 1]; ++q) p[M.woff[l] + q] = nd(rng);
+    }
+    cudaStream_t s = ctx->stream;
+    M.d_p = (float*)dalloc(ctx, sizeof(float) * M.nparam);
+    M.d_m = (float*)dalloc(ctx, sizeof(float) * M.nparam);
+    M.d_v = (float*)dalloc(ctx, sizeof(float) * M.nparam);
+    M.d_g = (float*)dalloc(ctx, sizeof(float) * M.nparam);
+    MWB_CUDA(cudaMemcpyAsync(M.d_p, p.data(), sizeof(float) * M.nparam, cudaMemcpyHostToDevice, s));
+    MWB_CUDA(cudaMemsetAsync(M.d_m, 0, sizeof(float) * M.nparam, s));
+    MWB_CUDA(cudaMemsetAsync(M.d_v, 0, sizeof(float) * M.nparam, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
+}
+
+// forward over N rows of X; keeps the activations of every layer in acts (for backward)
+void mlp_forward(Mlp& M, const float* d_X, int N, std::vector<float*>& acts, cudaStream_t s) {
+    const int L = (int)M.dims.size() - 1;
+    acts.assign(L + 1, nullptr);
+    acts[0] = const_cast<float*>(d_X);
+    for (int l = 0; l < L; ++l) {
+        acts[l + 1] = (float*)dalloc(M.ctx, sizeof(float) * (size_t)N * M.dims[l + 1]);
+        dim3 blk(16, 16), grd((N + 15) / 16, (M.dims[l + 1] + 15) / 16);
+        k_lin_fwd<<<grd, blk, 0, s>>>(acts[l], M.d_p + M.woff[l], M.d_p + M.boff[l], acts[l + 1], N, M.dims[l],
+                                      M.dims[l + 1], l + 1 < L ? 1 : 0);
+    }
+    MWB_CUDA(cudaGetLastError());
+}
+
+// gradient of the weighted BCE loss into d_g; returns the loss
+double mlp_backward(Mlp& M, std::vector<float*>& acts, const float* d_y, const float* d_w, int N, cudaStream_t s) {
+    const int L = (int)M.dims.size() - 1;
+    Ctx* ctx = M.ctx;
+    float* dz = (float*)dalloc(ctx, sizeof(float) * N);
+    const int nb = 120;
+    float* d_lp = (float*)dalloc(ctx, sizeof(float) * nb);
+    k_bce<<<nb, 256, 0, s>>>(acts[L], d_y, d_w, N, dz, d_lp);
+    float* dcur = dz;
+    for (int l = L - 1; l >= 0; --l) {
+        dim3 blk(16, 16);
+        k_lin_bwd_w<<<dim3((M.dims[l] + 15) / 16, (M.dims[l + 1] + 15) / 16), blk, 0, s>>>(
+            dcur, acts[l], M.d_g + M.woff[l], M.d_g + M.boff[l], N, M.dims[l], M.dims[l + 1]);
+        if (l > 0) {
+            float* dprev = (float*)dalloc(ctx, sizeof(float) * (size_t)N * M.dims[l]);
+            k_lin_bwd_x<<<dim3((N + 15) / 16, (M.dims[l] + 15) / 16), blk, 0, s>>>(dcur, M.d_p + M.woff[l], dprev, N,
+                                                                                     M.dims[l], M.dims[l + 1]);
+            k_relu_mask<<<256, 256, 0, s>>>(dprev, acts[l], (size_t)N * M.dims[l]);
+            if (dcur != dz) dfree(ctx, dcur);
+            dcur = dprev;
+        }
+    }
+    MWB_CUDA(cudaGetLastError());
+    if (dcur != dz) dfree(ctx, dcur);
+    std::vector<float> lp(nb);
+    MWB_CUDA(cudaMemcpyAsync(lp.data(), d_lp, sizeof(float) * nb, cudaMemcpyDeviceToHost, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
+    dfree(ctx, dz);
+    dfree(ctx, d_lp);
+    double loss = 0.0;
+    for (float v : lp) loss += v;
+    return loss / N;
+}
+
+void free_acts(Mlp& M, std::vector<float*>& acts) {
+    for (size_t l = 1; l < acts.size(); ++l) dfree(M.ctx, acts[l]);
+    acts.clear();
+}
+
+// logits of N feature rows already on the device
+std::vector<float> mlp_logits(Mlp& M, const float* d_X, int N, cudaStream_t s) {
+    std::vector<float*> acts;
+    mlp_forward(M, d_X, N, acts, s);
+    std::vector<float> z(N);
+    MWB_CUDA(cudaMemcpyAsync(z.data(), acts.back(), sizeof(float) * N, cudaMemcpyDeviceToHost, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
+    free_acts(M, acts);
+    return z;
+}
+
+// ---------------------------------------------------------------------------------------------
+// features of a node list of several trees
+// ---------------------------------------------------------------------------------------------
+float* features(Ctx* ctx, std::vector<FeatCtx>& fc, const std::vector<int2>& items, cudaStream_t s) {
+    const int n = (int)items.size();
+    std::vector<FeatTree> ft(fc.size());
+    for (size_t t = 0; t < fc.size(); ++t) {
+        FeatCtx& c = fc[t];
+        const Mra& m = *c.out->mra;
+        FeatTree& f = ft[t];
+        f.okey = c.out->key;
+        f.ikey = c.inp->key;
+        f.inorm2 = c.inp->norm2;
+        f.iwnorm2 = c.inp->wnorm2;
+        f.hkey = c.inp->hkey;
+        f.hval = c.inp->hval;
+        f.hcap = c.inp->hcap;
+        f.root_w = c.d_root_w;
+        f.n0 = m.n0;
+        for (int q = 0; q < 3; ++q) f.boxes[q] = m.boxes[q];
+        f.thr0 = c.prec * c.g0;
+        f.mu = c.op->mu;
+        f.prec = c.prec;
+    }
+    // root ancestor index of each node (roots are the first nodes of every output tree, Morton order)
+    std::vector<int> root_index(n, -1);
+    float* d_F = (float*)dalloc(ctx, sizeof(float) * (size_t)std::max(1, n) * kNF);
+    if (n == 0) return d_F;
+    FeatTree* d_ft = (FeatTree*)dalloc(ctx, sizeof(FeatTree) * ft.size());
+    int2* d_items = (int2*)dalloc(ctx, sizeof(int2) * n);
+    int* d_ri = (int*)dalloc(ctx, sizeof(int) * n);
+    MWB_CUDA(cudaMemcpyAsync(d_ft, ft.data(), sizeof(FeatTree) * ft.size(), cudaMemcpyHostToDevice, s));
+    MWB_CUDA(cudaMemcpyAsync(d_items, items.data(), sizeof(int2) * n, cudaMemcpyHostToDevice, s));
+    // root ancestor: follow parents on the host copy is costly; use the key (root translation = t >> depth)
+    {
+        std::vector<std::vector<uint64_t>> keys(fc.size());
+        for (size_t t = 0; t < fc.size(); ++t) {
+            keys[t].resize(fc[t].out->n);
+            MWB_CUDA(cudaMemcpyAsync(keys[t].data(), fc[t].out->key, sizeof(uint64_t) * fc[t].out->n,
+                                     cudaMemcpyDeviceToHost, s));
+        }
+        MWB_CUDA(cudaStreamSynchronize(s));
+        for (size_t t = 0; t < fc.size(); ++t) {
+            const int nroot = fc[t].out->level_begin.size() > 1 ? fc[t].out->level_begin[1] : 0;
+            std::unordered_map<uint64_t, int> rmap;
+            for (int r = 0; r < nroot; ++r) rmap[keys[t][r]] = r;
+            for (int i = 0; i < n; ++i) {
+                if (items[i].x != (int)t) continue;
+                const uint64_t k = keys[t][items[i].y];
+                const int d = (int)(k >> 59);
+                long long tr[3];
+                host_key_trans(k, tr);
+                auto it = rmap.find(host_make_key(0, tr[0] >> d, tr[1] >> d, tr[2] >> d));
+                root_index[i] = it == rmap.end() ? -1 : it->second;
+            }
+        }
+    }
+    MWB_CUDA(cudaMemcpyAsync(d_ri, root_index.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    k_features<<<(n + 127) / 128, 128, 0, s>>>(d_items, n, d_ft, d_ri, d_F);
+    MWB_CUDA(cudaGetLastError());
+    MWB_CUDA(cudaStreamSynchronize(s));
+    dfree(ctx, d_ft);
+    dfree(ctx, d_items);
+    dfree(ctx, d_ri);
+    return d_F;
+}
+
+double* root_wnorms(Tree& out) {
+    Ctx* ctx = out.mra->ctx;
+    const int nroot = out.level_begin[1];
+    double* d = (double*)dalloc(ctx, sizeof(double) * nroot);
+    MWB_CUDA(cudaMemcpyAsync(d, out.wnorm2, sizeof(double) * nroot, cudaMemcpyDeviceToDevice, ctx->stream));
+    return d;
+}
+
+// ---------------------------------------------------------------------------------------------
+// training set collection from a plain apply (labels: the node was split)
+// ---------------------------------------------------------------------------------------------
+void mlp_append(Mlp& M, const float* d_F, const std::vector<float>& y, cudaStream_t s) {
+    const int n = (int)y.size();
+    if (M.n_data + n > M.cap_data) {
+        int ncap = std::max(M.n_data + n, 2 * M.cap_data + 1024);
+        float* X = (float*)dalloc(M.ctx, sizeof(float) * (size_t)ncap * kNF);
+        float* Y = (float*)dalloc(M.ctx, sizeof(float) * ncap);
+        if (M.n_data) {
+            MWB_CUDA(cudaMemcpyAsync(X, M.d_X, sizeof(float) * (size_t)M.n_data * kNF, cudaMemcpyDeviceToDevice, s));
+            MWB_CUDA(cudaMemcpyAsync(Y, M.d_y, sizeof(float) * M.n_data, cudaMemcpyDeviceToDevice, s));
+        }
+        dfree(M.ctx, M.d_X);
+        dfree(M.ctx, M.d_y);
+        M.d_X = X;
+        M.d_y = Y;
+        M.cap_data = ncap;
+    }
+    MWB_CUDA(cudaMemcpyAsync(M.d_X + (size_t)M.n_data * kNF, d_F, sizeof(float) * (size_t)n * kNF,
+                             cudaMemcpyDeviceToDevice, s));
+    MWB_CUDA(cudaMemcpyAsync(M.d_y + M.n_data, y.data(), sizeof(float) * n, cudaMemcpyHostToDevice, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
+    M.n_data += n;
+}
+
+// ---------------------------------------------------------------------------------------------
+// tree surgery: keep a subset of nodes and rebuild in (depth, Morton) order
+// ---------------------------------------------------------------------------------------------
+__global__ void k_gather_nodes(const double* __restrict__ coef, const double* __restrict__ n2,
+                               const double* __restrict__ w2, const uint64_t* __restrict__ key,
+                               const int* __restrict__ perm, int n, size_t bs, double* ncoef, double* nn2, double* nw2,
+                               uint64_t* nkey) {
+    const int i = blockIdx.x;
+    if (i >= n) return;
+    const int o = perm[i];
+    for (size_t e = threadIdx.x; e < bs; e += blockDim.x) ncoef[(size_t)i * bs + e] = coef[(size_t)o * bs + e];
+    if (threadIdx.x == 0) {
+        nn2[i] = n2[o];
+        nw2[i] = w2[o];
+        nkey[i] = key[o];
+    }
+}
+
+// rebuild `t` with the nodes whose keep flag is set (the kept set must be a tree: every kept node's
+// parent kept, siblings kept together); nodes are reordered by key (parents before children)
+void tree_rebuild(Tree& t, const std::vector<char>& keep) {
+    Ctx* ctx = t.mra->ctx;
+    cudaStream_t s = ctx->stream;
+    const int n = t.n;
+    std::vector<uint64_t> key(n);
+    MWB_CUDA(cudaMemcpyAsync(key.data(), t.key, sizeof(uint64_t) * n, cudaMemcpyDeviceToHost, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> perm;
+    for (int i = 0; i < n; ++i)
+        if (keep[i]) perm.push_back(i);
+    std::sort(perm.begin(), perm.end(), [&](int a, int b) { return key[a] < key[b]; });
+    const int nn = (int)perm.size();
+    std::unordered_map<uint64_t, int> pos;
+    pos.reserve(nn * 2);
+    for (int i = 0; i < nn; ++i) pos[key[perm[i]]] = i;
+    std::vector<int> parent(nn, -1), child0(nn, -1);
+    int maxd = 0;
+    for (int i = 0; i < nn; ++i) {
+        const uint64_t k = key[perm[i]];
+        const int d = (int)(k >> 59);
+        maxd = std::max(maxd, d);
+        long long tr[3];
+        host_key_trans(k, tr);
+        if (d > 0) parent[i] = pos.at(host_make_key(d - 1, tr[0] >> 1, tr[1] >> 1, tr[2] >> 1));
+        auto it = pos.find(host_make_key(d + 1, 2 * tr[0], 2 * tr[1], 2 * tr[2]));
+        if (it != pos.end()) child0[i] = it->second;
+    }
+    std::vector<int> lb(maxd + 2, 0);
+    for (int i = 0; i < nn; ++i) lb[(key[perm[i]] >> 59) + 1]++;
+    for (size_t d = 1; d < lb.size(); ++d) lb[d] += lb[d - 1];
+    const size_t BS = t.mra->bsize();
+    int* d_perm = (int*)dalloc(ctx, sizeof(int) * std::max(1, nn));
+    double* ncoef = (double*)dalloc(ctx, sizeof(double) * BS * std::max(1, nn));
+    double* nn2 = (double*)dalloc(ctx, sizeof(double) * std::max(1, nn));
+    double* nw2 = (double*)dalloc(ctx, sizeof(double) * std::max(1, nn));
+    uint64_t* nkey = (uint64_t*)dalloc(ctx, sizeof(uint64_t) * std::max(1, nn));
+    MWB_CUDA(cudaMemcpyAsync(d_perm, perm.data(), sizeof(int) * nn, cudaMemcpyHostToDevice, s));
+    k_gather_nodes<<<nn, 256, 0, s>>>(t.coef, t.norm2, t.wnorm2, t.key, d_perm, nn, BS, ncoef, nn2, nw2, nkey);
+    MWB_CUDA(cudaGetLastError());
+    MWB_CUDA(cudaMemcpyAsync(t.coef, ncoef, sizeof(double) * BS * nn, cudaMemcpyDeviceToDevice, s));
+    MWB_CUDA(cudaMemcpyAsync(t.norm2, nn2, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
+    MWB_CUDA(cudaMemcpyAsync(t.wnorm2, nw2, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
+    MWB_CUDA(cudaMemcpyAsync(t.key, nkey, sizeof(uint64_t) * nn, cudaMemcpyDeviceToDevice, s));
+    MWB_CUDA(cudaMemcpyAsync(t.parent, parent.data(), sizeof(int) * nn, cudaMemcpyHostToDevice, s));
+    MWB_CUDA(cudaMemcpyAsync(t.child0, child0.data(), sizeof(int) * nn, cudaMemcpyHostToDevice, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
+    for (void* p : {(void*)d_perm, (void*)ncoef, (void*)nn2, (void*)nw2, (void*)nkey}) dfree(ctx, p);
+    t.n = nn;
+    t.level_begin = lb;
+    launch_hash_reset(t, s);
+    launch_hash_insert(t, 0, nn, s);
+    MWB_CUDA(cudaStreamSynchronize(s));
+}
+
+// class-balanced weights for the current training set
+static std::vector<float> balance_weights(const std::vector<float>& y) {
+    double npos = 0.0;
+    for (float v : y) npos += v;
+    const double n = (double)y.size(), nneg = n - npos;
+    const float wp = npos > 0 ? (float)(n / (2.0 * npos)) : 0.0f, wn = nneg > 0 ? (float)(n / (2.0 * nneg)) : 0.0f;
+    std::vector<float> w(y.size());
+    for (size_t i = 0; i < y.size(); ++i) w[i] = y[i] > 0.5f ? wp : wn;
+    return w;
+}
+
+double mlp_train(Mlp& M, int epochs, int batch, float lr, unsigned seed) {
+    Ctx* ctx = M.ctx;
+    cudaStream_t s = ctx->stream;
+    const int N = M.n_data;
+    if (N == 0) throw Error(-3, "empty training set");
+    std::vector<float> y(N);
+    MWB_CUDA(cudaMemcpyAsync(y.data(), M.d_y, sizeof(float) * N, cudaMemcpyDeviceToHost, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
+    const std::vector<float> w = balance_weights(y);
+    float* d_w = (float*)dalloc(ctx, sizeof(float) * N);
+    MWB_CUDA(cudaMemcpyAsync(d_w, w.data(), sizeof(float) * N, cudaMemcpyHostToDevice, s));
+    batch = std::max(1, std::min(batch, N));
+    float* d_bx = (float*)dalloc(ctx, sizeof(float) * (size_t)batch * kNF);
+    float* d_by = (float*)dalloc(ctx, sizeof(float) * batch);
+    float* d_bw = (float*)dalloc(ctx, sizeof(float) * batch);
+    int* d_idx = (int*)dalloc(ctx, sizeof(int) * batch);
+    std::vector<int> perm(N);
+    std::iota(perm.begin(), perm.end(), 0);
+    std::mt19937 rng(seed);
+    double last = 0.0;
+    const float b1 = 0.9f, b2 = 0.999f;
+    for (int ep = 0; ep < epochs; ++ep) {
+        std::shuffle(perm.begin(), perm.end(), rng);
+        double tot = 0.0;
+        int nb = 0;
+        for (int b0 = 0; b0 + batch <= N || (b0 < N && nb == 0); b0 += batch) {
+            const int bn = std::min(batch, N - b0);
+            MWB_CUDA(cudaMemcpyAsync(d_idx, perm.data() + b0, sizeof(int) * bn, cudaMemcpyHostToDevice, s));
+            k_gather_rows<<<bn, 64, 0, s>>>(M.d_X, d_idx, bn, kNF, d_bx);
+            k_gather_rows<<<bn, 32, 0, s>>>(M.d_y, d_idx, bn, 1, d_by);
+            k_gather_rows<<<bn, 32, 0, s>>>(d_w, d_idx, bn, 1, d_bw);
+            std::vector<float*> acts;
+            mlp_forward(M, d_bx, bn, acts, s);
+            tot += mlp_backward(M, acts, d_by, d_bw, bn, s);
+            free_acts(M, acts);
+            ++M.adam_t;
+            const float c1 = 1.0f - std::pow(b1, (float)M.adam_t), c2 = 1.0f - std::pow(b2, (float)M.adam_t);
+            k_adam<<<((int)M.nparam + 255) / 256, 256, 0, s>>>(M.d_p, M.d_g, M.d_m, M.d_v, (int)M.nparam, lr, b1, b2,
+                                                               1e-8f, c1, c2);
+            MWB_CUDA(cudaGetLastError());
+            ++nb;
+        }
+        last = tot / std::max(1, nb);
+    }
+    MWB_CUDA(cudaStreamSynchronize(s));
+    for (void* q : {(void*)d_w, (void*)d_bx, (void*)d_by, (void*)d_bw, (void*)d_idx}) dfree(ctx, q);
+    return last;
+}
+
+}  // namespace mwb

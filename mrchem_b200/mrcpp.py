@@ -30,6 +30,7 @@ _ip = ctypes.POINTER(ctypes.c_int)
 _lp = ctypes.POINTER(ctypes.c_longlong)
 _vp = ctypes.c_void_p
 _vpp = ctypes.POINTER(ctypes.c_void_p)
+_fp = ctypes.POINTER(ctypes.c_float)
 
 BASIS_INTERPOLATING = 0
 BASIS_LEGENDRE = 1
@@ -70,6 +71,19 @@ SYMBOLS = [
     ("mw_apply", ctypes.c_int, [ctypes.c_double, _vp, _vp, _vp, ctypes.c_int]),
     ("mw_apply_batched", ctypes.c_int, [ctypes.c_int, ctypes.c_double, _vpp, _vpp, _vpp, ctypes.c_int]),
     ("mw_apply_stats", ctypes.c_int, [_vp, _lp]),
+    ("mw_mlp_create", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint, _vpp]),
+    ("mw_mlp_destroy", ctypes.c_int, [_vp]),
+    ("mw_mlp_nparams", ctypes.c_int, [_vp, _lp, _ip]),
+    ("mw_mlp_get_params", ctypes.c_int, [_vp, _fp]),
+    ("mw_mlp_set_params", ctypes.c_int, [_vp, _fp]),
+    ("mw_mlp_forward", ctypes.c_int, [_vp, ctypes.c_int, _fp, _fp]),
+    ("mw_mlp_gradient", ctypes.c_int, [_vp, ctypes.c_int, _fp, _fp, _fp, _dp, _fp]),
+    ("mw_mlp_collect", ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    ("mw_mlp_dataset", ctypes.c_int, [_vp, _ip, _ip]),
+    ("mw_mlp_dataset_get", ctypes.c_int, [_vp, _fp, _fp]),
+    ("mw_mlp_train", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_uint, _dp]),
+    ("mw_apply_learned", ctypes.c_int, [ctypes.c_int, ctypes.c_double, _vpp, _vpp, _vpp, ctypes.c_int, _vp,
+                                         ctypes.c_float, _lp]),
 ]
 
 _lib = None
@@ -326,9 +340,105 @@ def apply_batched(prec, outs, ops, inps, flags=APPLY_FP64):
     return int(st[1])
 
 
+def apply_stats(out: FunctionTree):
+    """(triples of this tree or -1 after a batch, triples of the batch, refinement passes, nodes)."""
+    st = np.zeros(8, np.int64)
+    _check(_lib.mw_apply_stats(out._h, st.ctypes.data_as(_lp)))
+    return tuple(int(x) for x in st[:4])
+
+
 def apply(prec, out: FunctionTree, op: ConvolutionOperator, inp: FunctionTree, flags=APPLY_FP64):
     """out = op * inp (adaptive); returns (triples, triples_gen, passes, out_nodes)."""
     _check(_lib.mw_apply(float(prec), out._h, op._h, inp._h, int(flags)))
     st = np.zeros(4, np.int64)
     _check(_lib.mw_apply_stats(out._h, st.ctypes.data_as(_lp)))
     return tuple(int(x) for x in st)
+
+
+class ProposalNet:
+    """Learned output-tree proposal: an FP32 MLP (hidden_layers x width) on the device, trained by the
+    library's own forward/backward/Adam kernels on labels from plain applies."""
+
+    def __init__(self, ctx=None, hidden_layers=3, width=128, seed=0):
+        L = load_library()
+        self.ctx = ctx or Context.default()
+        h = ctypes.c_void_p()
+        _check(L.mw_mlp_create(self.ctx._h, int(hidden_layers), int(width), int(seed), ctypes.byref(h)))
+        self._h = h
+        n, nf = ctypes.c_longlong(), ctypes.c_int()
+        _check(L.mw_mlp_nparams(h, ctypes.byref(n), ctypes.byref(nf)))
+        self.nparams, self.nfeatures = n.value, nf.value
+        self.dims = [self.nfeatures] + [int(width)] * int(hidden_layers) + [1]
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.mw_mlp_destroy(self._h)
+            self._h = None
+
+    def params(self):
+        p = np.zeros(self.nparams, np.float32)
+        _check(_lib.mw_mlp_get_params(self._h, p.ctypes.data_as(_fp)))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        _check(_lib.mw_mlp_set_params(self._h, p.ctypes.data_as(_fp)))
+
+    def layers(self, p=None):
+        """[(W, b)] views of a parameter vector (W: out x in)."""
+        p = self.params() if p is None else p
+        out, off = [], 0
+        for i in range(len(self.dims) - 1):
+            nin, nout = self.dims[i], self.dims[i + 1]
+            W = p[off:off + nin * nout].reshape(nout, nin)
+            off += nin * nout
+            b = p[off:off + nout]
+            off += nout
+            out.append((W, b))
+        return out
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, np.float32)
+        z = np.zeros(len(x), np.float32)
+        _check(_lib.mw_mlp_forward(self._h, len(x), x.ctypes.data_as(_fp), z.ctypes.data_as(_fp)))
+        return z
+
+    def gradient(self, x, y, w):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        w = np.ascontiguousarray(w, np.float32)
+        g = np.zeros(self.nparams, np.float32)
+        loss = ctypes.c_double()
+        _check(_lib.mw_mlp_gradient(self._h, len(x), x.ctypes.data_as(_fp), y.ctypes.data_as(_fp),
+                                    w.ctypes.data_as(_fp), ctypes.byref(loss), g.ctypes.data_as(_fp)))
+        return loss.value, g
+
+    def collect(self, out, op, inp):
+        """Add the split labels of a plain apply (out = op * inp) to the training set."""
+        _check(_lib.mw_mlp_collect(self._h, out._h, op._h, inp._h))
+
+    def dataset(self, with_data=False):
+        n, npos = ctypes.c_int(), ctypes.c_int()
+        _check(_lib.mw_mlp_dataset(self._h, ctypes.byref(n), ctypes.byref(npos)))
+        if not with_data:
+            return n.value, npos.value
+        x = np.zeros((n.value, self.nfeatures), np.float32)
+        y = np.zeros(n.value, np.float32)
+        _check(_lib.mw_mlp_dataset_get(self._h, x.ctypes.data_as(_fp), y.ctypes.data_as(_fp)))
+        return x, y
+
+    def train(self, epochs=20, batch=4096, lr=1e-3, seed=0):
+        loss = ctypes.c_double()
+        _check(_lib.mw_mlp_train(self._h, int(epochs), int(batch), float(lr), int(seed), ctypes.byref(loss)))
+        return loss.value
+
+
+def apply_learned(prec, outs, ops, inps, net: ProposalNet, tau=0.5, flags=APPLY_FP64):
+    """Learned apply of a batch; same result as apply_batched.  Returns dict of statistics."""
+    n = len(outs)
+    arr = lambda objs: (ctypes.c_void_p * n)(*[o._h.value for o in objs])
+    st = np.zeros(8, np.int64)
+    _check(_lib.mw_apply_learned(n, float(prec), arr(outs), arr(ops), arr(inps), int(flags), net._h, float(tau),
+                                 st.ctypes.data_as(_lp)))
+    keys = ["triples", "passes", "proposed", "pruned", "missed", "out_nodes"]
+    return {k: int(v) for k, v in zip(keys, st[:6])}

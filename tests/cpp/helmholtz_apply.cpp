@@ -1,0 +1,41 @@
+// Drop-in check of the C++ front-end: the calls below have the shapes of the reference's call sites
+// (src/mrenv.cpp:52-66, src/scf_solver/HelmholtzVector.cpp:169-180, src/SCFDriver.cpp:279,
+// src/qmoperators/two_electron/CoulombPotential.cpp:80-85) and run on the GPU through libmwb200.so.
+#include <cmath>
+#include <cstdio>
+
+#include "mrcpp_b200.h"
+
+int main() {
+    int min_scale = -2;
+    int corner[3] = {-5, -5, -5};
+    int boxes[3] = {10, 10, 10};
+    mrcpp::BoundingBox<3> world(min_scale, corner, boxes);
+    mrcpp::InterpolatingBasis basis(7);
+    mrcpp::MultiResolutionAnalysis<3> MRA(world, basis, 14);
+
+    const double prec = 1.0e-5;
+    mrcpp::GaussExp<3> phi_f;  // a normalised Gaussian "orbital"
+    const double alpha = 3.0, pos[3] = {0.1, -0.2, 0.3};
+    phi_f.append(std::pow(2.0 * alpha / M_PI, 0.75), alpha, pos);
+    mrcpp::FunctionTree<3> phi(MRA);
+    mrcpp::project(prec, phi, phi_f);
+
+    // HelmholtzVector::apply: mu = sqrt(-2 lambda), H(MRA, mu, prec), apply, rescale(-1/2pi)
+    const double lambda = -0.5;
+    const double mu = std::sqrt(-2.0 * lambda);
+    mrcpp::HelmholtzOperator H(MRA, mu, prec);
+    mrcpp::FunctionTree<3> out(MRA);
+    mrcpp::apply(prec, out, H, phi);
+    out.rescale(-1.0 / (2.0 * M_PI));
+    std::printf("helmholtz nodes %d norm2 %.15e dot %.15e\n", out.getNNodes(), out.getSquareNorm(),
+                mrcpp::dot(out, phi));
+
+    // CoulombPotential::setupPotential: P(MRA, prec), abs_prec = prec / ||rho||, apply
+    mrcpp::PoissonOperator P(MRA, prec);
+    const double abs_prec = prec / std::sqrt(phi.getSquareNorm());
+    mrcpp::FunctionTree<3> V(MRA);
+    mrcpp::apply(abs_prec, V, P, phi);
+    std::printf("poisson nodes %d norm2 %.15e dot %.15e\n", V.getNNodes(), V.getSquareNorm(), mrcpp::dot(V, phi));
+    return 0;
+}
