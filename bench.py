@@ -109,6 +109,7 @@ def dist_env():
 
 
 def workload(rank, n, seed=2):
+    """Config-2 orbitals and Helmholtz mu for a rank (weak scaling: every rank its own batch)."""
     from mrchem_b200 import workloads as W
 
     return W.orbitals(n, seed=seed + 1000 * rank), W.helmholtz_mus(n, seed=seed + 1000 * rank)
@@ -202,10 +203,10 @@ def run_gpu(args):
         if world > 1:
             torch.distributed.barrier()
 
-    def timed(flags, outs_):
-        """W untimed + K timed steps of the batched apply with the given precision flag."""
+    def timed(run):
+        """W untimed + K timed steps of `run()` (returns the step's contracted triples)."""
         for _ in range(args.warmup):
-            G.apply_batched(args.prec, outs_, ops, inps, flags)
+            run()
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         barrier()
@@ -215,7 +216,7 @@ def run_gpu(args):
         with Clocks(local) as clk:
             ev0.record(stream)
             for _ in range(args.steps):
-                trip += G.apply_batched(args.prec, outs_, ops, inps, flags)
+                trip += run()
             ev1.record(stream)
             torch.cuda.synchronize()
         barrier()
@@ -228,17 +229,47 @@ def run_gpu(args):
             ms_ = float(tt.item())
         return ms_, trip, prof, clk.summary()
 
-    # plain FP64 (the reference method on the GPU) and the mixed path (FP32 products, FP64
-    # accumulation), same inputs, same operators
-    ms64, trip64, prof64, _ = timed(G.APPLY_FP64, outs)
+    # learned tree proposal: trained (untimed) on plain applies of a disjoint seeded orbital set
+    t_train = time.perf_counter()
+    net = G.ProposalNet(ctx=ctx, hidden_layers=3, width=128, seed=5)
+    tr_orbs, tr_mus = workload(rank, args.orbitals, seed=1000 + 7)
+    tr_in = []
+    for f in tr_orbs:
+        t = G.FunctionTree(m)
+        G.project(args.prec, t, f)
+        tr_in.append(t)
+    tr_ops = [G.HelmholtzOperator(m, mu, args.prec) for mu in tr_mus]
+    tr_out = [G.FunctionTree(m) for _ in tr_in]
+    G.apply_batched(args.prec, tr_out, tr_ops, tr_in)
+    for o, op, t in zip(tr_out, tr_ops, tr_in):
+        net.collect(o, op, t)
+    n_train, n_pos = net.dataset()
+    train_loss = net.train(epochs=40, batch=4096, lr=2e-3, seed=0)
+    del tr_in, tr_out, tr_ops
+    t_train = time.perf_counter() - t_train
+
+    # plain FP64 (the reference method on the GPU), the mixed path (FP32 products, FP64
+    # accumulation) and mixed + learned proposal, same inputs, same operators
+    ms64, trip64, prof64, _ = timed(lambda: G.apply_batched(args.prec, outs, ops, inps, G.APPLY_FP64))
     outs32 = [G.FunctionTree(m) for _ in range(args.orbitals)]
-    ms, triples, prof32, clocks = timed(G.APPLY_FP32, outs32)
+    ms32, trip32, prof32m, _ = timed(lambda: G.apply_batched(args.prec, outs32, ops, inps, G.APPLY_FP32))
+    outsL = [G.FunctionTree(m) for _ in range(args.orbitals)]
+    lstats = {}
+
+    def run_learned():
+        st = G.apply_learned(args.prec, outsL, ops, inps, net, tau=0.97, flags=G.APPLY_FP32)
+        lstats.update(st)
+        return st["triples"]
+
+    ms, triples, prof32, clocks = timed(run_learned)
     launches, apply_launches, apply_ms = prof32
-    # error of the mixed result against the FP64 one: ||g32 - g64|| / ||g64|| per orbital
+    # error of the mixed + learned result against the FP64 one: ||g - g64|| / ||g64|| per orbital
     rel_err = 0.0
-    for a, b in zip(outs32, outs):
+    same_tree = True
+    for a, b in zip(outsL, outs):
         na, nb, ab = a.square_norm(), b.square_norm(), G.dot(a, b)
         rel_err = max(rel_err, np.sqrt(max(na + nb - 2 * ab, 0.0) / nb))
+        same_tree &= a.nnodes() == b.nnodes()
     total_applies = args.orbitals * args.steps * world
     value = total_applies / (ms / 1e3)
 
@@ -257,9 +288,9 @@ def run_gpu(args):
         for i in range(args.orbitals):
             h = host[i]
             e_in[i].load(h["depth"], h["trans"], h["parent"], h["child0"], h["coef"])
-        G.apply_batched(args.prec, outs32, ops, e_in, G.APPLY_FP32)
+        G.apply_learned(args.prec, outsL, ops, e_in, net, tau=0.97, flags=G.APPLY_FP32)
         for i in range(args.orbitals):
-            res = outs32[i].export()
+            res = outsL[i].export()
             d2h += sum(v.nbytes for v in res.values() if v is not None)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
@@ -293,15 +324,23 @@ def run_gpu(args):
             "vs_baseline": None, "dtype": "f32 products, f64 accumulation", "data": "synthetic",
             "config": {"workload": "helmholtz_batch_32orb_k10_prec1e-6", "orbitals": args.orbitals,
                        "order": args.order, "k": k, "prec": args.prec, "mu": "U[0.5,3]", "world": "[-20,20]^3",
-                       "path": "mixed: FP32 products, FP64 accumulation; batched passes", "parallelism": f"replicas x{world}",
+                       "path": "mixed (FP32 products, FP64 accumulation) + learned tree proposal; batched", "parallelism": f"replicas x{world}",
                        "l2": f"inputs larger than L2 ({in_bytes / 1e9:.2f} GB of input blocks per step)"},
             "e2e": {"value": e2e_val, "unit": "applies/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "plain_fp64": {"value": args.orbitals * args.steps * world / (ms64 / 1e3), "unit": "applies/s",
                            "ms_per_step": ms64 / args.steps, "kernel_ms_per_step": prof64[2] / args.steps,
                            "triples_per_step": trip64 // max(1, args.steps)},
+            "mixed_no_learning": {"value": args.orbitals * args.steps * world / (ms32 / 1e3), "unit": "applies/s",
+                                  "ms_per_step": ms32 / args.steps, "kernel_ms_per_step": prof32m[2] / args.steps},
             "speedup_vs_plain_fp64": ms64 / ms,
             "rel_error_vs_fp64": rel_err,
+            "same_node_count_as_fp64": bool(same_tree),
+            "learned": {"passes": lstats.get("passes"), "proposed": lstats.get("proposed"),
+                        "pruned": lstats.get("pruned"), "missed": lstats.get("missed"),
+                        "out_nodes": lstats.get("out_nodes"), "train_rows": n_train, "train_positive": n_pos,
+                        "train_loss": train_loss, "train_s": t_train,
+                        "train_data": "plain applies of 32 other seeded orbitals (seed 1007)"},
             "roofline": {"bound": "tensor", "kernel": "k_bapply<10,float>", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if not peaks.get("_fallback")

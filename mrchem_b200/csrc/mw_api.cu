@@ -147,27 +147,19 @@ static int* range_list(Ctx* ctx, int begin, int end) {
 
 // bottom-up: every internal node becomes the compression of its children's scaling parts
 static void tree_compress_bottom_up(Tree& t) {
-    Ctx* ctx = t.mra->ctx;
-    cudaStream_t s = ctx->stream;
+    cudaStream_t s = t.mra->ctx->stream;
     for (int d = t.levels() - 2; d >= 0; --d) {
         const int b = t.level_begin[d], e = t.level_begin[d + 1];
-        int* d_list = (int*)dalloc(ctx, sizeof(int) * (e - b));
-        int ni = launch_internal_list(t, b, e, d_list, s);
-        launch_transform_nodes(t, TM_COMPRESS, d_list, ni, nullptr, s);
-        dfree(ctx, d_list);
+        launch_transform_nodes(t, TM_COMPRESS, nullptr, e - b, nullptr, s, b);
     }
 }
 
 // top-down sum-up of an NS-form output: children's scaling parts += reconstruction of the parent
 static void tree_sumup_top_down(Tree& t) {
-    Ctx* ctx = t.mra->ctx;
-    cudaStream_t s = ctx->stream;
+    cudaStream_t s = t.mra->ctx->stream;
     for (int d = 0; d + 1 < t.levels(); ++d) {
         const int b = t.level_begin[d], e = t.level_begin[d + 1];
-        int* d_list = (int*)dalloc(ctx, sizeof(int) * (e - b));
-        int ni = launch_internal_list(t, b, e, d_list, s);
-        launch_transform_nodes(t, TM_SUMUP, d_list, ni, nullptr, s);
-        dfree(ctx, d_list);
+        launch_transform_nodes(t, TM_SUMUP, nullptr, e - b, nullptr, s, b);
     }
 }
 
@@ -433,21 +425,35 @@ static void op_init(Op& op, Mra* m, double mu, double prec) {
 // apply
 // ---------------------------------------------------------------------------------------------
 
-static void tree_add_children(Tree& t, const std::vector<int>& list) {
-    const int ns = (int)list.size();
-    if (ns == 0) return;
-    Ctx* ctx = t.mra->ctx;
+// append the 8 children of every listed node, for several trees, with one synchronisation
+static void add_children_many(const std::vector<Tree*>& ts, const std::vector<std::vector<int>>& lists) {
+    if (ts.empty()) return;
+    Ctx* ctx = ts[0]->mra->ctx;
     cudaStream_t s = ctx->stream;
-    tree_reserve(t, t.n + 8 * ns);
-    int* d_list = (int*)dalloc(ctx, sizeof(int) * ns);
-    MWB_CUDA(cudaMemcpyAsync(d_list, list.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, s));
-    launch_make_children(t, d_list, ns, s);
-    launch_hash_insert(t, t.n, t.n + 8 * ns, s);
+    size_t tot = 0;
+    for (auto& l : lists) tot += l.size();
+    if (tot == 0) return;
+    std::vector<int> flat;
+    flat.reserve(tot);
+    for (auto& l : lists) flat.insert(flat.end(), l.begin(), l.end());
+    int* d_list = (int*)dalloc(ctx, sizeof(int) * tot);
+    MWB_CUDA(cudaMemcpyAsync(d_list, flat.data(), sizeof(int) * tot, cudaMemcpyHostToDevice, s));
+    size_t off = 0;
+    for (size_t i = 0; i < ts.size(); ++i) {
+        Tree& t = *ts[i];
+        const int ns = (int)lists[i].size();
+        if (ns == 0) continue;
+        tree_reserve(t, t.n + 8 * ns);
+        launch_make_children(t, d_list + off, ns, s);
+        launch_hash_insert(t, t.n, t.n + 8 * ns, s);
+        t.n += 8 * ns;
+        t.level_begin.push_back(t.n);
+        off += ns;
+    }
     MWB_CUDA(cudaStreamSynchronize(s));
     dfree(ctx, d_list);
-    t.n += 8 * ns;
-    t.level_begin.push_back(t.n);
 }
+
 
 // Adaptive NS-form apply of a batch: out[i] = op[i] * inp[i], all trees on one world.  The passes
 // run in lock-step over the batch (one launch per stage for all trees of a depth).
@@ -470,10 +476,15 @@ static void apply_batched(double prec, int n, Tree** out, Op** op, Tree** inp, i
     long long total_trip = 0;
     std::vector<int> passes(n, 0);
     std::vector<bool> active(n, true);
-    for (int i = 0; i < n; ++i) {
-        tree_make_roots(*out[i]);
-        fnorm[i] = std::sqrt(reduce_leaf_norm2(*inp[i], s));
-        nu_max[i] = std::sqrt(reduce_max_norm2(*inp[i], s));
+    {
+        std::vector<Tree*> ins(inp, inp + n);
+        std::vector<double> l2, m2;
+        reduce_norms_many(ins, l2, m2, s);
+        for (int i = 0; i < n; ++i) {
+            tree_make_roots(*out[i]);
+            fnorm[i] = std::sqrt(l2[i]);
+            nu_max[i] = std::sqrt(m2[i]);
+        }
     }
     for (int depth = 0;; ++depth) {
         BatchPass bp;
@@ -507,6 +518,8 @@ static void apply_batched(double prec, int n, Tree** out, Op** op, Tree** inp, i
         }
         if (bp.trees.empty()) break;
         run_batch_pass(bp, s);
+        std::vector<Tree*> grow;
+        std::vector<std::vector<int>> lists;
         for (size_t q = 0; q < idx.size(); ++q) {
             const int i = idx[q];
             ++passes[i];
@@ -515,8 +528,10 @@ static void apply_batched(double prec, int n, Tree** out, Op** op, Tree** inp, i
                 active[i] = false;
                 continue;
             }
-            tree_add_children(*out[i], bp.split_lists[q]);
+            grow.push_back(out[i]);
+            lists.push_back(bp.split_lists[q]);
         }
+        add_children_many(grow, lists);
         total_trip += bp.triples;
     }
     for (int i = 0; i < n; ++i) {
@@ -602,11 +617,16 @@ static void apply_learned(double prec, int n, Tree** out, Op** op, Tree** inp, i
     long long trip = 0, proposed = 0, pruned = 0, missed = 0;
     int passes = 0;
     std::vector<Entry> ents;
-    for (int i = 0; i < n; ++i) {
-        tree_make_roots(*out[i]);
-        fnorm[i] = std::sqrt(reduce_leaf_norm2(*inp[i], s));
-        nu_max[i] = std::sqrt(reduce_max_norm2(*inp[i], s));
-        ents.push_back(Entry{i, 0, 0, out[i]->n});
+    {
+        std::vector<Tree*> ins(inp, inp + n);
+        std::vector<double> l2, m2;
+        reduce_norms_many(ins, l2, m2, s);
+        for (int i = 0; i < n; ++i) {
+            tree_make_roots(*out[i]);
+            fnorm[i] = std::sqrt(l2[i]);
+            nu_max[i] = std::sqrt(m2[i]);
+            ents.push_back(Entry{i, 0, 0, out[i]->n});
+        }
     }
     // exact root pass (sets g0)
     {
@@ -633,17 +653,19 @@ static void apply_learned(double prec, int n, Tree** out, Op** op, Tree** inp, i
         run_batch_pass(bp, s);
         trip += bp.triples;
         ++passes;
+        std::vector<Tree*> rt(out, out + n);
+        std::vector<std::vector<int>> rl(n);
         for (int i = 0; i < n; ++i) {
             g0[i] = bp.trees[i].g0;
-            if (g0[i] > 0.0) tree_add_children(*out[i], bp.split_lists[i]);
+            if (g0[i] > 0.0) rl[i] = bp.split_lists[i];
         }
+        add_children_many(rt, rl);
     }
     // proposal: level by level, the network decides which nodes will split
-    std::vector<double*> rootw(n, nullptr);
-    for (int i = 0; i < n; ++i) rootw[i] = root_wnorms(*out[i]);
     std::vector<FeatCtx> fc(n);
-    for (int i = 0; i < n; ++i) fc[i] = FeatCtx{out[i], inp[i], op[i], prec, g0[i], rootw[i]};
+    for (int i = 0; i < n; ++i) fc[i] = FeatCtx{out[i], inp[i], op[i], prec, g0[i]};
     std::vector<long long> budget_used(n, 0);
+    std::vector<Tree*> all(out, out + n);
     for (int depth = 1;; ++depth) {
         std::vector<int2> items;
         for (int i = 0; i < n; ++i) {
@@ -663,14 +685,11 @@ static void apply_learned(double prec, int n, Tree** out, Op** op, Tree** inp, i
             const long long room = 2LL * inp[i]->n - budget_used[i];
             if ((long long)lists[i].size() * 8 > room) lists[i].resize(std::max(0LL, room / 8));
             budget_used[i] += 8LL * (long long)lists[i].size();
+            proposed += 8LL * (long long)lists[i].size();
+            any |= !lists[i].empty();
         }
-        for (int i = 0; i < n; ++i)
-            if (!lists[i].empty()) {
-                tree_add_children(*out[i], lists[i]);
-                proposed += 8 * (long long)lists[i].size();
-                any = true;
-            }
         if (!any) break;
+        add_children_many(all, lists);
     }
     // compute every node below the root level in one pass set
     ents.clear();
@@ -682,74 +701,91 @@ static void apply_learned(double prec, int n, Tree** out, Op** op, Tree** inp, i
         trip += run_entries(prec, precision, ents, out, op, inp, fnorm, nu_max, g0);
         ++passes;
     }
-    // exact criterion on every computed node, top-down; prune extras, refine misses
-    for (int iter = 0;; ++iter) {
-        std::vector<Entry> next;
+    // exact criterion on every computed node, top-down from the roots: nodes below a node the
+    // criterion does not split are dropped (they stay in the arrays until the final rebuild), splits
+    // without children are refined by further passes
+    std::vector<std::vector<char>> keeps(n);
+    std::vector<std::vector<uint64_t>> keys(n);
+    std::vector<long long> computed(n);
+    for (int i = 0; i < n; ++i) computed[i] = out[i]->n;
+    for (;;) {
+        std::vector<std::vector<double>> w2(n);
+        std::vector<std::vector<int>> c0(n);
         for (int i = 0; i < n; ++i) {
             Tree& t = *out[i];
-            const int nn = t.n;
-            std::vector<double> w2(nn);
-            std::vector<int> c0(nn);
-            std::vector<uint64_t> key(nn);
-            MWB_CUDA(cudaMemcpyAsync(w2.data(), t.wnorm2, sizeof(double) * nn, cudaMemcpyDeviceToHost, s));
-            MWB_CUDA(cudaMemcpyAsync(c0.data(), t.child0, sizeof(int) * nn, cudaMemcpyDeviceToHost, s));
-            MWB_CUDA(cudaMemcpyAsync(key.data(), t.key, sizeof(uint64_t) * nn, cudaMemcpyDeviceToHost, s));
-            MWB_CUDA(cudaStreamSynchronize(s));
-            std::vector<char> keep(nn, 0);
-            std::vector<uint64_t> miss;
+            w2[i].resize(t.n);
+            c0[i].resize(t.n);
+            keys[i].resize(t.n);
+            MWB_CUDA(cudaMemcpyAsync(w2[i].data(), t.wnorm2, sizeof(double) * t.n, cudaMemcpyDeviceToHost, s));
+            MWB_CUDA(cudaMemcpyAsync(c0[i].data(), t.child0, sizeof(int) * t.n, cudaMemcpyDeviceToHost, s));
+            MWB_CUDA(cudaMemcpyAsync(keys[i].data(), t.key, sizeof(uint64_t) * t.n, cudaMemcpyDeviceToHost, s));
+        }
+        MWB_CUDA(cudaStreamSynchronize(s));
+        std::vector<std::vector<int>> lists(n);
+        std::vector<std::vector<uint64_t>> misses(n);
+        bool any = false;
+        for (int i = 0; i < n; ++i) {
+            const Tree& t = *out[i];
+            keeps[i].assign(t.n, 0);
             std::vector<int> stack;
             for (int q = 0; q < t.level_begin[1]; ++q) stack.push_back(q);
             while (!stack.empty()) {
                 const int q = stack.back();
                 stack.pop_back();
-                keep[q] = 1;
-                const int d = (int)(key[q] >> 59);
-                const bool split = d < m->depth_limit && std::sqrt(w2[q]) > split_threshold(prec, g0[i], d);
-                if (split) {
-                    if (c0[q] >= 0)
-                        for (int c = 0; c < 8; ++c) stack.push_back(c0[q] + c);
+                keeps[i][q] = 1;
+                const int d = (int)(keys[i][q] >> 59);
+                if (d < m->depth_limit && std::sqrt(w2[i][q]) > split_threshold(prec, g0[i], d)) {
+                    if (c0[i][q] >= 0)
+                        for (int c = 0; c < 8; ++c) stack.push_back(c0[i][q] + c);
                     else
-                        miss.push_back(key[q]);
+                        lists[i].push_back(q);
                 }
             }
-            long long nk = 0;
-            for (char k : keep) nk += k;
-            if (nk < nn) {
-                pruned += nn - nk;
-                tree_rebuild(t, keep);
-            } else if (iter > 0) {
-                tree_rebuild(t, keep);  // restore (depth, Morton) order after appended refinements
-            }
-            if (!miss.empty()) {
-                missed += (long long)miss.size();
-                std::sort(miss.begin(), miss.end());  // depth-major: children come out grouped by depth
-                std::vector<uint64_t> k2(t.n);
-                MWB_CUDA(cudaMemcpyAsync(k2.data(), t.key, sizeof(uint64_t) * t.n, cudaMemcpyDeviceToHost, s));
-                MWB_CUDA(cudaStreamSynchronize(s));
-                std::unordered_map<uint64_t, int> pos;
-                for (int q = 0; q < t.n; ++q) pos[k2[q]] = q;
-                std::vector<int> list;
-                for (uint64_t k : miss) list.push_back(pos.at(k));
-                const int base = t.n;
-                tree_add_children(t, list);
-                // one entry per depth of the appended children
-                int b = base;
-                for (size_t q = 0; q < miss.size();) {
-                    const int d = (int)(miss[q] >> 59) + 1;
-                    size_t r = q;
-                    while (r < miss.size() && (int)(miss[r] >> 59) + 1 == d) ++r;
-                    next.push_back(Entry{i, d, b, b + 8 * (int)(r - q)});
-                    b += 8 * (int)(r - q);
-                    q = r;
-                }
-            }
+            // depth-major order: the appended children come out grouped by depth
+            std::sort(lists[i].begin(), lists[i].end(), [&](int a, int b) { return keys[i][a] < keys[i][b]; });
+            missed += (long long)lists[i].size();
+            any |= !lists[i].empty();
         }
-        if (next.empty()) break;
+        if (!any) break;
+        std::vector<int> base(n);
+        for (int i = 0; i < n; ++i) base[i] = out[i]->n;
+        add_children_many(all, lists);
+        std::vector<Entry> next;
+        for (int i = 0; i < n; ++i) {
+            int b = base[i];
+            for (size_t q = 0; q < lists[i].size();) {
+                const int d = (int)(keys[i][lists[i][q]] >> 59) + 1;
+                size_t r = q;
+                while (r < lists[i].size() && (int)(keys[i][lists[i][r]] >> 59) + 1 == d) ++r;
+                next.push_back(Entry{i, d, b, b + 8 * (int)(r - q)});
+                b += 8 * (int)(r - q);
+                q = r;
+            }
+            computed[i] = out[i]->n;
+        }
         trip += run_entries(prec, precision, next, out, op, inp, fnorm, nu_max, g0);
         ++passes;
     }
+    // one rebuild of every tree whose arrays hold dropped nodes or appended refinements
+    {
+        std::vector<Tree*> ts;
+        std::vector<std::vector<char>> kk;
+        std::vector<std::vector<uint64_t>> ky;
+        for (int i = 0; i < n; ++i) {
+            long long nk = 0;
+            for (char k : keeps[i]) nk += k;
+            pruned += computed[i] - nk;
+            const bool sorted_levels = nk == out[i]->n && (int)keys[i].size() == out[i]->n &&
+                                       std::is_sorted(keys[i].begin(), keys[i].end());
+            if (!sorted_levels) {
+                ts.push_back(out[i]);
+                kk.push_back(keeps[i]);
+                ky.push_back(keys[i]);
+            }
+        }
+        trees_rebuild(ts, kk, ky);
+    }
     for (int i = 0; i < n; ++i) {
-        dfree(ctx, rootw[i]);
         tree_sumup_top_down(*out[i]);
         tree_compress_bottom_up(*out[i]);
         launch_node_norms(*out[i], 0, out[i]->n, s);
@@ -778,8 +814,7 @@ static void collect_training(Mlp& M, Tree& out, Op& op, Tree& inp) {
     if (out.n == 0 || out.levels() < 2) return;
     Ctx* ctx = out.mra->ctx;
     cudaStream_t s = ctx->stream;
-    double* rw = root_wnorms(out);
-    std::vector<FeatCtx> fc{FeatCtx{&out, &inp, &op, out.prec, out.g0, rw}};
+    std::vector<FeatCtx> fc{FeatCtx{&out, &inp, &op, out.prec, out.g0}};
     std::vector<int2> items;
     std::vector<int> c0(out.n);
     MWB_CUDA(cudaMemcpyAsync(c0.data(), out.child0, sizeof(int) * out.n, cudaMemcpyDeviceToHost, s));
@@ -792,7 +827,6 @@ static void collect_training(Mlp& M, Tree& out, Op& op, Tree& inp) {
     float* d_F = features(ctx, fc, items, s);
     mlp_append(M, d_F, y, s);
     dfree(ctx, d_F);
-    dfree(ctx, rw);
 }
 
 }  // namespace mwb

@@ -129,14 +129,18 @@ struct WorldGeo {
 constexpr int kTransformThreads = 256;
 
 template <int K>
-__global__ void __launch_bounds__(kTransformThreads) k_transform(int mode, const int* __restrict__ nodes, TView t, const double* __restrict__ Mg,
-                            FuncDesc f, WorldGeo wg) {
+__global__ void __launch_bounds__(kTransformThreads) k_transform(int mode, const int* __restrict__ nodes, int begin,
+                                                                 TView t, const double* __restrict__ Mg, FuncDesc f,
+                                                                 WorldGeo wg) {
     using G = Geo<K>;
     extern __shared__ double sm[];
     double* A = sm;
     double* M = A + G::VOL;
     double* red = M + G::K2 * G::K2;
-    const int node = nodes[blockIdx.x];
+    // node list, or (nodes == nullptr) the range begin + blockIdx.x, where leaves have nothing to do
+    // for the compress / sum-up modes (the whole block leaves together, before any barrier)
+    const int node = nodes ? nodes[blockIdx.x] : begin + blockIdx.x;
+    if (!nodes && mode != TM_PROJECT && t.child0[node] < 0) return;
     for (int i = threadIdx.x; i < G::K2 * G::K2; i += blockDim.x) M[i] = Mg[i];
     double fac = 1.0;
     if (mode == TM_PROJECT) {
@@ -355,8 +359,8 @@ static WorldGeo world_geo(const Mra& m) {
     return g;
 }
 
-void launch_transform_nodes(Tree& t, int mode, const int* d_nodes, int nnodes, const FuncDesc* f,
-                            cudaStream_t s) {
+void launch_transform_nodes(Tree& t, int mode, const int* d_nodes, int nnodes, const FuncDesc* f, cudaStream_t s,
+                            int begin) {
     if (nnodes <= 0) return;
     const Mra& m = *t.mra;
     const double* M = (mode == TM_PROJECT) ? m.d_PF : (mode == TM_COMPRESS ? m.d_F : m.d_FT);
@@ -368,7 +372,7 @@ void launch_transform_nodes(Tree& t, int mode, const int* d_nodes, int nnodes, c
         size_t smem = sizeof(double) * (Geo<KK>::VOL + 4 * KK * KK + 64);                            \
         MWB_CUDA(cudaFuncSetAttribute(k_transform<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
                                       (int)smem));                                                    \
-        k_transform<KK><<<nnodes, kTransformThreads, smem, s>>>(mode, d_nodes, tv, M, fd, wg);          \
+        k_transform<KK><<<nnodes, kTransformThreads, smem, s>>>(mode, d_nodes, begin, tv, M, fd, wg);   \
     }
     MWB_DISPATCH_K(m.k, L_TR)
 #undef L_TR
@@ -469,6 +473,33 @@ static double reduce_impl(Tree& t, int begin, int end, int leaves, int mx, cudaS
     return h;
 }
 double reduce_leaf_norm2(Tree& t, cudaStream_t s) { return reduce_impl(t, 0, t.n, 1, 0, s); }
+
+// squared norm (leaves) and largest node norm^2 of several trees with one synchronisation
+void reduce_norms_many(const std::vector<Tree*>& ts, std::vector<double>& leaf2, std::vector<double>& max2,
+                       cudaStream_t s) {
+    const int n = (int)ts.size();
+    leaf2.assign(n, 0.0);
+    max2.assign(n, 0.0);
+    if (n == 0) return;
+    Ctx* ctx = ts[0]->mra->ctx;
+    double* d = (double*)dalloc(ctx, sizeof(double) * 2 * n);
+    MWB_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * 2 * n, s));
+    for (int i = 0; i < n; ++i) {
+        if (ts[i]->n == 0) continue;
+        k_reduce_norm2<<<1, 1024, 0, s>>>(ts[i]->norm2, ts[i]->child0, 0, ts[i]->n, 1, 0, d + i);
+        k_reduce_norm2<<<1, 1024, 0, s>>>(ts[i]->norm2, ts[i]->child0, 0, ts[i]->n, 0, 1, d + n + i);
+        count(ctx, 2);
+    }
+    MWB_CUDA(cudaGetLastError());
+    std::vector<double> h(2 * n);
+    MWB_CUDA(cudaMemcpyAsync(h.data(), d, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
+    dfree(ctx, d);
+    for (int i = 0; i < n; ++i) {
+        leaf2[i] = h[i];
+        max2[i] = h[n + i];
+    }
+}
 double reduce_range_norm2(Tree& t, int begin, int end, cudaStream_t s) { return reduce_impl(t, begin, end, 0, 0, s); }
 double reduce_max_norm2(Tree& t, cudaStream_t s) { return reduce_impl(t, 0, t.n, 0, 1, s); }
 

@@ -30,8 +30,9 @@ struct InView {
     const double* norm2;
 };
 
-void launch_transform_nodes(Tree& t, int mode, const int* d_nodes, int nnodes, const FuncDesc* f,
-                            cudaStream_t s);
+// d_nodes == nullptr: the node range [begin, begin + nnodes) (compress / sum-up skip leaves)
+void launch_transform_nodes(Tree& t, int mode, const int* d_nodes, int nnodes, const FuncDesc* f, cudaStream_t s,
+                            int begin = 0);
 void launch_node_norms(Tree& t, int begin, int end, cudaStream_t s);
 void launch_hash_reset(Tree& t, cudaStream_t s);
 void launch_hash_insert(Tree& t, int begin, int end, cudaStream_t s);
@@ -47,6 +48,8 @@ int launch_internal_list(Tree& t, int begin, int end, int* d_list, cudaStream_t 
 double reduce_leaf_norm2(Tree& t, cudaStream_t s);
 double reduce_range_norm2(Tree& t, int begin, int end, cudaStream_t s);
 double reduce_max_norm2(Tree& t, cudaStream_t s);
+void reduce_norms_many(const std::vector<Tree*>& ts, std::vector<double>& leaf2, std::vector<double>& max2,
+                       cudaStream_t s);
 void launch_rescale(Tree& t, double c, cudaStream_t s);
 double launch_dot(Tree& a, Tree& b, cudaStream_t s);
 

@@ -40,7 +40,10 @@ struct FeatTree {
     const uint64_t* hkey;
     const int* hval;
     uint32_t hcap;
-    const double* root_w;   // output root-node wavelet norms^2 (exact pass), indexed by root order
+    const double* owind2;   // output wavelet norms^2 (the root nodes' are exact after the root pass)
+    const uint64_t* ohkey;  // output hash index (root lookup)
+    const int* ohval;
+    uint32_t ohcap;
     int n0;
     int boxes[3];
     double thr0;            // split threshold at depth 0 (prec * g0)
@@ -50,8 +53,7 @@ struct FeatTree {
 __device__ inline float lg(double v) { return (float)(log10(v + 1e-30) * 0.1); }
 
 // one thread per (entry, node): writes kNF features
-__global__ void k_features(const int2* __restrict__ items, int n, const FeatTree* __restrict__ trees,
-                           const int* __restrict__ root_index, float* F) {
+__global__ void k_features(const int2* __restrict__ items, int n, const FeatTree* __restrict__ trees, float* F) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int2 it = items[i];
@@ -94,8 +96,8 @@ __global__ void k_features(const int2* __restrict__ items, int n, const FeatTree
     f[60] = (float)log10(edge);
     f[61] = (float)log10(T.mu * edge + 1e-3);
     f[62] = lg(thr);
-    const int r = root_index ? root_index[i] : -1;
-    f[63] = r >= 0 ? lg(sqrt(T.root_w[r]) / T.thr0) : 0.0f;
+    const int r = hlookup(T.ohkey, T.ohval, T.ohcap, make_key(0, t[0] >> d, t[1] >> d, t[2] >> d));
+    f[63] = r >= 0 ? lg(sqrt(T.owind2[r]) / T.thr0) : 0.0f;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -309,6 +311,8 @@ std::vector<float> mlp_logits(Mlp& M, const float* d_X, int N, cudaStream_t s) {
 // ---------------------------------------------------------------------------------------------
 float* features(Ctx* ctx, std::vector<FeatCtx>& fc, const std::vector<int2>& items, cudaStream_t s) {
     const int n = (int)items.size();
+    float* d_F = (float*)dalloc(ctx, sizeof(float) * (size_t)std::max(1, n) * kNF);
+    if (n == 0) return d_F;
     std::vector<FeatTree> ft(fc.size());
     for (size_t t = 0; t < fc.size(); ++t) {
         FeatCtx& c = fc[t];
@@ -321,62 +325,26 @@ float* features(Ctx* ctx, std::vector<FeatCtx>& fc, const std::vector<int2>& ite
         f.hkey = c.inp->hkey;
         f.hval = c.inp->hval;
         f.hcap = c.inp->hcap;
-        f.root_w = c.d_root_w;
+        f.owind2 = c.out->wnorm2;
+        f.ohkey = c.out->hkey;
+        f.ohval = c.out->hval;
+        f.ohcap = c.out->hcap;
         f.n0 = m.n0;
         for (int q = 0; q < 3; ++q) f.boxes[q] = m.boxes[q];
         f.thr0 = c.prec * c.g0;
         f.mu = c.op->mu;
         f.prec = c.prec;
     }
-    // root ancestor index of each node (roots are the first nodes of every output tree, Morton order)
-    std::vector<int> root_index(n, -1);
-    float* d_F = (float*)dalloc(ctx, sizeof(float) * (size_t)std::max(1, n) * kNF);
-    if (n == 0) return d_F;
     FeatTree* d_ft = (FeatTree*)dalloc(ctx, sizeof(FeatTree) * ft.size());
     int2* d_items = (int2*)dalloc(ctx, sizeof(int2) * n);
-    int* d_ri = (int*)dalloc(ctx, sizeof(int) * n);
     MWB_CUDA(cudaMemcpyAsync(d_ft, ft.data(), sizeof(FeatTree) * ft.size(), cudaMemcpyHostToDevice, s));
     MWB_CUDA(cudaMemcpyAsync(d_items, items.data(), sizeof(int2) * n, cudaMemcpyHostToDevice, s));
-    // root ancestor: follow parents on the host copy is costly; use the key (root translation = t >> depth)
-    {
-        std::vector<std::vector<uint64_t>> keys(fc.size());
-        for (size_t t = 0; t < fc.size(); ++t) {
-            keys[t].resize(fc[t].out->n);
-            MWB_CUDA(cudaMemcpyAsync(keys[t].data(), fc[t].out->key, sizeof(uint64_t) * fc[t].out->n,
-                                     cudaMemcpyDeviceToHost, s));
-        }
-        MWB_CUDA(cudaStreamSynchronize(s));
-        for (size_t t = 0; t < fc.size(); ++t) {
-            const int nroot = fc[t].out->level_begin.size() > 1 ? fc[t].out->level_begin[1] : 0;
-            std::unordered_map<uint64_t, int> rmap;
-            for (int r = 0; r < nroot; ++r) rmap[keys[t][r]] = r;
-            for (int i = 0; i < n; ++i) {
-                if (items[i].x != (int)t) continue;
-                const uint64_t k = keys[t][items[i].y];
-                const int d = (int)(k >> 59);
-                long long tr[3];
-                host_key_trans(k, tr);
-                auto it = rmap.find(host_make_key(0, tr[0] >> d, tr[1] >> d, tr[2] >> d));
-                root_index[i] = it == rmap.end() ? -1 : it->second;
-            }
-        }
-    }
-    MWB_CUDA(cudaMemcpyAsync(d_ri, root_index.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
-    k_features<<<(n + 127) / 128, 128, 0, s>>>(d_items, n, d_ft, d_ri, d_F);
+    k_features<<<(n + 127) / 128, 128, 0, s>>>(d_items, n, d_ft, d_F);
     MWB_CUDA(cudaGetLastError());
-    MWB_CUDA(cudaStreamSynchronize(s));
+    MWB_CUDA(cudaStreamSynchronize(s));  // ft / items leave scope
     dfree(ctx, d_ft);
     dfree(ctx, d_items);
-    dfree(ctx, d_ri);
     return d_F;
-}
-
-double* root_wnorms(Tree& out) {
-    Ctx* ctx = out.mra->ctx;
-    const int nroot = out.level_begin[1];
-    double* d = (double*)dalloc(ctx, sizeof(double) * nroot);
-    MWB_CUDA(cudaMemcpyAsync(d, out.wnorm2, sizeof(double) * nroot, cudaMemcpyDeviceToDevice, ctx->stream));
-    return d;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -423,60 +391,72 @@ __global__ void k_gather_nodes(const double* __restrict__ coef, const double* __
     }
 }
 
-// rebuild `t` with the nodes whose keep flag is set (the kept set must be a tree: every kept node's
-// parent kept, siblings kept together); nodes are reordered by key (parents before children)
-void tree_rebuild(Tree& t, const std::vector<char>& keep) {
-    Ctx* ctx = t.mra->ctx;
+// Rebuild each tree keeping the nodes whose flag is set (every kept node's parent kept, siblings kept
+// together), reordered by key so that parents precede children; keys[i] are the trees' current
+// node keys (host copies).  All trees are rebuilt with one synchronisation.
+void trees_rebuild(const std::vector<Tree*>& ts, const std::vector<std::vector<char>>& keeps,
+                   const std::vector<std::vector<uint64_t>>& keys) {
+    if (ts.empty()) return;
+    Ctx* ctx = ts[0]->mra->ctx;
     cudaStream_t s = ctx->stream;
-    const int n = t.n;
-    std::vector<uint64_t> key(n);
-    MWB_CUDA(cudaMemcpyAsync(key.data(), t.key, sizeof(uint64_t) * n, cudaMemcpyDeviceToHost, s));
-    MWB_CUDA(cudaStreamSynchronize(s));
-    std::vector<int> perm;
-    for (int i = 0; i < n; ++i)
-        if (keep[i]) perm.push_back(i);
-    std::sort(perm.begin(), perm.end(), [&](int a, int b) { return key[a] < key[b]; });
-    const int nn = (int)perm.size();
-    std::unordered_map<uint64_t, int> pos;
-    pos.reserve(nn * 2);
-    for (int i = 0; i < nn; ++i) pos[key[perm[i]]] = i;
-    std::vector<int> parent(nn, -1), child0(nn, -1);
-    int maxd = 0;
-    for (int i = 0; i < nn; ++i) {
-        const uint64_t k = key[perm[i]];
-        const int d = (int)(k >> 59);
-        maxd = std::max(maxd, d);
-        long long tr[3];
-        host_key_trans(k, tr);
-        if (d > 0) parent[i] = pos.at(host_make_key(d - 1, tr[0] >> 1, tr[1] >> 1, tr[2] >> 1));
-        auto it = pos.find(host_make_key(d + 1, 2 * tr[0], 2 * tr[1], 2 * tr[2]));
-        if (it != pos.end()) child0[i] = it->second;
+    const size_t BS = ts[0]->mra->bsize();
+    struct Host {
+        std::vector<int> perm, parent, child0;
+        int* d_perm;
+        double *ncoef, *nn2, *nw2;
+        uint64_t* nkey;
+    };
+    std::vector<Host> H(ts.size());
+    for (size_t q = 0; q < ts.size(); ++q) {
+        Tree& t = *ts[q];
+        const std::vector<uint64_t>& key = keys[q];
+        Host& h = H[q];
+        for (int i = 0; i < t.n; ++i)
+            if (keeps[q][i]) h.perm.push_back(i);
+        std::sort(h.perm.begin(), h.perm.end(), [&](int a, int b) { return key[a] < key[b]; });
+        const int nn = (int)h.perm.size();
+        std::unordered_map<uint64_t, int> pos;
+        pos.reserve(2 * nn);
+        for (int i = 0; i < nn; ++i) pos[key[h.perm[i]]] = i;
+        h.parent.assign(nn, -1);
+        h.child0.assign(nn, -1);
+        int maxd = 0;
+        for (int i = 0; i < nn; ++i) {
+            const uint64_t k = key[h.perm[i]];
+            const int d = (int)(k >> 59);
+            maxd = std::max(maxd, d);
+            long long tr[3];
+            host_key_trans(k, tr);
+            if (d > 0) h.parent[i] = pos.at(host_make_key(d - 1, tr[0] >> 1, tr[1] >> 1, tr[2] >> 1));
+            auto it = pos.find(host_make_key(d + 1, 2 * tr[0], 2 * tr[1], 2 * tr[2]));
+            if (it != pos.end()) h.child0[i] = it->second;
+        }
+        std::vector<int> lb(maxd + 2, 0);
+        for (int i = 0; i < nn; ++i) lb[(key[h.perm[i]] >> 59) + 1]++;
+        for (size_t d = 1; d < lb.size(); ++d) lb[d] += lb[d - 1];
+        h.d_perm = (int*)dalloc(ctx, sizeof(int) * std::max(1, nn));
+        h.ncoef = (double*)dalloc(ctx, sizeof(double) * BS * std::max(1, nn));
+        h.nn2 = (double*)dalloc(ctx, sizeof(double) * std::max(1, nn));
+        h.nw2 = (double*)dalloc(ctx, sizeof(double) * std::max(1, nn));
+        h.nkey = (uint64_t*)dalloc(ctx, sizeof(uint64_t) * std::max(1, nn));
+        MWB_CUDA(cudaMemcpyAsync(h.d_perm, h.perm.data(), sizeof(int) * nn, cudaMemcpyHostToDevice, s));
+        k_gather_nodes<<<nn, 256, 0, s>>>(t.coef, t.norm2, t.wnorm2, t.key, h.d_perm, nn, BS, h.ncoef, h.nn2, h.nw2,
+                                          h.nkey);
+        MWB_CUDA(cudaGetLastError());
+        MWB_CUDA(cudaMemcpyAsync(t.coef, h.ncoef, sizeof(double) * BS * nn, cudaMemcpyDeviceToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(t.norm2, h.nn2, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(t.wnorm2, h.nw2, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(t.key, h.nkey, sizeof(uint64_t) * nn, cudaMemcpyDeviceToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(t.parent, h.parent.data(), sizeof(int) * nn, cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(t.child0, h.child0.data(), sizeof(int) * nn, cudaMemcpyHostToDevice, s));
+        t.n = nn;
+        t.level_begin = lb;
+        launch_hash_reset(t, s);
+        launch_hash_insert(t, 0, nn, s);
     }
-    std::vector<int> lb(maxd + 2, 0);
-    for (int i = 0; i < nn; ++i) lb[(key[perm[i]] >> 59) + 1]++;
-    for (size_t d = 1; d < lb.size(); ++d) lb[d] += lb[d - 1];
-    const size_t BS = t.mra->bsize();
-    int* d_perm = (int*)dalloc(ctx, sizeof(int) * std::max(1, nn));
-    double* ncoef = (double*)dalloc(ctx, sizeof(double) * BS * std::max(1, nn));
-    double* nn2 = (double*)dalloc(ctx, sizeof(double) * std::max(1, nn));
-    double* nw2 = (double*)dalloc(ctx, sizeof(double) * std::max(1, nn));
-    uint64_t* nkey = (uint64_t*)dalloc(ctx, sizeof(uint64_t) * std::max(1, nn));
-    MWB_CUDA(cudaMemcpyAsync(d_perm, perm.data(), sizeof(int) * nn, cudaMemcpyHostToDevice, s));
-    k_gather_nodes<<<nn, 256, 0, s>>>(t.coef, t.norm2, t.wnorm2, t.key, d_perm, nn, BS, ncoef, nn2, nw2, nkey);
-    MWB_CUDA(cudaGetLastError());
-    MWB_CUDA(cudaMemcpyAsync(t.coef, ncoef, sizeof(double) * BS * nn, cudaMemcpyDeviceToDevice, s));
-    MWB_CUDA(cudaMemcpyAsync(t.norm2, nn2, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
-    MWB_CUDA(cudaMemcpyAsync(t.wnorm2, nw2, sizeof(double) * nn, cudaMemcpyDeviceToDevice, s));
-    MWB_CUDA(cudaMemcpyAsync(t.key, nkey, sizeof(uint64_t) * nn, cudaMemcpyDeviceToDevice, s));
-    MWB_CUDA(cudaMemcpyAsync(t.parent, parent.data(), sizeof(int) * nn, cudaMemcpyHostToDevice, s));
-    MWB_CUDA(cudaMemcpyAsync(t.child0, child0.data(), sizeof(int) * nn, cudaMemcpyHostToDevice, s));
     MWB_CUDA(cudaStreamSynchronize(s));
-    for (void* p : {(void*)d_perm, (void*)ncoef, (void*)nn2, (void*)nw2, (void*)nkey}) dfree(ctx, p);
-    t.n = nn;
-    t.level_begin = lb;
-    launch_hash_reset(t, s);
-    launch_hash_insert(t, 0, nn, s);
-    MWB_CUDA(cudaStreamSynchronize(s));
+    for (Host& h : H)
+        for (void* p : {(void*)h.d_perm, (void*)h.ncoef, (void*)h.nn2, (void*)h.nw2, (void*)h.nkey}) dfree(ctx, p);
 }
 
 // class-balanced weights for the current training set

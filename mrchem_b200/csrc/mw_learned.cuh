@@ -30,7 +30,6 @@ struct FeatCtx {
     Tree* inp;
     Op* op;
     double prec, g0;
-    double* d_root_w;  // wavelet norms^2 of the output root nodes (exact pass)
 };
 
 void mlp_init(Mlp& M, Ctx* ctx, int nhidden, int width, unsigned seed);
@@ -42,8 +41,8 @@ double mlp_train(Mlp& M, int epochs, int batch, float lr, unsigned seed);
 void mlp_append(Mlp& M, const float* d_F, const std::vector<float>& y, cudaStream_t s);
 // device features (n x kNF) of output nodes items[i] = (feature context index, node)
 float* features(Ctx* ctx, std::vector<FeatCtx>& fc, const std::vector<int2>& items, cudaStream_t s);
-double* root_wnorms(Tree& out);
-void tree_rebuild(Tree& t, const std::vector<char>& keep);
+void trees_rebuild(const std::vector<Tree*>& ts, const std::vector<std::vector<char>>& keeps,
+                   const std::vector<std::vector<uint64_t>>& keys);
 uint64_t host_make_key(int depth, long long tx, long long ty, long long tz);
 void host_key_trans(uint64_t k, long long t[3]);
 
