@@ -44,6 +44,7 @@ def parse():
     p.add_argument("--prec", type=float, default=1e-6)
     p.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--tau", type=float, default=0.97, help="proposal threshold of the learned apply")
     return p.parse_args()
 
 
@@ -257,7 +258,7 @@ def run_gpu(args):
     lstats = {}
 
     def run_learned():
-        st = G.apply_learned(args.prec, outsL, ops, inps, net, tau=0.97, flags=G.APPLY_FP32)
+        st = G.apply_learned(args.prec, outsL, ops, inps, net, tau=args.tau, flags=G.APPLY_FP32)
         lstats.update(st)
         return st["triples"]
 
@@ -288,7 +289,7 @@ def run_gpu(args):
         for i in range(args.orbitals):
             h = host[i]
             e_in[i].load(h["depth"], h["trans"], h["parent"], h["child0"], h["coef"])
-        G.apply_learned(args.prec, outsL, ops, e_in, net, tau=0.97, flags=G.APPLY_FP32)
+        G.apply_learned(args.prec, outsL, ops, e_in, net, tau=args.tau, flags=G.APPLY_FP32)
         for i in range(args.orbitals):
             res = outsL[i].export()
             d2h += sum(v.nbytes for v in res.values() if v is not None)
@@ -339,7 +340,7 @@ def run_gpu(args):
             "learned": {"passes": lstats.get("passes"), "proposed": lstats.get("proposed"),
                         "pruned": lstats.get("pruned"), "missed": lstats.get("missed"),
                         "out_nodes": lstats.get("out_nodes"), "train_rows": n_train, "train_positive": n_pos,
-                        "train_loss": train_loss, "train_s": t_train,
+                        "train_loss": train_loss, "train_s": t_train, "tau": args.tau,
                         "train_data": "plain applies of 32 other seeded orbitals (seed 1007)"},
             "roofline": {"bound": "tensor", "kernel": "k_bapply<10,float>", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
