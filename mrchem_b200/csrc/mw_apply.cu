@@ -16,9 +16,13 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <string>
+#include <type_traits>
 
 #include "mw_device.cuh"
 #include "mw_kernels.cuh"
+#include "mw_tmem.cuh"
 
 namespace mwb {
 
@@ -588,6 +592,419 @@ __global__ void __launch_bounds__(ACfg<K, R>::NT, 1)
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// 5b. GEMM-tiled contraction.  Each mode product of a term is a GEMM C[2k x (2k)^2] = M A with the
+//     data operand in shared memory as k-major rows (row = contracted index, columns = the other two
+//     indices), and every step writes its result in the row layout the next step reads:
+//        X [a][b + P c]  --x-->  T1 [b][a' + P c]  --y-->  T2 [c][a' + P b']  --z-->  acc [c'][a' + P b']
+//     (P = 2k rounded up to a multiple of 4, padding zero).  A thread owns an MT x NT tile of every
+//     step; a warp is 4 row tiles x 8 column tiles, so per contracted index a warp reads MT broadcast
+//     operator values and NT data values per lane and issues MT*NT FMAs.  Operators are staged
+//     transposed (At[k][o] = M[o][k]); the z step uses the beta-scaled tables.
+//     Below the root the s->s block is taken out with three k x k x k GEMMs on the top-left k x k
+//     operator blocks (U1, U2, Uc); the owners of the z tiles subtract Uc one phase later.
+//     Generated inputs (scaling part only) contract over k instead of 2k and skip the tiles that
+//     only see their zero wavelet part.
+//     Barriers per term: after x, after y.  Shared-memory hazards across terms are resolved by
+//     loading each operator in a phase that the two barriers separate from its readers:
+//     Mx(t+1) and Mz(t) during y(t), My(t+1) during z(t).
+// ---------------------------------------------------------------------------------------------
+__host__ __device__ constexpr int gcfg_nc(int k, int nthr) {
+    int d = 1;
+    while (d < k && (k % d != 0 || 2 * k * k / d > nthr)) ++d;
+    return d;
+}
+// Row-stride padding of the T1 (x-step output) and T2 (y-step output) buffers, chosen per basis size
+// so that the epilogue stores of a warp fall into distinct banks (counted wavefronts per step,
+// consecutive column tiles per warp; the FP64 x step with an odd tile width uses strided tiles).
+__host__ __device__ constexpr int gcfg_pad1(int k, bool f32) {
+    return f32 ? ((k == 5 || k == 6 || k == 9 || k == 10) ? 8 : (k == 11 || k == 12) ? 4 : 0) : 0;
+}
+__host__ __device__ constexpr int gcfg_pad2(int k) {
+    return (k == 5 || k == 6 || k == 9 || k == 10) ? 0 : (k == 11 || k == 12) ? 8 : 2;
+}
+
+template <int K, typename R>
+struct GCfg {
+    static constexpr bool F32 = sizeof(R) == 4;
+    static constexpr int K2 = 2 * K;
+    static constexpr int KP = (K2 + 3) / 4 * 4;
+    static constexpr int NN = KP * KP;
+    static constexpr int MT = KP / 4;
+    static constexpr int NT = (F32 && MT * (KP / 2) <= 50) ? KP / 2 : KP / 4;
+    static constexpr int LDX = NN + 2;
+    static constexpr int LD1 = NN + gcfg_pad1(K, F32);
+    static constexpr int LD2 = NN + gcfg_pad2(K);
+    static constexpr bool XSTRIDED = !F32 && (NT % 2 == 1);
+    static constexpr int NTILE = NN / NT;
+    static constexpr int NWARP = (NTILE + 7) / 8;
+    static constexpr int NTHR = 32 * NWARP;
+    static constexpr int KK = K * K;
+    static constexpr int KKK = K * K * K;
+    static constexpr int NC = gcfg_nc(K, NTHR);  // correction tile columns
+    static constexpr int NCT = KK / NC;
+    static constexpr int ND = MT * NT;  // accumulators per thread
+    // FP32: accumulators in TMEM, 2 columns per double, warps sharing a lane quarter side by side
+    static constexpr int TCOLS_NEED = ((NWARP + 3) / 4) * 2 * ND;
+    static constexpr int TCOLS = TCOLS_NEED <= 32 ? 32 : TCOLS_NEED <= 64 ? 64 : TCOLS_NEED <= 128 ? 128
+                                 : TCOLS_NEED <= 256 ? 256 : 512;
+    static constexpr size_t SMEM =
+        sizeof(R) * ((size_t)KP * (LDX + LD1 + LD2) + 3 * (size_t)KP * KP + 3 * (size_t)KKK) + 64;
+    static constexpr int MINB = (F32 && 2 * (SMEM + 16 + 1024) <= 233472) ? 2 : 1;
+    static constexpr bool FITS = SMEM + 16 + 1024 <= 232448 && 2 * NCT <= NTHR && TCOLS_NEED <= 512 &&
+                                 (size_t)KP * LDX * sizeof(R) >= 64 * sizeof(double) && (!F32 || TCOLS * MINB <= 512);
+};
+
+__device__ __forceinline__ float mfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double mfma(double a, double b, double c) { return fma(a, b, c); }
+
+// c (+)= At^T B on a thread tile: c[i][j] (+)= sum_{k < kdim} At[k lda + o0 + i] B[k ldb + n0 + j]
+template <int MT, int NT, bool ACC, typename R, typename CT>
+__device__ __forceinline__ void gemm_tile(const R* __restrict__ At, int lda, const R* __restrict__ B, int ldb,
+                                          int o0, int n0, int kdim, CT (&c)[MT][NT]) {
+    if (!ACC) {
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NT; ++j) c[i][j] = CT(0);
+    }
+    const R* ap = At + o0;
+    const R* bp = B + n0;
+#pragma unroll 2
+    for (int k = 0; k < kdim; ++k) {
+        R a[MT], b[NT];
+#pragma unroll
+        for (int i = 0; i < MT; ++i) a[i] = ap[i];
+        if constexpr (NT % 2 == 0) {
+            using V2 = typename std::conditional<sizeof(R) == 4, float2, double2>::type;
+#pragma unroll
+            for (int j = 0; j < NT; j += 2) {
+                const V2 v = *reinterpret_cast<const V2*>(bp + j);
+                b[j] = v.x;
+                b[j + 1] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < NT; ++j) b[j] = bp[j];
+        }
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NT; ++j) c[i][j] = mfma((CT)a[i], (CT)b[j], c[i][j]);
+        ap += lda;
+        bp += ldb;
+    }
+}
+
+// the same with per-column offsets (correction GEMMs; columns not contiguous)
+template <int MT, int NT, typename R>
+__device__ __forceinline__ void gemm_tile_off(const R* __restrict__ At, int lda, const R* __restrict__ B, int ldb,
+                                              int o0, const int (&off)[NT], int kdim, R (&c)[MT][NT]) {
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) c[i][j] = R(0);
+    for (int k = 0; k < kdim; ++k) {
+        R a[MT], b[NT];
+#pragma unroll
+        for (int i = 0; i < MT; ++i) a[i] = At[k * lda + o0 + i];
+#pragma unroll
+        for (int j = 0; j < NT; ++j) b[j] = B[k * ldb + off[j]];
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NT; ++j) c[i][j] = mfma(a[i], b[j], c[i][j]);
+    }
+}
+
+template <int K, typename R>
+__global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
+    k_gapply(const Chunk* __restrict__ chunks, const Item* __restrict__ items, const BTree* __restrict__ trees,
+             const int* __restrict__ cdelta, const int* __restrict__ csrc, const double* __restrict__ gblk,
+             const double* __restrict__ gnorm2, double* partials, unsigned long long* ntrip_out) {
+    using C = GCfg<K, R>;
+    constexpr int K2 = C::K2, KP = C::KP, MT = C::MT, NT = C::NT, NC = C::NC, ND = C::ND;
+    constexpr int LDX = C::LDX, LD1 = C::LD1, LD2 = C::LD2;
+    constexpr int KK = C::KK, KKK = C::KKK;
+    constexpr int BS = K2 * K2 * K2;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ uint32_t tmem_slot;
+    R* X = reinterpret_cast<R*>(smraw);  // [KP][LDX]
+    R* T1 = X + KP * LDX;                // [KP][LD1]
+    R* T2 = T1 + KP * LD1;               // [KP][LD2]
+    R* Mx = T2 + KP * LD2;               // [KP][KP], At[k][o] = M[o][k]
+    R* My = Mx + KP * KP;
+    R* Mz = My + KP * KP;
+    R* U1 = Mz + KP * KP;  // [K][K][K]
+    R* U2 = U1 + KKK;
+    R* Uc = U2 + KKK;
+    const Chunk ch = chunks[blockIdx.x];
+    const Item it = items[ch.item];
+    const BTree& TR = trees[it.tree];
+    const R* mats = reinterpret_cast<const R*>(C::F32 ? (const void*)TR.mats32 : (const void*)TR.mats);
+    const R* matsb = reinterpret_cast<const R*>(C::F32 ? (const void*)TR.matsb32 : (const void*)TR.matsb);
+    const bool root = TR.root != 0;
+    const double theta = TR.theta;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // tiles: 4 row tiles x 8 column tiles per warp; consecutive column tiles (y and z steps, and the
+    // x step unless strided), or column tiles strided by the warp count (x step)
+    const int rt = lane & 3;
+    const int ct_c = warp * 8 + (lane >> 2);
+    const int ct_x = C::XSTRIDED ? warp + C::NWARP * (lane >> 2) : ct_c;
+    const bool own = ct_c < C::NTILE, own_x = ct_x < C::NTILE;
+    const int o0 = rt * MT;
+    const int n0 = own ? ct_c * NT : 0, n0x = own_x ? ct_x * NT : 0;
+    const int tb0 = n0 % KP, tc0 = n0 / KP;     // y tile: first a', c;  z tile: first a', b'
+    const int xb0 = n0x % KP, xc0 = n0x / KP;   // x tile: first b, c
+    // correction tile
+    const int crt = tid & 1, cct = tid >> 1;
+    const bool cown = !root && cct < C::NCT;
+    const int co0 = crt * MT, cn0 = cown ? cct * NC : 0;
+
+    // accumulators: registers (FP64 kernel) or this thread's TMEM lane (FP32 kernel)
+    double acc[C::F32 ? 1 : MT][C::F32 ? 1 : NT];
+    uint32_t tacc = 0;
+    if constexpr (C::F32) {
+        if (warp == 0) {
+            tmem_alloc(&tmem_slot, C::TCOLS);
+            tmem_relinquish();
+        }
+        tmem_fence_before_sync();
+        __syncthreads();
+        tmem_fence_after_sync();
+        tacc = tmem_slot + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)((warp >> 2) * 2 * ND);
+        tmem_visit<ND, true>(tacc, [&](int, int n, auto& r) {
+#pragma unroll
+            for (int q = 0; q < 2 * n; ++q) r[q] = 0u;
+        });
+    } else {
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NT; ++j) acc[i][j] = 0.0;
+    }
+    unsigned long long ntrip = 0;
+    bool pend2 = false;     // c2 holds a correction block not yet written to Uc
+    bool uc_valid = false;  // Uc holds a correction block not yet subtracted
+    R c2[MT][NC];
+
+    // dst[k KP + o] = M[o][k] (zero padded)
+    auto load_mat = [&](R* dst, const R* tab, int mi) {
+        const R* src = tab + (size_t)mi * K2 * K2;
+        for (int e = tid; e < KP * KP; e += blockDim.x) {
+            const int o = e / KP, k = e % KP;
+            dst[k * KP + o] = (o < K2 && k < K2) ? src[o * K2 + k] : R(0);
+        }
+    };
+    // correction block of element (c', a', b') of this thread's z tile, 0 outside s->s
+    auto uc_at = [&](int i, int j) -> double {
+        const int cz = o0 + i, n = n0 + j, ax = n % KP, by = n / KP;
+        return (cz < K && ax < K && by < K) ? (double)Uc[cz * KK + ax + K * by] : 0.0;
+    };
+    auto write_c2 = [&]() {
+        if (!cown) return;
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NC; ++j)
+                if (co0 + i < K) Uc[(co0 + i) * KK + cn0 + j] = c2[i][j];
+    };
+    if (KP > K2) {  // padding rows/columns of X stay zero for the whole kernel
+        for (int e = tid; e < KP * LDX; e += blockDim.x) X[e] = R(0);
+    }
+
+    for (int ci = ch.c0; ci < ch.c1; ++ci) {
+        const int src = csrc[ci];
+        const bool gen = src < 0;
+        const double nu = gen ? sqrt(gnorm2[-src - 1]) : sqrt(TR.in.norm2[src]);
+        const DeltaRec de = TR.deltas[cdelta[ci]];
+        if (!(nu > 0.0) || de.maxb * nu < theta) continue;
+        if (TR.terms[de.t0].bound * nu < theta) continue;
+        __syncthreads();  // every reader of X and of the operators of the previous candidate is done
+        if (gen) {
+            const double* blk = gblk + (size_t)(-src - 1) * KKK;
+            for (int e = tid; e < BS; e += blockDim.x) {
+                const int a = e % K2, b = (e / K2) % K2, c = e / (K2 * K2);
+                X[a * LDX + b + KP * c] = (a < K && b < K && c < K) ? (R)blk[a + K * (b + K * c)] : R(0);
+            }
+        } else {
+            const double* blk = TR.in.coef + (size_t)src * BS;
+            for (int e = tid; e < BS; e += blockDim.x) {
+                const int a = e % K2, b = (e / K2) % K2, c = e / (K2 * K2);
+                X[a * LDX + b + KP * c] = (R)blk[e];
+            }
+        }
+        {
+            const TermRec t0 = TR.terms[de.t0];
+            load_mat(Mx, mats, t0.mx);
+            load_mat(My, mats, t0.my);
+        }
+        __syncthreads();
+        const int kd = gen ? K : KP;  // contracted length of every step
+        for (int ti = de.t0; ti < de.t1; ++ti) {
+            const TermRec tr = TR.terms[ti];
+            if (tr.bound * nu < theta) break;
+            const bool has_next = ti + 1 < de.t1 && !(TR.terms[ti + 1].bound * nu < theta);
+            const TermRec tn = has_next ? TR.terms[ti + 1] : tr;
+            // ---- x: T1[b][a' + P c] = sum_a Mx[a'][a] X[a][b + P c]
+            if (own_x && (!gen || (xb0 < K && xc0 < K))) {
+                R c[MT][NT];
+                gemm_tile<MT, NT, false>(Mx, KP, X, LDX, o0, n0x, kd, c);
+#pragma unroll
+                for (int j = 0; j < NT; ++j)
+#pragma unroll
+                    for (int i = 0; i < MT; ++i) T1[(xb0 + j) * LD1 + o0 + i + KP * xc0] = c[i][j];
+            }
+            if (cown) {  // U1[b][a' + k c] = sum_{a<k} Tx[a'][a] X[a][b + P c]
+                int off[NC];
+#pragma unroll
+                for (int j = 0; j < NC; ++j) off[j] = (cn0 + j) % K + KP * ((cn0 + j) / K);
+                R c[MT][NC];
+                gemm_tile_off<MT, NC>(Mx, KP, X, LDX, co0, off, K, c);
+#pragma unroll
+                for (int i = 0; i < MT; ++i)
+#pragma unroll
+                    for (int j = 0; j < NC; ++j) {
+                        const int n = cn0 + j;
+                        if (co0 + i < K) U1[(n % K) * KK + co0 + i + K * (n / K)] = c[i][j];
+                    }
+            }
+            __syncthreads();
+            // ---- y: T2[c][a' + P b'] = sum_b My[b'][b] T1[b][a' + P c]
+            if (pend2) {  // the previous term's correction block, subtracted in this term's z phase
+                write_c2();
+                pend2 = false;
+                uc_valid = true;
+            }
+            if (has_next) load_mat(Mx, mats, tn.mx);
+            load_mat(Mz, matsb, tr.mz);
+            if (own && (!gen || tc0 < K)) {
+                R c[MT][NT];
+                gemm_tile<MT, NT, false>(My, KP, T1, LD1, o0, n0, kd, c);
+#pragma unroll
+                for (int i = 0; i < MT; ++i) {
+                    R* row = T2 + tc0 * LD2 + tb0 + KP * (o0 + i);
+                    if constexpr (NT % 2 == 0) {
+                        using V2 = typename std::conditional<sizeof(R) == 4, float2, double2>::type;
+#pragma unroll
+                        for (int j = 0; j < NT; j += 2) {
+                            V2 v;
+                            v.x = c[i][j];
+                            v.y = c[i][j + 1];
+                            *reinterpret_cast<V2*>(row + j) = v;
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < NT; ++j) row[j] = c[i][j];
+                    }
+                }
+            }
+            if (cown) {  // U2[c][a' + k b'] = sum_{b<k} Ty[b'][b] U1[b][a' + k c]
+                int off[NC];
+#pragma unroll
+                for (int j = 0; j < NC; ++j) off[j] = cn0 + j;
+                R c[MT][NC];
+                gemm_tile_off<MT, NC>(My, KP, U1, KK, co0, off, K, c);
+#pragma unroll
+                for (int i = 0; i < MT; ++i)
+#pragma unroll
+                    for (int j = 0; j < NC; ++j) {
+                        const int n = cn0 + j;
+                        if (co0 + i < K) U2[(n / K) * KK + (n % K) + K * (co0 + i)] = c[i][j];
+                    }
+            }
+            __syncthreads();
+            // ---- z: acc[c'][a' + P b'] += sum_c (beta Mz)[c'][c] T2[c][a' + P b']  (- previous correction)
+            if (has_next) load_mat(My, mats, tn.my);
+            if constexpr (C::F32) {
+                float c[MT][NT];
+                if (own) {
+                    gemm_tile<MT, NT, false>(Mz, KP, T2, LD2, o0, n0, kd, c);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < MT; ++i)
+#pragma unroll
+                        for (int j = 0; j < NT; ++j) c[i][j] = 0.0f;
+                }
+                const bool fold = uc_valid && own;
+                tmem_visit<ND, true>(tacc, [&](int d0, int n, auto& r) {
+#pragma unroll
+                    for (int q = 0; q < n; ++q) {
+                        const int d = d0 + q, i = d / NT, j = d % NT;
+                        double v = words_to_double(r[2 * q], r[2 * q + 1]) + (double)c[i][j];
+                        if (fold) v -= uc_at(i, j);
+                        double_to_words(v, r[2 * q], r[2 * q + 1]);
+                    }
+                });
+            } else {
+                if (own) {
+                    gemm_tile<MT, NT, true>(Mz, KP, T2, LD2, o0, n0, kd, acc);
+                    if (uc_valid) {
+#pragma unroll
+                        for (int i = 0; i < MT; ++i)
+#pragma unroll
+                            for (int j = 0; j < NT; ++j) acc[i][j] -= uc_at(i, j);
+                    }
+                }
+            }
+            uc_valid = false;
+            if (cown) {  // c2[c'][a' + k b'] = sum_{c<k} (beta Tz)[c'][c] U2[c][a' + k b']
+                int off[NC];
+#pragma unroll
+                for (int j = 0; j < NC; ++j) off[j] = cn0 + j;
+                gemm_tile_off<MT, NC>(Mz, KP, U2, KK, co0, off, K, c2);
+            }
+            pend2 = !root;
+            ++ntrip;
+        }
+    }
+    __syncthreads();  // z-phase readers of Uc are done
+    if (pend2) write_c2();
+    uc_valid = pend2;
+    __syncthreads();
+    double* dst = ch.slot < 0 ? TR.ocoef + (size_t)it.node * BS : partials + (size_t)ch.slot * BS;
+    double n2 = 0.0, w2 = 0.0;
+    auto emit = [&](int i, int j, double v) {
+        const int cz = o0 + i, n = n0 + j, ax = n % KP, by = n / KP;
+        if (uc_valid) v -= uc_at(i, j);
+        if (cz < K2 && ax < K2 && by < K2) {
+            dst[ax + K2 * (by + K2 * cz)] = v;
+            n2 += v * v;
+            if (!(ax < K && by < K && cz < K)) w2 += v * v;
+        }
+    };
+    if constexpr (C::F32) {
+        tmem_visit<ND, false>(tacc, [&](int d0, int n, auto& r) {
+#pragma unroll
+            for (int q = 0; q < n; ++q) {
+                const int d = d0 + q;
+                if (own) emit(d / NT, d % NT, words_to_double(r[2 * q], r[2 * q + 1]));
+            }
+        });
+        tmem_fence_before_sync();
+        __syncthreads();
+        tmem_fence_after_sync();
+        if (warp == 0) tmem_dealloc(tmem_slot, C::TCOLS);
+    } else {
+        if (own) {
+#pragma unroll
+            for (int i = 0; i < MT; ++i)
+#pragma unroll
+                for (int j = 0; j < NT; ++j) emit(i, j, acc[i][j]);
+        }
+    }
+    double* red = reinterpret_cast<double*>(X);  // X is no longer read
+    __syncthreads();
+    block_sum2(n2, w2, red);
+    if (tid == 0) {
+        if (ch.slot < 0) {
+            TR.onorm2[it.node] = n2;
+            TR.ownorm2[it.node] = w2;
+        }
+        atomicAdd(ntrip_out, ntrip);
+    }
+}
+
 // add the partial blocks of a multi-chunk node in chunk order; write block and norms
 template <int K>
 __global__ void __launch_bounds__(256) k_breduce(const Chunk* __restrict__ chunks, const int* __restrict__ choff,
@@ -661,6 +1078,16 @@ __global__ void k_gather_int(const int* __restrict__ src, const int* __restrict_
 // ---------------------------------------------------------------------------------------------
 
 static inline void count(Ctx* c, int n = 1) { c->launches += n; }
+
+// MWB200_CONTRACTION=pencil selects the pencil contraction kernel even where the GEMM-tiled one fits
+// (both compute the same sums; kept for comparison and for bases too large for the tiled kernel)
+static bool contraction_pencil() {
+    static const bool v = [] {
+        const char* e = std::getenv("MWB200_CONTRACTION");
+        return e != nullptr && std::string(e) == "pencil";
+    }();
+    return v;
+}
 
 template <typename T>
 static T* upload(Ctx* ctx, const std::vector<T>& v) {
@@ -839,9 +1266,22 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     unsigned long long* d_ntrip_tot = (unsigned long long*)dalloc(ctx, sizeof(unsigned long long));
     MWB_CUDA(cudaMemsetAsync(d_ntrip_tot, 0, sizeof(unsigned long long), s));
     if (ctx->prof) MWB_CUDA(cudaEventRecord(ctx->ev0, s));
+    const bool pencil = contraction_pencil();
 #define L_AP(KK)                                                                                             \
     {                                                                                                        \
-        if (bp.precision == 1) {                                                                             \
+        if (bp.precision == 1 && GCfg<KK, float>::FITS && !pencil) {                                          \
+            size_t smem = GCfg<KK, float>::SMEM;                                                             \
+            MWB_CUDA(cudaFuncSetAttribute(k_gapply<KK, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+            k_gapply<KK, float><<<nchunks, GCfg<KK, float>::NTHR, smem, s>>>(d_chunks, d_items, d_trees, d_cdelta, \
+                                                                              d_csrc, d_gblk, d_gnorm2, d_partials, \
+                                                                              d_ntrip_tot);                        \
+        } else if (bp.precision != 1 && GCfg<KK, double>::FITS && !pencil) {                                  \
+            size_t smem = GCfg<KK, double>::SMEM;                                                            \
+            MWB_CUDA(cudaFuncSetAttribute(k_gapply<KK, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+            k_gapply<KK, double><<<nchunks, GCfg<KK, double>::NTHR, smem, s>>>(d_chunks, d_items, d_trees, d_cdelta, \
+                                                                                d_csrc, d_gblk, d_gnorm2, d_partials, \
+                                                                                d_ntrip_tot);                       \
+        } else if (bp.precision == 1) {                                                                      \
             size_t smem = ACfg<KK, float>::SMEM;                                                             \
             MWB_CUDA(cudaFuncSetAttribute(k_bapply<KK, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
             k_bapply<KK, float><<<nchunks, ACfg<KK, float>::NT, smem, s>>>(d_chunks, d_items, d_trees, d_cdelta,  \
