@@ -210,6 +210,10 @@ Op::~Op() {
         dfree(c, kv.second->d_mats32);
         dfree(c, kv.second->d_matsb);
         dfree(c, kv.second->d_matsb32);
+        dfree(c, kv.second->d_matsT);
+        dfree(c, kv.second->d_matsT32);
+        dfree(c, kv.second->d_matsbT);
+        dfree(c, kv.second->d_matsbT32);
         dfree(c, kv.second->d_deltas);
         dfree(c, kv.second->d_terms);
     }
@@ -383,6 +387,27 @@ static const OpDepth& op_depth(Op& op, int depth) {
         for (size_t q = 0; q < n; ++q) mb[b0 + q] = op.terms[mi].beta * od->mats[b0 + q];
     }
     std::vector<float> mb32(mb.begin(), mb.end());
+    // transposed, zero-padded copies for the GEMM-tiled contraction
+    const int KP = (K2 + 3) / 4 * 4;
+    const size_t nmat = od->mats.size() / ((size_t)K2 * K2);
+    std::vector<double> mT(nmat * KP * KP, 0.0), mbT(nmat * KP * KP, 0.0);
+    for (size_t mi = 0; mi < nmat; ++mi)
+        for (int o = 0; o < K2; ++o)
+            for (int k = 0; k < K2; ++k) {
+                mT[mi * KP * KP + (size_t)k * KP + o] = od->mats[mi * K2 * K2 + (size_t)o * K2 + k];
+                mbT[mi * KP * KP + (size_t)k * KP + o] = mb[mi * K2 * K2 + (size_t)o * K2 + k];
+            }
+    std::vector<float> mT32(mT.begin(), mT.end()), mbT32(mbT.begin(), mbT.end());
+    od->d_matsT = (double*)dalloc(ctx, sizeof(double) * std::max<size_t>(1, mT.size()));
+    od->d_matsT32 = (float*)dalloc(ctx, sizeof(float) * std::max<size_t>(1, mT.size()));
+    od->d_matsbT = (double*)dalloc(ctx, sizeof(double) * std::max<size_t>(1, mT.size()));
+    od->d_matsbT32 = (float*)dalloc(ctx, sizeof(float) * std::max<size_t>(1, mT.size()));
+    if (!mT.empty()) {
+        MWB_CUDA(cudaMemcpyAsync(od->d_matsT, mT.data(), sizeof(double) * mT.size(), cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(od->d_matsT32, mT32.data(), sizeof(float) * mT.size(), cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(od->d_matsbT, mbT.data(), sizeof(double) * mT.size(), cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(od->d_matsbT32, mbT32.data(), sizeof(float) * mT.size(), cudaMemcpyHostToDevice, s));
+    }
     if (!od->mats.empty()) {
         MWB_CUDA(cudaMemcpyAsync(od->d_mats, od->mats.data(), sizeof(double) * od->mats.size(), cudaMemcpyHostToDevice, s));
         MWB_CUDA(cudaMemcpyAsync(od->d_mats32, m32.data(), sizeof(float) * m32.size(), cudaMemcpyHostToDevice, s));

@@ -41,6 +41,10 @@ struct BTree {
     const float* mats32;
     const double* matsb;    // beta-scaled copies (z-step operators)
     const float* matsb32;
+    const double* matsT;    // transposed, zero-padded copies (GEMM-tiled contraction)
+    const float* matsT32;
+    const double* matsbT;
+    const float* matsbT32;
     int nprefix;
     int root;
     double theta;
@@ -741,8 +745,8 @@ __global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
     const Chunk ch = chunks[blockIdx.x];
     const Item it = items[ch.item];
     const BTree& TR = trees[it.tree];
-    const R* mats = reinterpret_cast<const R*>(C::F32 ? (const void*)TR.mats32 : (const void*)TR.mats);
-    const R* matsb = reinterpret_cast<const R*>(C::F32 ? (const void*)TR.matsb32 : (const void*)TR.matsb);
+    const R* mats = reinterpret_cast<const R*>(C::F32 ? (const void*)TR.matsT32 : (const void*)TR.matsT);
+    const R* matsb = reinterpret_cast<const R*>(C::F32 ? (const void*)TR.matsbT32 : (const void*)TR.matsbT);
     const bool root = TR.root != 0;
     const double theta = TR.theta;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -788,13 +792,14 @@ __global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
     bool uc_valid = false;  // Uc holds a correction block not yet subtracted
     R c2[MT][NC];
 
-    // dst[k KP + o] = M[o][k] (zero padded)
+    // asynchronous copy of a transposed operator (At[k][o] = M[o][k], P x P) into shared memory; the
+    // copies a thread issued are complete at its next cp_async_wait_all(), which precedes every
+    // barrier that publishes an operator
     auto load_mat = [&](R* dst, const R* tab, int mi) {
-        const R* src = tab + (size_t)mi * K2 * K2;
-        for (int e = tid; e < KP * KP; e += blockDim.x) {
-            const int o = e / KP, k = e % KP;
-            dst[k * KP + o] = (o < K2 && k < K2) ? src[o * K2 + k] : R(0);
-        }
+        constexpr int NV = KP * KP * (int)sizeof(R) / 16;
+        const char* src = reinterpret_cast<const char*>(tab + (size_t)mi * KP * KP);
+        for (int e = tid; e < NV; e += blockDim.x) cp_async16(reinterpret_cast<char*>(dst) + 16 * e, src + 16 * e);
+        cp_async_commit();
     };
     // correction block of element (c', a', b') of this thread's z tile, 0 outside s->s
     auto uc_at = [&](int i, int j) -> double {
@@ -820,6 +825,12 @@ __global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
         const DeltaRec de = TR.deltas[cdelta[ci]];
         if (!(nu > 0.0) || de.maxb * nu < theta) continue;
         if (TR.terms[de.t0].bound * nu < theta) continue;
+        if (tid == 0 && ci + 1 < ch.c1) {  // the next candidate's block: into L2 while this one runs
+            const int s1 = csrc[ci + 1];
+            if (s1 < 0) prefetch_l2_bulk(gblk + (size_t)(-s1 - 1) * KKK, (unsigned)(KKK * sizeof(double)));
+            else prefetch_l2_bulk(TR.in.coef + (size_t)s1 * BS, (unsigned)(BS * sizeof(double)));
+        }
+        cp_async_wait_all();
         __syncthreads();  // every reader of X and of the operators of the previous candidate is done
         if (gen) {
             const double* blk = gblk + (size_t)(-src - 1) * KKK;
@@ -839,6 +850,7 @@ __global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
             load_mat(Mx, mats, t0.mx);
             load_mat(My, mats, t0.my);
         }
+        cp_async_wait_all();
         __syncthreads();
         const int kd = gen ? K : KP;  // contracted length of every step
         for (int ti = de.t0; ti < de.t1; ++ti) {
@@ -869,6 +881,7 @@ __global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
                         if (co0 + i < K) U1[(n % K) * KK + co0 + i + K * (n / K)] = c[i][j];
                     }
             }
+            cp_async_wait_all();
             __syncthreads();
             // ---- y: T2[c][a' + P b'] = sum_b My[b'][b] T1[b][a' + P c]
             if (pend2) {  // the previous term's correction block, subtracted in this term's z phase
@@ -913,6 +926,7 @@ __global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
                         if (co0 + i < K) U2[(n / K) * KK + (n % K) + K * (co0 + i)] = c[i][j];
                     }
             }
+            cp_async_wait_all();
             __syncthreads();
             // ---- z: acc[c'][a' + P b'] += sum_c (beta Mz)[c'][c] T2[c][a' + P b']  (- previous correction)
             if (has_next) load_mat(My, mats, tn.my);
@@ -958,6 +972,7 @@ __global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
             ++ntrip;
         }
     }
+    cp_async_wait_all();
     __syncthreads();  // z-phase readers of Uc are done
     if (pend2) write_c2();
     uc_valid = pend2;
@@ -1150,6 +1165,10 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         d.mats32 = b.tab->d_mats32;
         d.matsb = b.tab->d_matsb;
         d.matsb32 = b.tab->d_matsb32;
+        d.matsT = b.tab->d_matsT;
+        d.matsT32 = b.tab->d_matsT32;
+        d.matsbT = b.tab->d_matsbT;
+        d.matsbT32 = b.tab->d_matsbT32;
         d.nprefix = b.nprefix;
         d.root = b.depth == 0;
         d.theta = b.theta;

@@ -75,6 +75,23 @@ struct Geo {
     __device__ static inline int at(int a, int b, int c) { return a + P * (b + K2 * c); }
 };
 
+// 16-byte asynchronous global -> shared copies (cp.async, L2 only), their commit and completion
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem_dst)),
+                 "l"(gmem_src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// prefetch the 16-byte-aligned part of [gmem, gmem + bytes) into L2 through the bulk-copy engine
+// (the instruction wants a 16-byte aligned address and a size that is a multiple of 16)
+__device__ __forceinline__ void prefetch_l2_bulk(const void* gmem, unsigned bytes) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(gmem);
+    const uintptr_t lo = (a + 15) & ~uintptr_t(15), hi = (a + bytes) & ~uintptr_t(15);
+    if (hi > lo)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(lo), "r"((unsigned)(hi - lo)) : "memory");
+}
+
 // Sum two values over the block; the result is valid in thread 0.  `red` holds 64 doubles.
 __device__ static inline void block_sum2(double& a, double& b, double* red) {
     for (int o = 16; o; o >>= 1) {

@@ -83,6 +83,12 @@ struct OpDepth {
     float* d_mats32 = nullptr;  // FP32 copy of d_mats (mixed-precision apply)
     double* d_matsb = nullptr;  // each matrix scaled by its term's beta (z-step operators)
     float* d_matsb32 = nullptr;
+    // the same four tables transposed and zero-padded to P x P (P = 2k rounded up to a multiple of
+    // 4), entry [k][o] = M[o][k]: the layout the GEMM-tiled contraction copies into shared memory
+    double* d_matsT = nullptr;
+    float* d_matsT32 = nullptr;
+    double* d_matsbT = nullptr;
+    float* d_matsbT32 = nullptr;
     DeltaRec* d_deltas = nullptr;
     TermRec* d_terms = nullptr;
 };
