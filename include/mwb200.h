@@ -127,6 +127,26 @@ int mw_apply_batched(int n, double prec, mw_tree* out, mw_op* ops, mw_tree* inp,
  * [2] refinement passes, [3] output nodes */
 int mw_apply_stats(mw_tree out, long long* stats);
 
+/* Pointwise product out = c a b.  Replaces mrcpp::multiply(prec, out, c, a, b[, maxIter]):
+ * reference src/qmfunctions/qmfunction_utils.cpp:209-217, src/qmoperators/two_electron/ExchangePotential.cpp:
+ * 131,253,312.  `out` keeps its current grid (an empty tree starts from the root boxes); every leaf is
+ * computed, then leaves whose wavelet norm exceeds prec ||out|| 2^{-depth/2} are split and their
+ * children computed, at most max_iter times (max_iter < 0: until no node splits; prec <= 0 or
+ * max_iter = 0: the grid is kept, as in the reference's union-grid form).  `out` is left compressed
+ * with valid norms.  Orders up to 10 (k <= 11). */
+int mw_multiply(double prec, mw_tree out, double c, mw_tree a, mw_tree b, int max_iter);
+/* out[i] = c[i] a[i] b[i] for i < n with the refinement passes of the batch in lock-step (c may be NULL:
+ * all 1).  Same result per product as n calls of mw_multiply. */
+int mw_multiply_batched(int n, double prec, mw_tree* out, const double* c, mw_tree* a, mw_tree* b, int max_iter);
+/* out = a^2: mrcpp::square(prec, out, a), reference src/qmfunctions/density_utils.cpp:74 */
+int mw_square(double prec, mw_tree out, mw_tree a, int max_iter);
+/* Grids.  mw_tree_build_grid extends the grid of `out` by that of `inp` (new nodes have zero blocks;
+ * mrcpp::build_grid, reference qmfunction_utils.cpp:211-212); mw_tree_copy_grid = clear + build_grid
+ * (mrcpp::copy_grid, density_utils.cpp:73); mw_tree_clear empties a tree. */
+int mw_tree_build_grid(mw_tree out, mw_tree inp);
+int mw_tree_copy_grid(mw_tree out, mw_tree inp);
+int mw_tree_clear(mw_tree tree);
+
 /* Learned output-tree proposal.  No counterpart in the reference: MRCPP refines the output tree
  * pass by pass (the plain path above).  A small FP32 MLP predicts which output nodes the wavelet-norm
  * check will split, from 64 features per node (level, position, block and wavelet norms of the 27

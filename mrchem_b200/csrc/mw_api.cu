@@ -56,7 +56,7 @@ Tree::~Tree() {
     cudaStreamSynchronize(c->stream);
 }
 
-static void tree_reserve(Tree& t, int need) {
+void tree_reserve(Tree& t, int need) {
     Ctx* ctx = t.mra->ctx;
     cudaStream_t s = ctx->stream;
     if (need > t.cap) {
@@ -92,7 +92,7 @@ static void tree_reserve(Tree& t, int need) {
 }
 
 // root boxes in Morton order
-static void tree_make_roots(Tree& t) {
+void tree_make_roots(Tree& t) {
     const Mra& m = *t.mra;
     std::vector<uint64_t> keys;
     for (int z = 0; z < m.boxes[2]; ++z)
@@ -146,7 +146,7 @@ static int* range_list(Ctx* ctx, int begin, int end) {
 }
 
 // bottom-up: every internal node becomes the compression of its children's scaling parts
-static void tree_compress_bottom_up(Tree& t) {
+void tree_compress_bottom_up(Tree& t) {
     cudaStream_t s = t.mra->ctx->stream;
     for (int d = t.levels() - 2; d >= 0; --d) {
         const int b = t.level_begin[d], e = t.level_begin[d + 1];
@@ -1001,7 +1001,23 @@ int mw_mra_create(mw_ctx ctx, int min_scale, const int* corner, const int* boxes
                     for (int j = 0; j < k; ++j) s += m->F[a * K2 + c * k + j] * m->W[j * k + q];
                     PF[a * K2 + c * k + q] = s;
                 }
+        // MV = blkdiag(E, E) F^T, E[q][j] = phi_j(x_q): compressed block -> values at the children's
+        // quadrature points (up to the scale factor 2^{3(n+1)/2}), used by the pointwise product
+        std::vector<double> MV(K2 * K2, 0.0), E(k * k), ph(k);
+        for (int q = 0; q < k; ++q) {
+            m->basis.values(m->basis.qx[q], ph.data());
+            for (int j = 0; j < k; ++j) E[q * k + j] = ph[j];
+        }
+        for (int c = 0; c < 2; ++c)
+            for (int q = 0; q < k; ++q)
+                for (int b = 0; b < K2; ++b) {
+                    double v = 0.0;
+                    for (int j = 0; j < k; ++j) v += E[q * k + j] * m->F[b * K2 + c * k + j];
+                    MV[(c * k + q) * K2 + b] = v;
+                }
         cudaStream_t s = ctx->stream;
+        m->d_MV = (double*)dalloc(ctx, sizeof(double) * K2 * K2);
+        MWB_CUDA(cudaMemcpyAsync(m->d_MV, MV.data(), sizeof(double) * K2 * K2, cudaMemcpyHostToDevice, s));
         m->d_F = (double*)dalloc(ctx, sizeof(double) * K2 * K2);
         m->d_FT = (double*)dalloc(ctx, sizeof(double) * K2 * K2);
         m->d_PF = (double*)dalloc(ctx, sizeof(double) * K2 * K2);
@@ -1020,6 +1036,7 @@ int mw_mra_destroy(mw_mra m) {
         dfree(m->ctx, m->d_F);
         dfree(m->ctx, m->d_FT);
         dfree(m->ctx, m->d_PF);
+        dfree(m->ctx, m->d_MV);
         cudaStreamSynchronize(m->ctx->stream);
         delete m;
     })

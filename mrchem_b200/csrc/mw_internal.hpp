@@ -59,6 +59,7 @@ struct Mra {
     double* d_F = nullptr;   // F
     double* d_FT = nullptr;  // F^T
     double* d_PF = nullptr;  // projection matrix F * blkdiag(W, W)
+    double* d_MV = nullptr;  // evaluation matrix blkdiag(E, E) * F^T (pointwise product)
     size_t bsize() const { return (size_t)8 * k * k * k; }
 };
 

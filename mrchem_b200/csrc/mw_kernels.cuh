@@ -53,6 +53,11 @@ void reduce_norms_many(const std::vector<Tree*>& ts, std::vector<double>& leaf2,
 void launch_rescale(Tree& t, double c, cudaStream_t s);
 double launch_dot(Tree& a, Tree& b, cudaStream_t s);
 
+// tree bookkeeping shared by the drivers (mw_api.cu)
+void tree_reserve(Tree& t, int need);
+void tree_make_roots(Tree& t);
+void tree_compress_bottom_up(Tree& t);
+
 // one refinement pass of a batched apply (mw_apply.cu)
 struct BatchTree {
     Tree* out = nullptr;

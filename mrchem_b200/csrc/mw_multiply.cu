@@ -1,0 +1,436 @@
+// mw_multiply.cu -- pointwise product of two functions on the device (multiwavelet multiplication)
+// and the union-grid helpers it is used with.
+//
+// Contract: mrcpp::multiply(prec, out, c, a, b[, maxIter]) and mrcpp::build_grid / copy_grid as called
+// at reference src/qmfunctions/qmfunction_utils.cpp:209-217 (union grid: build_grid(out, a),
+// build_grid(out, b), multiply(..., maxIter = 0); adaptive: multiply on the output's current grid,
+// refined until converged), src/qmoperators/two_electron/ExchangePotential.cpp:131,253,312 and
+// src/qmfunctions/density_utils.cpp:65-91 (square).
+//
+// Per output node (scale n): both factors are taken at scale n+1 on the node's 8 children -- the
+// reconstructed node block, or, where a factor's tree is coarser, the block generated below its
+// deepest existing ancestor (zero wavelets) -- evaluated at the children's k^3 Gauss-Legendre points
+// (one (2k)x(2k) matrix per dimension, MV = blkdiag(E, E) F^T), multiplied, and projected back and
+// compressed with the projection matrix PF = F blkdiag(W, W) and the scale c 2^{3(n+1)/2}.
+// Refinement follows the adaptive projection: after every pass the leaves whose wavelet norm exceeds
+// prec ||out|| 2^{-depth/2} are split and their children computed.
+//
+// Work per node: 9 to 9 + 6 L in-place pencil transforms of a (2k)^3 FP64 tensor (L = levels of
+// generation), 2 blocks read and 1 written: compute-bound on the FP64 pipe, off the apply's hot path.
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/mwb200.h"
+#include "mw_device.cuh"
+#include "mw_kernels.cuh"
+#include "mw_learned.cuh"
+
+namespace mwb {
+
+void set_last_error(const std::string& msg);
+
+struct MulTree {
+    uint64_t* okey;
+    double* ocoef;
+    double* onorm2;
+    double* ownorm2;
+    const uint64_t* ahk;
+    const int* ahv;
+    uint32_t ahcap;
+    const double* acoef;
+    const uint64_t* bhk;
+    const int* bhv;
+    uint32_t bhcap;
+    const double* bcoef;
+    double c;
+};
+
+struct MulItem {
+    int tree;
+    int node;
+};
+
+constexpr int kMulThreads = 256;
+
+template <int K>
+struct MulCfg {
+    using G = Geo<K>;
+    static constexpr int K2 = 2 * K;
+    static constexpr int KKK = K * K * K;
+    static constexpr int PER = (KKK + kMulThreads - 1) / kMulThreads;  // octant values per thread
+    static constexpr size_t SMEM = sizeof(double) * (2 * (size_t)G::VOL + 3 * K2 * K2 + 64) + 16;
+    static constexpr bool FITS = SMEM <= 227 * 1024;
+};
+
+// Block of a factor at node `key` into the padded tensor T: the node's own compressed block, or the
+// scaling-only block generated below the deepest existing ancestor.  `slot` is a shared int.
+template <int K>
+__device__ void mul_fetch(double* T, const double* FT, const uint64_t* hk, const int* hv, uint32_t hcap,
+                          const double* coef, uint64_t key, int* slot) {
+    using G = Geo<K>;
+    using C = MulCfg<K>;
+    const int depth = key_depth(key);
+    long long tr[3];
+    key_trans(key, tr);
+    if (threadIdx.x == 0) {
+        int idx = hlookup(hk, hv, hcap, key), da = depth;
+        while (idx < 0 && da > 0) {
+            --da;
+            const int sh = depth - da;
+            idx = hlookup(hk, hv, hcap, make_key(da, tr[0] >> sh, tr[1] >> sh, tr[2] >> sh));
+        }
+        slot[0] = idx;
+        slot[1] = da;
+    }
+    __syncthreads();
+    const int idx = slot[0], da = slot[1];
+    if (idx < 0) {  // outside the factor's roots (cannot happen on one world): zero
+        for (int e = threadIdx.x; e < G::VOL; e += blockDim.x) T[e] = 0.0;
+        return;
+    }
+    const double* blk = coef + (size_t)idx * G::BS;
+    for (int e = threadIdx.x; e < G::BS; e += blockDim.x) {
+        const int a = e % G::K2, b = (e / G::K2) % G::K2, c = e / (G::K2 * G::K2);
+        T[G::at(a, b, c)] = blk[e];
+    }
+    for (int lev = da; lev < depth; ++lev) {
+        // reconstruct to the children's scaling parts, keep the child on the path (zero wavelets)
+        __syncthreads();
+        pencil_transform<K, 0>(FT, T);
+        __syncthreads();
+        pencil_transform<K, 1>(FT, T);
+        __syncthreads();
+        pencil_transform<K, 2>(FT, T);
+        __syncthreads();
+        const int sh = depth - lev - 1;
+        const int cx = (int)((tr[0] >> sh) & 1), cy = (int)((tr[1] >> sh) & 1), cz = (int)((tr[2] >> sh) & 1);
+        double v[C::PER];
+#pragma unroll
+        for (int r = 0; r < C::PER; ++r) {
+            const int e = threadIdx.x + r * kMulThreads;
+            v[r] = 0.0;
+            if (e < C::KKK) {
+                const int x = e % K, y = (e / K) % K, z = e / (K * K);
+                v[r] = T[G::at(cx * K + x, cy * K + y, cz * K + z)];
+            }
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < G::VOL; e += blockDim.x) T[e] = 0.0;
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < C::PER; ++r) {
+            const int e = threadIdx.x + r * kMulThreads;
+            if (e < C::KKK) {
+                const int x = e % K, y = (e / K) % K, z = e / (K * K);
+                T[G::at(x, y, z)] = v[r];
+            }
+        }
+    }
+}
+
+template <int K>
+__global__ void __launch_bounds__(kMulThreads) k_mul(const MulItem* __restrict__ items, const MulTree* __restrict__ trees,
+                                                     const double* __restrict__ MVg, const double* __restrict__ PFg,
+                                                     const double* __restrict__ FTg, int n0) {
+    using G = Geo<K>;
+    constexpr int K2 = G::K2;
+    extern __shared__ __align__(16) double msm[];
+    double* TA = msm;
+    double* TB = TA + G::VOL;
+    double* MV = TB + G::VOL;
+    double* PF = MV + K2 * K2;
+    double* FT = PF + K2 * K2;
+    double* red = FT + K2 * K2;
+    int* slot = reinterpret_cast<int*>(red + 64);
+    const MulItem it = items[blockIdx.x];
+    const MulTree& T = trees[it.tree];
+    for (int i = threadIdx.x; i < K2 * K2; i += blockDim.x) {
+        MV[i] = MVg[i];
+        PF[i] = PFg[i];
+        FT[i] = FTg[i];
+    }
+    const uint64_t key = T.okey[it.node];
+    __syncthreads();
+    mul_fetch<K>(TA, FT, T.ahk, T.ahv, T.ahcap, T.acoef, key, slot);
+    __syncthreads();
+    mul_fetch<K>(TB, FT, T.bhk, T.bhv, T.bhcap, T.bcoef, key, slot);
+    __syncthreads();
+    // values of both factors at the children's quadrature points
+    pencil_transform<K, 0>(MV, TA);
+    pencil_transform<K, 0>(MV, TB);
+    __syncthreads();
+    pencil_transform<K, 1>(MV, TA);
+    pencil_transform<K, 1>(MV, TB);
+    __syncthreads();
+    pencil_transform<K, 2>(MV, TA);
+    pencil_transform<K, 2>(MV, TB);
+    __syncthreads();
+    for (int e = threadIdx.x; e < G::VOL; e += blockDim.x) TA[e] *= TB[e];
+    __syncthreads();
+    pencil_transform<K, 0>(PF, TA);
+    __syncthreads();
+    pencil_transform<K, 1>(PF, TA);
+    __syncthreads();
+    // last dimension in registers, scaled, written with the block norms
+    const double fac = T.c * exp2(1.5 * (double)(n0 + key_depth(key) + 1));
+    double* dst = T.ocoef + (size_t)it.node * G::BS;
+    double n2 = 0.0, w2 = 0.0;
+    for (int p = threadIdx.x; p < G::NP; p += blockDim.x) {
+        const int a = p % K2, b = p / K2;
+        double x[K2];
+#pragma unroll
+        for (int i = 0; i < K2; ++i) x[i] = TA[G::at(a, b, i)];
+#pragma unroll 1
+        for (int o = 0; o < K2; ++o) {
+            double s = 0.0;
+#pragma unroll
+            for (int i = 0; i < K2; ++i) s = fma(PF[o * K2 + i], x[i], s);
+            s *= fac;
+            dst[a + K2 * (b + K2 * o)] = s;
+            n2 += s * s;
+            if (!(a < K && b < K && o < K)) w2 += s * s;
+        }
+    }
+    block_sum2(n2, w2, red);
+    if (threadIdx.x == 0) {
+        T.onorm2[it.node] = n2;
+        T.ownorm2[it.node] = w2;
+    }
+}
+
+#define MWB_MUL_DISPATCH_K(k, F)                                                                \
+    switch (k) {                                                                                \
+        case 4: F(4); break;                                                                    \
+        case 5: F(5); break;                                                                    \
+        case 6: F(6); break;                                                                    \
+        case 7: F(7); break;                                                                    \
+        case 8: F(8); break;                                                                    \
+        case 9: F(9); break;                                                                    \
+        case 10: F(10); break;                                                                  \
+        case 11: F(11); break;                                                                  \
+        default: throw Error(MW_ERR_ARG, "multiply supports k = 4..11 (order 3..10)");          \
+    }
+
+namespace {
+
+inline double mul_split_threshold(double prec, double ref, int depth) { return prec * ref * std::pow(2.0, -0.5 * depth); }
+
+std::vector<uint64_t> host_keys(Tree& t, cudaStream_t s) {
+    std::vector<uint64_t> k(t.n);
+    if (t.n > 0) MWB_CUDA(cudaMemcpyAsync(k.data(), t.key, sizeof(uint64_t) * t.n, cudaMemcpyDeviceToHost, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
+    return k;
+}
+
+// Append nodes with the given keys (zero blocks) and restore the level order (parents before
+// children, keys ascending); returns the tree's keys in the new order.
+std::vector<uint64_t> tree_add_keys(Tree& t, const std::vector<uint64_t>& add, cudaStream_t s) {
+    if (!add.empty()) {
+        const size_t BS = t.mra->bsize();
+        const int n0 = t.n, na = (int)add.size();
+        tree_reserve(t, n0 + na);
+        MWB_CUDA(cudaMemcpyAsync(t.key + n0, add.data(), sizeof(uint64_t) * na, cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemsetAsync(t.coef + (size_t)n0 * BS, 0, sizeof(double) * BS * na, s));
+        MWB_CUDA(cudaMemsetAsync(t.norm2 + n0, 0, sizeof(double) * na, s));
+        MWB_CUDA(cudaMemsetAsync(t.wnorm2 + n0, 0, sizeof(double) * na, s));
+        MWB_CUDA(cudaStreamSynchronize(s));  // `add` may leave scope
+        t.n = n0 + na;
+    }
+    std::vector<uint64_t> keys = host_keys(t, s);
+    trees_rebuild({&t}, {std::vector<char>(t.n, 1)}, {keys});
+    std::sort(keys.begin(), keys.end());
+    return keys;
+}
+
+std::vector<uint64_t> children_keys(uint64_t k) {
+    long long tr[3];
+    host_key_trans(k, tr);
+    const int d = (int)(k >> 59);
+    std::vector<uint64_t> c;
+    for (int q = 0; q < 8; ++q)
+        c.push_back(host_make_key(d + 1, 2 * tr[0] + (q & 1), 2 * tr[1] + ((q >> 1) & 1), 2 * tr[2] + ((q >> 2) & 1)));
+    return c;
+}
+
+// extend the grid of `out` by the grid of `inp` (both on one world)
+void build_grid(Tree& out, Tree& inp) {
+    cudaStream_t s = out.mra->ctx->stream;
+    if (out.n == 0) tree_make_roots(out);
+    const std::vector<uint64_t> ko = host_keys(out, s), ki = host_keys(inp, s);
+    std::vector<uint64_t> add;
+    std::vector<uint64_t> so(ko);
+    std::sort(so.begin(), so.end());
+    for (uint64_t k : ki)
+        if (!std::binary_search(so.begin(), so.end(), k)) add.push_back(k);
+    tree_add_keys(out, add, s);
+}
+
+// out[i] = c[i] a[i] b[i], lock-step passes over the batch
+void multiply_batched(double prec, int n, Tree** out, const double* c, Tree** a, Tree** b, int max_iter) {
+    const Mra* m = a[0]->mra;
+    Ctx* ctx = m->ctx;
+    cudaStream_t s = ctx->stream;
+    const int K = m->k;
+    for (int i = 0; i < n; ++i) {
+        if (!out[i] || !a[i] || !b[i]) throw Error(MW_ERR_ARG, "null tree");
+        if (out[i]->mra != m || a[i]->mra != m || b[i]->mra != m) throw Error(MW_ERR_ARG, "trees on different worlds");
+        if (a[i]->n == 0 || b[i]->n == 0) throw Error(MW_ERR_STATE, "empty input tree");
+        for (int j = 0; j < n; ++j)
+            if (j != i && out[j] == out[i]) throw Error(MW_ERR_ARG, "output tree listed twice");
+        if (out[i] == a[i] || out[i] == b[i]) throw Error(MW_ERR_ARG, "output tree is also an input");
+    }
+    // work: the current leaves of every output tree (roots for an empty tree)
+    std::vector<std::vector<int>> work(n);
+    std::vector<std::vector<uint64_t>> keys(n);
+    for (int i = 0; i < n; ++i) {
+        if (out[i]->n == 0) tree_make_roots(*out[i]);
+        std::vector<int> c0(out[i]->n);
+        MWB_CUDA(cudaMemcpyAsync(c0.data(), out[i]->child0, sizeof(int) * out[i]->n, cudaMemcpyDeviceToHost, s));
+        MWB_CUDA(cudaStreamSynchronize(s));
+        for (int q = 0; q < out[i]->n; ++q)
+            if (c0[q] < 0) work[i].push_back(q);
+        keys[i] = host_keys(*out[i], s);
+    }
+    std::vector<MulTree> mt(n);
+    MulTree* d_trees = (MulTree*)dalloc(ctx, sizeof(MulTree) * n);
+    for (int iter = 0;; ++iter) {
+        std::vector<MulItem> items;
+        for (int i = 0; i < n; ++i) {
+            Tree& o = *out[i];
+            mt[i] = MulTree{o.key, o.coef, o.norm2, o.wnorm2, a[i]->hkey, a[i]->hval, a[i]->hcap, a[i]->coef,
+                            b[i]->hkey, b[i]->hval, b[i]->hcap, b[i]->coef, c ? c[i] : 1.0};
+            for (int q : work[i]) items.push_back({i, q});
+        }
+        if (items.empty()) break;
+        MWB_CUDA(cudaMemcpyAsync(d_trees, mt.data(), sizeof(MulTree) * n, cudaMemcpyHostToDevice, s));
+        MulItem* d_items = (MulItem*)dalloc(ctx, sizeof(MulItem) * items.size());
+        MWB_CUDA(cudaMemcpyAsync(d_items, items.data(), sizeof(MulItem) * items.size(), cudaMemcpyHostToDevice, s));
+#define L_MUL(KK)                                                                                                 \
+    {                                                                                                             \
+        const size_t smem = MulCfg<KK>::SMEM;                                                                     \
+        MWB_CUDA(cudaFuncSetAttribute(k_mul<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));        \
+        k_mul<KK><<<(unsigned)items.size(), kMulThreads, smem, s>>>(d_items, d_trees, m->d_MV, m->d_PF, m->d_FT, \
+                                                                     m->n0);                                      \
+    }
+        MWB_MUL_DISPATCH_K(K, L_MUL)
+#undef L_MUL
+        MWB_CUDA(cudaGetLastError());
+        ctx->launches++;
+        MWB_CUDA(cudaStreamSynchronize(s));  // the item list leaves scope
+        dfree(ctx, d_items);
+        if (prec <= 0.0 || (max_iter >= 0 && iter >= max_iter)) break;
+        // split the computed nodes whose wavelet norm exceeds prec ||out|| 2^{-depth/2}
+        std::vector<Tree*> ts(out, out + n);
+        std::vector<double> leaf2, max2;
+        reduce_norms_many(ts, leaf2, max2, s);
+        bool any = false;
+        for (int i = 0; i < n; ++i) {
+            Tree& o = *out[i];
+            std::vector<double> w2(o.n);
+            MWB_CUDA(cudaMemcpyAsync(w2.data(), o.wnorm2, sizeof(double) * o.n, cudaMemcpyDeviceToHost, s));
+            MWB_CUDA(cudaStreamSynchronize(s));
+            const double ref = std::sqrt(leaf2[i]);
+            std::vector<uint64_t> add;
+            for (int q : work[i]) {
+                const int d = (int)(keys[i][q] >> 59);
+                if (d < m->depth_limit && std::sqrt(w2[q]) > mul_split_threshold(prec, ref, d)) {
+                    const std::vector<uint64_t> ch = children_keys(keys[i][q]);
+                    add.insert(add.end(), ch.begin(), ch.end());
+                }
+            }
+            work[i].clear();
+            if (add.empty()) continue;
+            any = true;
+            keys[i] = tree_add_keys(o, add, s);
+            std::sort(add.begin(), add.end());
+            for (uint64_t k : add)
+                work[i].push_back((int)(std::lower_bound(keys[i].begin(), keys[i].end(), k) - keys[i].begin()));
+        }
+        if (!any) break;
+    }
+    dfree(ctx, d_trees);
+    for (int i = 0; i < n; ++i) {
+        tree_compress_bottom_up(*out[i]);
+        launch_node_norms(*out[i], 0, out[i]->n, s);
+    }
+    MWB_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace
+}  // namespace mwb
+
+struct mw_tree_s : mwb::Tree {};
+
+#define MWM_TRY(...)                                \
+    try {                                           \
+        __VA_ARGS__;                                \
+        return MW_OK;                               \
+    } catch (const mwb::Error& e) {                 \
+        mwb::set_last_error(e.what());              \
+        return e.code;                              \
+    } catch (const std::exception& e) {             \
+        mwb::set_last_error(e.what());              \
+        return MW_ERR_STATE;                        \
+    }
+#define MWM_ARG(cond, msg) \
+    if (!(cond)) throw mwb::Error(MW_ERR_ARG, msg)
+
+extern "C" {
+
+int mw_multiply(double prec, mw_tree out, double c, mw_tree a, mw_tree b, int max_iter) {
+    MWM_TRY({
+        MWM_ARG(out && a && b, "null tree");
+        MWB_CUDA(cudaSetDevice(a->mra->ctx->device));
+        mwb::Tree* o = out;
+        mwb::Tree* pa = a;
+        mwb::Tree* pb = b;
+        mwb::multiply_batched(prec, 1, &o, &c, &pa, &pb, max_iter);
+    })
+}
+
+int mw_multiply_batched(int n, double prec, mw_tree* out, const double* c, mw_tree* a, mw_tree* b, int max_iter) {
+    MWM_TRY({
+        MWM_ARG(n > 0 && out && a && b, "null pointer or empty batch");
+        MWM_ARG(a[0], "null input tree");
+        MWB_CUDA(cudaSetDevice(a[0]->mra->ctx->device));
+        std::vector<mwb::Tree*> o(n), pa(n), pb(n);
+        for (int q = 0; q < n; ++q) {
+            o[q] = out[q];
+            pa[q] = a[q];
+            pb[q] = b[q];
+        }
+        mwb::multiply_batched(prec, n, o.data(), c, pa.data(), pb.data(), max_iter);
+    })
+}
+
+int mw_square(double prec, mw_tree out, mw_tree a, int max_iter) { return mw_multiply(prec, out, 1.0, a, a, max_iter); }
+
+int mw_tree_build_grid(mw_tree out, mw_tree inp) {
+    MWM_TRY({
+        MWM_ARG(out && inp, "null tree");
+        MWM_ARG(out->mra == inp->mra, "trees on different worlds");
+        MWM_ARG(out != inp, "a tree cannot extend itself");
+        MWB_CUDA(cudaSetDevice(inp->mra->ctx->device));
+        mwb::build_grid(*out, *inp);
+    })
+}
+
+int mw_tree_clear(mw_tree t) {
+    MWM_TRY({
+        MWM_ARG(t, "null tree");
+        t->n = 0;
+        t->level_begin.clear();
+        if (t->hcap > 0) mwb::launch_hash_reset(*t, t->mra->ctx->stream);
+        MWB_CUDA(cudaStreamSynchronize(t->mra->ctx->stream));
+    })
+}
+
+int mw_tree_copy_grid(mw_tree out, mw_tree inp) {
+    const int st = mw_tree_clear(out);
+    return st != MW_OK ? st : mw_tree_build_grid(out, inp);
+}
+
+}  // extern "C"

@@ -71,6 +71,12 @@ SYMBOLS = [
     ("mw_apply", ctypes.c_int, [ctypes.c_double, _vp, _vp, _vp, ctypes.c_int]),
     ("mw_apply_batched", ctypes.c_int, [ctypes.c_int, ctypes.c_double, _vpp, _vpp, _vpp, ctypes.c_int]),
     ("mw_apply_stats", ctypes.c_int, [_vp, _lp]),
+    ("mw_multiply", ctypes.c_int, [ctypes.c_double, _vp, ctypes.c_double, _vp, _vp, ctypes.c_int]),
+    ("mw_multiply_batched", ctypes.c_int, [ctypes.c_int, ctypes.c_double, _vpp, _dp, _vpp, _vpp, ctypes.c_int]),
+    ("mw_square", ctypes.c_int, [ctypes.c_double, _vp, _vp, ctypes.c_int]),
+    ("mw_tree_build_grid", ctypes.c_int, [_vp, _vp]),
+    ("mw_tree_copy_grid", ctypes.c_int, [_vp, _vp]),
+    ("mw_tree_clear", ctypes.c_int, [_vp]),
     ("mw_mlp_create", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint, _vpp]),
     ("mw_mlp_destroy", ctypes.c_int, [_vp]),
     ("mw_mlp_nparams", ctypes.c_int, [_vp, _lp, _ip]),
@@ -353,6 +359,45 @@ def apply(prec, out: FunctionTree, op: ConvolutionOperator, inp: FunctionTree, f
     st = np.zeros(4, np.int64)
     _check(_lib.mw_apply_stats(out._h, st.ctypes.data_as(_lp)))
     return tuple(int(x) for x in st)
+
+
+def multiply(prec, out: FunctionTree, c, a: FunctionTree, b: FunctionTree, max_iter=-1):
+    """out = c a b: mrcpp::multiply(prec, out, c, a, b, maxIter) (reference
+    src/qmfunctions/qmfunction_utils.cpp:209-217).  `out` keeps its grid (roots when empty) and is
+    refined while leaves fail the wavelet test, at most max_iter passes (-1: until converged)."""
+    _check(_lib.mw_multiply(float(prec), out._h, float(c), a._h, b._h, int(max_iter)))
+
+
+def multiply_batched(prec, outs, coefs, a_trees, b_trees, max_iter=-1):
+    """outs[i] = coefs[i] a_trees[i] b_trees[i], refinement passes in lock-step over the batch"""
+    n = len(outs)
+    if not (len(a_trees) == len(b_trees) == n):
+        raise MWError("batch lists must have equal length")
+    o = (ctypes.c_void_p * n)(*[t._h.value for t in outs])
+    a = (ctypes.c_void_p * n)(*[t._h.value for t in a_trees])
+    b = (ctypes.c_void_p * n)(*[t._h.value for t in b_trees])
+    c = None if coefs is None else np.ascontiguousarray(coefs, dtype=np.float64)
+    _check(_lib.mw_multiply_batched(n, float(prec), o, None if c is None else _d(c), a, b, int(max_iter)))
+
+
+def square(prec, out: FunctionTree, a: FunctionTree, max_iter=-1):
+    """out = a^2: mrcpp::square (reference src/qmfunctions/density_utils.cpp:74)"""
+    _check(_lib.mw_square(float(prec), out._h, a._h, int(max_iter)))
+
+
+def build_grid(out: FunctionTree, inp: FunctionTree):
+    """extend the grid of `out` by that of `inp`: mrcpp::build_grid (qmfunction_utils.cpp:211-212)"""
+    _check(_lib.mw_tree_build_grid(out._h, inp._h))
+
+
+def copy_grid(out: FunctionTree, inp: FunctionTree):
+    """out gets the grid of inp (blocks zero): mrcpp::copy_grid (density_utils.cpp:73)"""
+    _check(_lib.mw_tree_copy_grid(out._h, inp._h))
+
+
+def clear(tree: FunctionTree):
+    """empty the tree"""
+    _check(_lib.mw_tree_clear(tree._h))
 
 
 class ProposalNet:

@@ -1209,6 +1209,121 @@ double evalf(const Tree& tr, const double* r) {
     return s * std::pow(2.0, 1.5 * n1);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Pointwise product of two functions (multiwavelet multiplication)
+// ---------------------------------------------------------------------------------------------
+// Contract: mrcpp::multiply(prec, out, c, a, b[, maxIter]) as called at
+// src/qmfunctions/qmfunction_utils.cpp:209-217 (union grid: build_grid(out, a), build_grid(out, b),
+// then multiply with maxIter = 0; adaptive: multiply on the output's current grid, refined until
+// converged) and src/qmoperators/two_electron/ExchangePotential.cpp:131,253,312.
+// Method (restated from the MW literature, not from MRCPP): for an output node at scale n both
+// factors are taken at scale n+1 on the node's 8 children -- the reconstructed node block, or, where
+// a factor's tree is coarser, the block generated below its deepest existing ancestor (zero
+// wavelets) -- evaluated at the children's k^3 Gauss-Legendre points, multiplied, projected back
+// with the quadrature of the adaptive projection and compressed into the node block.  Refinement
+// uses the projection's wavelet criterion with the norm of the current product.
+
+// compressed block of `tr` at (depth, t): the node's own block, or the scaling-only block generated
+// below the deepest existing ancestor (a leaf)
+void block_at(const Tree& tr, int depth, const int64_t t[3], double* out) {
+    const MRA& mra = *tr.mra;
+    const int k = mra.k(), K2 = 2 * k;
+    const size_t BS = mra.bsize();
+    const int idx = tr.find(depth, t);
+    if (idx >= 0) {
+        std::memcpy(out, tr.nodes[idx].c.data(), sizeof(double) * BS);
+        return;
+    }
+    int leaf = -1;
+    for (int da = depth - 1; da >= 0 && leaf < 0; --da) {
+        int64_t ta[3] = {t[0] >> (depth - da), t[1] >> (depth - da), t[2] >> (depth - da)};
+        leaf = tr.find(da, ta);
+    }
+    std::fill(out, out + BS, 0.0);
+    if (leaf < 0) return;
+    std::vector<double> s((size_t)k * k * k);
+    generate_node(tr, leaf, depth, t, s.data());
+    for (int z = 0; z < k; ++z)
+        for (int y = 0; y < k; ++y)
+            for (int x = 0; x < k; ++x) out[x + K2 * (y + K2 * z)] = s[x + k * (y + k * z)];
+}
+
+// block of the product c a b at output node (depth, t)
+void multiply_node(const MRA& mra, double c, const Tree& a, const Tree& b, int depth, const int64_t t[3],
+                   double* out) {
+    const int k = mra.k(), K2 = 2 * k;
+    const size_t BS = mra.bsize();
+    const Basis& B = mra.basis;
+    // EE = blockdiag(E, E), E[q][j] = phi_j(x_q);  WW = blockdiag(W, W), W[j][q] = w_q phi_j(x_q)
+    std::vector<double> EE((size_t)K2 * K2, 0.0), WW((size_t)K2 * K2, 0.0);
+    for (int h = 0; h < 2; ++h)
+        for (int q = 0; q < k; ++q)
+            for (int j = 0; j < k; ++j) {
+                const double pj = B.phi(j, B.qx[q]);
+                EE[(h * k + q) * K2 + h * k + j] = pj;
+                WW[(h * k + j) * K2 + h * k + q] = B.qw[q] * pj;
+            }
+    std::vector<double> ba(BS), bb(BS), ra(BS), rb(BS), va(BS), vb(BS);
+    block_at(a, depth, t, ba.data());
+    block_at(b, depth, t, bb.data());
+    transform3(B.F, k, true, ba.data(), ra.data());
+    transform3(B.F, k, true, bb.data(), rb.data());
+    transform3(EE, k, false, ra.data(), va.data());
+    transform3(EE, k, false, rb.data(), vb.data());
+    for (size_t i = 0; i < BS; ++i) va[i] *= vb[i];
+    transform3(WW, k, false, va.data(), ra.data());
+    const double fac = c * std::pow(2.0, 1.5 * (mra.n0 + depth + 1));
+    for (size_t i = 0; i < BS; ++i) ra[i] *= fac;
+    transform3(B.F, k, false, ra.data(), out);
+}
+
+// out = c a b.  `out` keeps its current grid (roots if empty); every leaf is computed, then leaves
+// whose wavelet norm exceeds prec ||out|| 2^{-depth/2} are split and their children computed, at
+// most max_iter times (max_iter < 0: until no split; prec <= 0: no refinement).
+void multiply(double prec, Tree& out, double c, const Tree& a, const Tree& b, int max_iter) {
+    const MRA& mra = *a.mra;
+    out.mra = a.mra;
+    if (out.nodes.empty()) out.make_roots();
+    std::vector<int> work;
+    for (int i : out.level_order())
+        if (out.nodes[i].child0 < 0) work.push_back(i);
+    for (int iter = 0; !work.empty(); ++iter) {
+#pragma omp parallel for schedule(dynamic, 1)
+        for (size_t q = 0; q < work.size(); ++q) {
+            Node& nd = out.nodes[work[q]];
+            multiply_node(mra, c, a, b, nd.depth, nd.t, nd.c.data());
+        }
+        if (prec <= 0.0 || (max_iter >= 0 && iter >= max_iter)) break;
+        const double ref = std::sqrt(out.square_norm());
+        std::vector<int> next;
+        for (int i : work) {
+            const Node& nd = out.nodes[i];
+            if (nd.depth >= mra.max_depth) continue;
+            const double w = std::sqrt(wavelet_sq_norm(nd.c.data(), mra.k()));
+            if (w > split_threshold(prec, ref, nd.depth)) {
+                out.split(i);
+                const int c0 = out.nodes[i].child0;
+                for (int ch = 0; ch < 8; ++ch) next.push_back(c0 + ch);
+            }
+        }
+        work.swap(next);
+    }
+    compress_bottom_up(out);
+}
+
+// extend the grid of `out` by the grid of `inp` (union; new nodes have zero blocks)
+void build_grid(Tree& out, const Tree& inp) {
+    out.mra = inp.mra;
+    if (out.nodes.empty()) out.make_roots();
+    for (int i : inp.level_order()) {
+        const Node& nd = inp.nodes[i];
+        if (nd.depth == 0 || out.find(nd.depth, nd.t) >= 0) continue;
+        int64_t tp[3] = {nd.t[0] >> 1, nd.t[1] >> 1, nd.t[2] >> 1};
+        const int p = out.find(nd.depth - 1, tp);
+        if (p >= 0 && out.nodes[p].child0 < 0) out.split(p);
+    }
+}
+
 Func make_func(int type, const double* p) {
     Func f;
     if (type == 1) {
@@ -1358,6 +1473,17 @@ int oracle_apply(double prec, void* out, void* op, void* inp, long long* stats) 
         stats[3] = st.lines_yz;
         stats[4] = st.lines_z;
     }
+    return (int)((Tree*)out)->nodes.size();
+}
+
+// out = c a b (mrcpp::multiply contract); returns the number of output nodes
+int oracle_multiply(double prec, void* out, double c, void* a, void* b, int max_iter) {
+    multiply(prec, *(Tree*)out, c, *(Tree*)a, *(Tree*)b, max_iter);
+    return (int)((Tree*)out)->nodes.size();
+}
+// union of grids (mrcpp::build_grid contract); returns the number of nodes of `out`
+int oracle_build_grid(void* out, void* inp) {
+    build_grid(*(Tree*)out, *(Tree*)inp);
     return (int)((Tree*)out)->nodes.size();
 }
 

@@ -62,6 +62,8 @@ def lib():
         L.oracle_operator_ns.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp]
         L.oracle_scaling_matrix.argtypes = [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp]
         L.oracle_apply.argtypes = [ctypes.c_double, _vp, _vp, _vp, _lp]
+        L.oracle_multiply.argtypes = [ctypes.c_double, _vp, ctypes.c_double, _vp, _vp, ctypes.c_int]
+        L.oracle_build_grid.argtypes = [_vp, _vp]
         _lib = L
     return _lib
 
@@ -233,3 +235,14 @@ def apply_line_stats(prec, out, op, inp):
     st = np.zeros(8, np.int64)
     lib().oracle_apply(float(prec), out._h, op._h, inp._h, st.ctypes.data_as(_lp))
     return int(st[0]), int(st[3]), int(st[4])
+
+
+def multiply(prec, out: FunctionTree, c, a: FunctionTree, b: FunctionTree, max_iter=-1):
+    """out = c a b (mrcpp::multiply contract: qmfunction_utils.cpp:209-217, ExchangePotential.cpp:131);
+    returns the number of output nodes"""
+    return lib().oracle_multiply(float(prec), out._h, float(c), a._h, b._h, int(max_iter))
+
+
+def build_grid(out: FunctionTree, inp: FunctionTree):
+    """extend the grid of `out` by that of `inp` (mrcpp::build_grid, qmfunction_utils.cpp:211-212)"""
+    return lib().oracle_build_grid(out._h, inp._h)

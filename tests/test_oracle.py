@@ -201,3 +201,32 @@ def test_oracle_golden_regression(oracle_mod):
     keys = sorted((int(d), *map(int, t)) for d, t in zip(ex["depth"], ex["trans"]))
     assert np.array_equal(np.array(keys), g["out_keys"])
     assert abs(out.square_norm() - float(g["out_norm2"])) < 1e-10 * float(g["out_norm2"])
+
+
+def test_oracle_multiply_gaussian_product(oracle_mod):
+    """The MW product of two Gaussians against the closed form: the norm of
+    exp(-a1|r-c1|^2) exp(-a2|r-c2|^2), point values, and the union-grid form (maxIter 0)."""
+    O = oracle_mod
+    m = O.MultiResolutionAnalysis(*WORLD, 5, 12)
+    a1, c1, a2, c2 = 2.0, np.array([0.1, -0.2, 0.3]), 3.0, np.array([-0.3, 0.2, 0.1])
+    A, B = O.FunctionTree(m), O.FunctionTree(m)
+    O.project(1e-4, A, O.gauss_params([1.0], [a1], [c1]))
+    O.project(1e-4, B, O.gauss_params([1.0], [a2], [c2]))
+    exact2 = (np.pi / (2 * a1 + 2 * a2)) ** 1.5 * np.exp(-2 * a1 * a2 / (a1 + a2) * np.sum((c1 - c2) ** 2))
+    P = O.FunctionTree(m)
+    O.multiply(1e-4, P, 1.0, A, B)
+    assert abs(P.square_norm() - exact2) < 1e-8 * exact2
+    rng = np.random.default_rng(0)
+    for _ in range(50):
+        r = rng.uniform(-1.0, 1.0, 3)
+        ex = np.exp(-a1 * np.sum((r - c1) ** 2) - a2 * np.sum((r - c2) ** 2))
+        assert abs(P.evalf(r) - ex) < 1e-5
+    U = O.FunctionTree(m)
+    O.build_grid(U, A)
+    O.build_grid(U, B)
+    ka = {(int(d), *map(int, t)) for e in (A.export(False), B.export(False)) for d, t in zip(e["depth"], e["trans"])}
+    eu = U.export(False)
+    assert {(int(d), *map(int, t)) for d, t in zip(eu["depth"], eu["trans"])} == ka
+    O.multiply(-1.0, U, 2.0, A, B, 0)
+    assert U.nnodes() == len(ka)
+    assert abs(U.square_norm() - 4.0 * exact2) < 1e-8 * exact2
