@@ -15,6 +15,7 @@ Prints one JSON line on rank 0.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -45,6 +46,11 @@ def parse():
     p.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--tau", type=float, default=0.97, help="proposal threshold of the learned apply")
+    p.add_argument("--reserve-gib", type=int, default=64,
+                   help="device memory pool reserved up front (GiB): the working set of the step")
+    p.add_argument("--workload", default="helmholtz", choices=["helmholtz", "exchange"],
+                   help="helmholtz: 32-orbital Helmholtz batch (the headline); exchange: 16 orbitals -> 136 "
+                        "pair products, each followed by a Poisson apply")
     return p.parse_args()
 
 
@@ -58,7 +64,7 @@ def measured_peaks():
 class Clocks:
     """nvidia-smi sampling (200 ms) during the timed region."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -66,6 +72,7 @@ class Clocks:
         self.device = device
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.p = None
+        self.marks = []
 
     def __enter__(self):
         try:
@@ -76,6 +83,10 @@ class Clocks:
             self.p = None
         return self
 
+    def mark(self):
+        """record the wall time of a boundary of the timed region (samples outside are dropped)"""
+        self.marks.append(time.time())
+
     def __exit__(self, *a):
         if self.p is not None:
             self.p.terminate()
@@ -85,19 +96,31 @@ class Clocks:
                 self.p.kill()
 
     def summary(self):
+        """median SM clock, max clock and throttle reasons of the samples inside the timed region
+        (all samples when the region was shorter than the sampling period)"""
+        import datetime
+
         self.f.flush()
         rows = []
         for line in open(self.f.name):
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 9:
+            if len(parts) >= 10:
+                try:
+                    parts[0] = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                except ValueError:
+                    parts[0] = None
                 rows.append(parts)
         os.unlink(self.f.name)
+        if len(self.marks) >= 2:
+            inside = [r for r in rows if r[0] is not None and self.marks[0] <= r[0] <= self.marks[-1]]
+            if inside:
+                rows = inside
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[6 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows)}
 
@@ -188,6 +211,7 @@ def run_gpu(args):
 
     stream = torch.cuda.Stream()
     ctx = G.Context(local, stream=stream.cuda_stream)
+    ctx.reserve(args.reserve_gib << 30)  # the whole working set, so that no timed step grows the pool
     m = G.MultiResolutionAnalysis(W.WORLD["min_scale"], W.WORLD["corner"], W.WORLD["boxes"], args.order, 15,
                                   ctx=ctx)
     orbs, mus = workload(rank, args.orbitals)
@@ -204,22 +228,35 @@ def run_gpu(args):
         if world > 1:
             torch.distributed.barrier()
 
+    step_ms = []  # per timed region: device time of each step
+
     def timed(run):
-        """W untimed + K timed steps of `run()` (returns the step's contracted triples)."""
-        for _ in range(args.warmup):
-            run()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        barrier()
-        torch.cuda.synchronize()
-        ctx.profile(True)
-        trip = 0
+        """W untimed + K timed steps of `run()` (returns the step's contracted triples).  The clock
+        sampler starts before the warm-up steps, so that its start-up (NVML initialisation) is over
+        when the timed region begins."""
         with Clocks(local) as clk:
+            for _ in range(args.warmup):
+                run()
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+            gc.collect()  # no collector pass (tree destructors synchronise the stream) inside the region
+            gc.disable()
+            barrier()
+            torch.cuda.synchronize()
+            clk.mark()
+            ctx.profile(True)
+            trip = 0
             ev0.record(stream)
-            for _ in range(args.steps):
+            evs[0].record(stream)
+            for q in range(args.steps):
                 trip += run()
+                evs[q + 1].record(stream)
             ev1.record(stream)
             torch.cuda.synchronize()
+            clk.mark()
+            gc.enable()
+        step_ms.append([evs[q].elapsed_time(evs[q + 1]) for q in range(args.steps)])
         barrier()
         ms_ = ev0.elapsed_time(ev1)
         prof = ctx.profile_read()
@@ -265,12 +302,13 @@ def run_gpu(args):
     ms, triples, prof32, clocks = timed(run_learned)
     launches, apply_launches, apply_ms = prof32
     # error of the mixed + learned result against the FP64 one: ||g - g64|| / ||g64|| per orbital
+    # (from the coefficient differences, mw_tree_distance: no cancellation)
     rel_err = 0.0
     same_tree = True
     for a, b in zip(outsL, outs):
-        na, nb, ab = a.square_norm(), b.square_norm(), G.dot(a, b)
-        rel_err = max(rel_err, np.sqrt(max(na + nb - 2 * ab, 0.0) / nb))
+        rel_err = max(rel_err, G.distance(a, b) / np.sqrt(b.square_norm()))
         same_tree &= a.nnodes() == b.nnodes()
+    rel_err_mixed = max(G.distance(a, b) / np.sqrt(b.square_norm()) for a, b in zip(outs32, outs))
     total_applies = args.orbitals * args.steps * world
     value = total_applies / (ms / 1e3)
 
@@ -334,15 +372,18 @@ def run_gpu(args):
                            "triples_per_step": trip64 // max(1, args.steps)},
             "mixed_no_learning": {"value": args.orbitals * args.steps * world / (ms32 / 1e3), "unit": "applies/s",
                                   "ms_per_step": ms32 / args.steps, "kernel_ms_per_step": prof32m[2] / args.steps},
+            "step_ms": {"plain_fp64": step_ms[0], "mixed_no_learning": step_ms[1], "mixed_learned": step_ms[2]},
             "speedup_vs_plain_fp64": ms64 / ms,
             "rel_error_vs_fp64": rel_err,
+            "rel_error_vs_fp64_mixed_no_learning": rel_err_mixed,
+            "rel_error_definition": "max over orbitals of ||g - g_fp64|| / ||g_fp64|| (coefficient differences)",
             "same_node_count_as_fp64": bool(same_tree),
             "learned": {"passes": lstats.get("passes"), "proposed": lstats.get("proposed"),
                         "pruned": lstats.get("pruned"), "missed": lstats.get("missed"),
                         "out_nodes": lstats.get("out_nodes"), "train_rows": n_train, "train_positive": n_pos,
                         "train_loss": train_loss, "train_s": t_train, "tau": args.tau,
                         "train_data": "plain applies of 32 other seeded orbitals (seed 1007)"},
-            "roofline": {"bound": "tensor", "kernel": "k_bapply<10,float>", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "tensor", "kernel": "k_gapply<10,float>", "achieved": achieved, "peak": peak,
                          "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if not peaks.get("_fallback")
                          else "fallback", "fp32_simt_peak_nominal": FP32_PEAK_NOMINAL,
@@ -381,10 +422,77 @@ def cpu_baseline(args, inps, mus):
                       "FP64 CPU restatement (OpenMP), not MRCPP"}
 
 
+def run_exchange(args):
+    """Exchange pair batch: 16 orbitals (the Helmholtz batch's orbital model), the 136 pair products
+    phi_i phi_j (i <= j, adaptive multiply as at ExchangePotential.cpp:253,312), each followed by a
+    Poisson apply (ExchangePotential.cpp:137).  One step = all 136 products and applies; FP64 and mixed
+    applies (the products are FP64 in both); error per pair of the mixed potential against FP64."""
+    import torch
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    from mrchem_b200 import mrcpp as G
+    from mrchem_b200 import workloads as W
+
+    stream = torch.cuda.Stream()
+    ctx = G.Context(local, stream=stream.cuda_stream)
+    ctx.reserve(args.reserve_gib << 30)
+    m = G.MultiResolutionAnalysis(W.WORLD["min_scale"], W.WORLD["corner"], W.WORLD["boxes"], args.order, 15, ctx=ctx)
+    norb = 16
+    phis = []
+    for f in W.orbitals(norb, seed=2 + 1000 * rank):
+        t = G.FunctionTree(m)
+        G.project(args.prec, t, f)
+        phis.append(t)
+    pairs = [(i, j) for i in range(norb) for j in range(i, norb)]
+    P = G.PoissonOperator(m, args.prec)
+
+    def step(flags):
+        prods = [G.FunctionTree(m) for _ in pairs]
+        G.multiply_batched(args.prec, prods, None, [phis[i] for i, _ in pairs], [phis[j] for _, j in pairs])
+        outs = [G.FunctionTree(m) for _ in pairs]
+        half = (len(pairs) + 1) // 2
+        for a in range(0, len(pairs), half):
+            G.apply_batched(args.prec, outs[a:a + half], [P] * len(outs[a:a + half]), prods[a:a + half], flags)
+        return prods, outs
+
+    res = {}
+    for name, flags in (("fp64", G.APPLY_FP64), ("mixed", G.APPLY_FP32)):
+        for _ in range(args.warmup):
+            step(flags)
+        torch.cuda.synchronize()
+        ctx.profile(True)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            prods, outs = step(flags)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        launches, apply_launches, apply_ms = ctx.profile_read()
+        ctx.profile(False)
+        res[name] = {"ms_per_step": ms, "pairs_per_s": len(pairs) / (ms / 1e3),
+                     "apply_kernel_ms_per_step": apply_ms / args.steps,
+                     "product_nodes": sum(p.nnodes() for p in prods), "potential_nodes": sum(o.nnodes() for o in outs)}
+        res[name + "_outs"] = outs
+    errs = [G.distance(a, b) / np.sqrt(b.square_norm()) for a, b in zip(res["mixed_outs"], res["fp64_outs"])]
+    same = all(a.nnodes() == b.nnodes() for a, b in zip(res["mixed_outs"], res["fp64_outs"]))
+    if rank == 0:
+        line = {"metric": "exchange pair batch: 136 pair products + Poisson applies", "workload": "exchange_16orb_136pairs_k10_prec1e-6",
+                "value": res["mixed"]["pairs_per_s"], "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "order": args.order, "prec": args.prec, "data": "synthetic",
+                "fp64": res["fp64"], "mixed": res["mixed"],
+                "rel_error_per_pair": {"max": max(errs), "median": float(np.median(errs)), "min": min(errs)},
+                "same_node_count_as_fp64": bool(same)}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "exchange":
+        run_exchange(args)
     else:
         run_gpu(args)
 

@@ -207,6 +207,26 @@ inline double dot(FunctionTree<3>& a, FunctionTree<3>& b) {
     return v;
 }
 
+// out = c a b (reference call sites src/qmfunctions/qmfunction_utils.cpp:214,217); maxIter < 0 refines
+// until converged, 0 keeps the grid of `out`
+inline void multiply(double prec, FunctionTree<3>& out, double c, FunctionTree<3>& a, FunctionTree<3>& b,
+                     int maxIter = -1) {
+    detail::check(mw_multiply(prec, out.handle(), c, a.handle(), b.handle(), maxIter), "multiply");
+}
+
+// out = a^2 (reference src/qmfunctions/density_utils.cpp:74)
+inline void square(double prec, FunctionTree<3>& out, FunctionTree<3>& a, int maxIter = -1) {
+    detail::check(mw_square(prec, out.handle(), a.handle(), maxIter), "square");
+}
+
+// grid helpers (reference qmfunction_utils.cpp:211-212, density_utils.cpp:73)
+inline void build_grid(FunctionTree<3>& out, FunctionTree<3>& inp) {
+    detail::check(mw_tree_build_grid(out.handle(), inp.handle()), "build_grid");
+}
+inline void copy_grid(FunctionTree<3>& out, FunctionTree<3>& inp) {
+    detail::check(mw_tree_copy_grid(out.handle(), inp.handle()), "copy_grid");
+}
+
 }  // namespace mrcpp
 
 #endif  // MRCPP_B200_H

@@ -43,6 +43,11 @@ int mw_version(int* major, int* minor);
 int mw_ctx_create(int device, void* stream, mw_ctx* out);
 int mw_ctx_destroy(mw_ctx ctx);
 int mw_ctx_synchronize(mw_ctx ctx);
+/* Grow the context's device memory pool to at least `bytes` once, up front.  Every allocation of the
+ * library is stream-ordered from the device's default pool, which keeps freed memory (release
+ * threshold: unlimited); a pool that must still grow maps new memory inside the first calls that
+ * need it, which makes their time vary.  Reserving the working set once removes that. */
+int mw_ctx_reserve(mw_ctx ctx, unsigned long long bytes);
 /* Benchmark counters (no reference counterpart: the reference times with mrcpp::Timer around whole
  * calls, src/scf_solver/HelmholtzVector.cpp:68-82).  enable != 0 resets and starts them: number of
  * kernels this library launched, and number and CUDA-event time (ms) of contraction-kernel launches. */
@@ -88,6 +93,12 @@ int mw_project(double prec, mw_tree tree, int func_type, int nparams, const doub
 /* Inner product <a|b> of two compressed trees (reference: orbital::dot via mrcpp::dot,
  * tests/qmoperators/coulomb_operator.cpp:90). */
 int mw_dot(mw_tree a, mw_tree b, double* out);
+
+/* ||a - b|| (L2 norm of the difference of two compressed trees on one world, any grids; a node that
+ * one tree lacks counts with zero wavelets there).  Computed from the coefficient differences, so it
+ * resolves differences far below the cancellation limit of ||a||^2 + ||b||^2 - 2<a|b>.  Used to
+ * report the error of the mixed-precision apply against the FP64 one. */
+int mw_tree_distance(mw_tree a, mw_tree b, double* out);
 
 /* Allocation-free inner product <a|b>.  No counterpart in the reference: it serves callers that
  * cannot allocate device memory when they need the result -- a thread recording a CUDA graph

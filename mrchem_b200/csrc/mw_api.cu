@@ -118,7 +118,7 @@ void tree_make_roots(Tree& t) {
 }
 
 // split the nodes of the last level whose wavelet norm exceeds thr; returns the number of new nodes
-static int tree_refine_last_level(Tree& t, double thr) {
+int tree_refine_last_level(Tree& t, double thr) {
     Ctx* ctx = t.mra->ctx;
     cudaStream_t s = ctx->stream;
     const int b = t.level_begin[t.levels() - 1], e = t.level_begin[t.levels()];
@@ -151,15 +151,6 @@ void tree_compress_bottom_up(Tree& t) {
     for (int d = t.levels() - 2; d >= 0; --d) {
         const int b = t.level_begin[d], e = t.level_begin[d + 1];
         launch_transform_nodes(t, TM_COMPRESS, nullptr, e - b, nullptr, s, b);
-    }
-}
-
-// top-down sum-up of an NS-form output: children's scaling parts += reconstruction of the parent
-static void tree_sumup_top_down(Tree& t) {
-    cudaStream_t s = t.mra->ctx->stream;
-    for (int d = 0; d + 1 < t.levels(); ++d) {
-        const int b = t.level_begin[d], e = t.level_begin[d + 1];
-        launch_transform_nodes(t, TM_SUMUP, nullptr, e - b, nullptr, s, b);
     }
 }
 
@@ -559,11 +550,7 @@ static void apply_batched(double prec, int n, Tree** out, Op** op, Tree** inp, i
         add_children_many(grow, lists);
         total_trip += bp.triples;
     }
-    for (int i = 0; i < n; ++i) {
-        tree_sumup_top_down(*out[i]);
-        tree_compress_bottom_up(*out[i]);
-        launch_node_norms(*out[i], 0, out[i]->n, s);
-    }
+    trees_finish(std::vector<Tree*>(out, out + n), true, true, true, s);
     MWB_CUDA(cudaStreamSynchronize(s));
     for (int i = 0; i < n; ++i) {
         out[i]->g0 = g0[i];
@@ -810,10 +797,8 @@ static void apply_learned(double prec, int n, Tree** out, Op** op, Tree** inp, i
         }
         trees_rebuild(ts, kk, ky);
     }
+    trees_finish(std::vector<Tree*>(out, out + n), true, true, true, s);
     for (int i = 0; i < n; ++i) {
-        tree_sumup_top_down(*out[i]);
-        tree_compress_bottom_up(*out[i]);
-        launch_node_norms(*out[i], 0, out[i]->n, s);
         out[i]->g0 = g0[i];
         out[i]->prec = prec;
         out[i]->stats[0] = n == 1 ? trip : -1;
@@ -915,6 +900,19 @@ int mw_ctx_create(int device, void* stream, mw_ctx* out) {
         uint64_t thr = ~0ull;
         MWB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
         *out = c;
+    })
+}
+
+int mw_ctx_reserve(mw_ctx ctx, unsigned long long bytes) {
+    MW_TRY({
+        MW_ARG(ctx, "null context");
+        MWB_CUDA(cudaSetDevice(ctx->device));
+        if (bytes > 0) {
+            void* p = nullptr;
+            MWB_CUDA(cudaMallocAsync(&p, (size_t)bytes, ctx->stream));
+            MWB_CUDA(cudaFreeAsync(p, ctx->stream));
+            MWB_CUDA(cudaStreamSynchronize(ctx->stream));
+        }
     })
 }
 
@@ -1208,6 +1206,15 @@ int mw_dot(mw_tree a, mw_tree b, double* out) {
         MW_ARG(a->mra == b->mra, "trees must share the world");
         MWB_CUDA(cudaSetDevice(a->mra->ctx->device));
         *out = launch_dot(*a, *b, a->mra->ctx->stream);
+    })
+}
+
+int mw_tree_distance(mw_tree a, mw_tree b, double* out) {
+    MW_TRY({
+        MW_ARG(a && b && out, "null pointer");
+        MW_ARG(a->mra == b->mra, "trees on different worlds");
+        MWB_CUDA(cudaSetDevice(a->mra->ctx->device));
+        *out = launch_distance(*a, *b, a->mra->ctx->stream);
     })
 }
 

@@ -128,19 +128,16 @@ struct WorldGeo {
 
 constexpr int kTransformThreads = 256;
 
+// one node of a transform (the whole block); leaves must have been filtered out by the caller in
+// the compress / sum-up modes
 template <int K>
-__global__ void __launch_bounds__(kTransformThreads) k_transform(int mode, const int* __restrict__ nodes, int begin,
-                                                                 TView t, const double* __restrict__ Mg, FuncDesc f,
-                                                                 WorldGeo wg) {
+__device__ __forceinline__ void transform_node(int mode, int node, const TView& t, const double* __restrict__ Mg,
+                                               const FuncDesc& f, const WorldGeo& wg) {
     using G = Geo<K>;
     extern __shared__ double sm[];
     double* A = sm;
     double* M = A + G::VOL;
     double* red = M + G::K2 * G::K2;
-    // node list, or (nodes == nullptr) the range begin + blockIdx.x, where leaves have nothing to do
-    // for the compress / sum-up modes (the whole block leaves together, before any barrier)
-    const int node = nodes ? nodes[blockIdx.x] : begin + blockIdx.x;
-    if (!nodes && mode != TM_PROJECT && t.child0[node] < 0) return;
     for (int i = threadIdx.x; i < G::K2 * G::K2; i += blockDim.x) M[i] = Mg[i];
     double fac = 1.0;
     if (mode == TM_PROJECT) {
@@ -205,6 +202,55 @@ __global__ void __launch_bounds__(kTransformThreads) k_transform(int mode, const
             t.norm2[node] = n2;
             t.wnorm2[node] = w2;
         }
+    }
+}
+
+template <int K>
+__global__ void __launch_bounds__(kTransformThreads) k_transform(int mode, const int* __restrict__ nodes, int begin,
+                                                                 TView t, const double* __restrict__ Mg, FuncDesc f,
+                                                                 WorldGeo wg) {
+    // node list, or (nodes == nullptr) the range begin + blockIdx.x, where leaves have nothing to do
+    // for the compress / sum-up modes (the whole block leaves together, before any barrier)
+    const int node = nodes ? nodes[blockIdx.x] : begin + blockIdx.x;
+    if (!nodes && mode != TM_PROJECT && t.child0[node] < 0) return;
+    transform_node<K>(mode, node, t, Mg, f, wg);
+}
+
+// compress / sum-up of the internal nodes of one level of several trees: items (tree, node)
+template <int K>
+__global__ void __launch_bounds__(kTransformThreads) k_transform_multi(int mode, const int2* __restrict__ items,
+                                                                       const TView* __restrict__ views,
+                                                                       const double* __restrict__ Mg, WorldGeo wg) {
+    const int2 it = items[blockIdx.x];
+    const TView t = views[it.x];
+    if (t.child0[it.y] < 0) return;
+    transform_node<K>(mode, it.y, t, Mg, FuncDesc{0, 0, nullptr}, wg);
+}
+
+// one warp per (tree, node) item: squared norm of the block and of its wavelet part
+template <int K>
+__global__ void k_node_norms_multi(const int2* __restrict__ items, int nitems, const TView* __restrict__ views) {
+    using G = Geo<K>;
+    const int q = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x & 31;
+    if (q >= nitems) return;
+    const int2 it = items[q];
+    const TView t = views[it.x];
+    const double* c = t.coef + (size_t)it.y * G::BS;
+    double n2 = 0.0, w2 = 0.0;
+    for (int e = lane; e < G::BS; e += 32) {
+        const double v = c[e];
+        const int a = e % G::K2, b = (e / G::K2) % G::K2, cc = e / (G::K2 * G::K2);
+        n2 += v * v;
+        if (!(a < K && b < K && cc < K)) w2 += v * v;
+    }
+    for (int o = 16; o; o >>= 1) {
+        n2 += __shfl_down_sync(0xffffffffu, n2, o);
+        w2 += __shfl_down_sync(0xffffffffu, w2, o);
+    }
+    if (lane == 0) {
+        t.norm2[it.y] = n2;
+        t.wnorm2[it.y] = w2;
     }
 }
 
@@ -323,6 +369,33 @@ __global__ void k_dot_nodes(TView a, int na, const double* __restrict__ bcoef, c
     for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if (lane == 0) part[node] = s;
 }
+// ||a - b||^2 contributions of a's nodes (one warp per node): root scaling parts and all wavelet
+// parts of a - b, where b's node is missing its block counts as zero; with `only_missing` the
+// nodes of a that b lacks alone (the second half of the sum, run with the roles swapped)
+template <int K>
+__global__ void k_diff_nodes(TView a, int na, const double* __restrict__ bcoef, const uint64_t* hk, const int* hv,
+                             uint32_t hcap, int only_missing, double* part) {
+    using G = Geo<K>;
+    const int node = (blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    const int lane = threadIdx.x & 31;
+    if (node >= na) return;
+    const uint64_t key = a.key[node];
+    const int j = hlookup(hk, hv, hcap, key);
+    double s = 0.0;
+    if (!(only_missing && j >= 0)) {
+        const bool root = key_depth(key) == 0;
+        const double* x = a.coef + (size_t)node * G::BS;
+        const double* y = j >= 0 ? bcoef + (size_t)j * G::BS : nullptr;
+        for (int e = lane; e < G::BS; e += 32) {
+            const int aa = e % G::K2, bb = (e / G::K2) % G::K2, cc = e / (G::K2 * G::K2);
+            if (!root && aa < K && bb < K && cc < K) continue;
+            const double d = x[e] - (y ? y[e] : 0.0);
+            s += d * d;
+        }
+    }
+    for (int o = 16; o; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) part[node] = s;
+}
 __global__ void k_sum_array(const double* __restrict__ v, int n, double* out) {
     __shared__ double red[64];
     double s = 0.0, d = 0.0;
@@ -378,6 +451,64 @@ void launch_transform_nodes(Tree& t, int mode, const int* d_nodes, int nnodes, c
 #undef L_TR
     MWB_CUDA(cudaGetLastError());
     count(m.ctx);
+}
+
+// Finishing transforms of a batch of trees on one world, one launch per level for all trees:
+// sum-up top-down (sumup), then compress bottom-up (compress), then the norms of every node (norms).
+void trees_finish(const std::vector<Tree*>& ts, bool sumup, bool compress, bool norms, cudaStream_t s) {
+    if (ts.empty()) return;
+    const Mra& m = *ts[0]->mra;
+    Ctx* ctx = m.ctx;
+    int maxl = 0;
+    for (Tree* t : ts) maxl = std::max(maxl, t->levels());
+    // items grouped by level: [lvl_off[d], lvl_off[d+1]) are the nodes of depth d of every tree
+    std::vector<int2> items;
+    std::vector<int> lvl_off(maxl + 1, 0);
+    for (int d = 0; d < maxl; ++d) {
+        lvl_off[d] = (int)items.size();
+        for (size_t i = 0; i < ts.size(); ++i)
+            if (d < ts[i]->levels())
+                for (int q = ts[i]->level_begin[d]; q < ts[i]->level_begin[d + 1]; ++q) items.push_back(int2{(int)i, q});
+    }
+    lvl_off[maxl] = (int)items.size();
+    if (items.empty()) return;
+    std::vector<TView> views;
+    for (Tree* t : ts) views.push_back(view(*t));
+    int2* d_items = (int2*)dalloc(ctx, sizeof(int2) * items.size());
+    TView* d_views = (TView*)dalloc(ctx, sizeof(TView) * views.size());
+    MWB_CUDA(cudaMemcpyAsync(d_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, s));
+    MWB_CUDA(cudaMemcpyAsync(d_views, views.data(), sizeof(TView) * views.size(), cudaMemcpyHostToDevice, s));
+    WorldGeo wg = world_geo(m);
+    auto level = [&](int mode, int d) {
+        const int n = lvl_off[d + 1] - lvl_off[d];
+        if (n <= 0) return;
+        const double* M = mode == TM_COMPRESS ? m.d_F : m.d_FT;
+#define L_TRM(KK)                                                                                          \
+    {                                                                                                      \
+        size_t smem = sizeof(double) * (Geo<KK>::VOL + 4 * KK * KK + 64);                                 \
+        MWB_CUDA(cudaFuncSetAttribute(k_transform_multi<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
+                                      (int)smem));                                                         \
+        k_transform_multi<KK><<<n, kTransformThreads, smem, s>>>(mode, d_items + lvl_off[d], d_views, M, wg); \
+    }
+        MWB_DISPATCH_K(m.k, L_TRM)
+#undef L_TRM
+        MWB_CUDA(cudaGetLastError());
+        count(ctx);
+    };
+    if (sumup)
+        for (int d = 0; d + 1 < maxl; ++d) level(TM_SUMUP, d);
+    if (compress)
+        for (int d = maxl - 2; d >= 0; --d) level(TM_COMPRESS, d);
+    if (norms) {
+        const int n = (int)items.size();
+#define L_NNM(KK) k_node_norms_multi<KK><<<(n * 32 + 255) / 256, 256, 0, s>>>(d_items, n, d_views);
+        MWB_DISPATCH_K(m.k, L_NNM)
+#undef L_NNM
+        MWB_CUDA(cudaGetLastError());
+        count(ctx);
+    }
+    dfree(ctx, d_items);
+    dfree(ctx, d_views);
 }
 
 void launch_node_norms(Tree& t, int begin, int end, cudaStream_t s) {
@@ -530,6 +661,37 @@ double launch_dot(Tree& a, Tree& b, cudaStream_t s) {
     dfree(ctx, part);
     dfree(ctx, d);
     return h;
+}
+
+// ||a - b|| of two compressed trees on one world (any grids)
+double launch_distance(Tree& a, Tree& b, cudaStream_t s) {
+    Ctx* ctx = a.mra->ctx;
+    const int nmax = std::max(1, std::max(a.n, b.n));
+    double* part = (double*)dalloc(ctx, sizeof(double) * nmax);
+    double* d = (double*)dalloc(ctx, sizeof(double) * 2);
+    MWB_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * 2, s));
+    TView av = view(a), bv = view(b);
+    if (a.n > 0) {
+#define L_DIFF(KK) k_diff_nodes<KK><<<(a.n * 32 + 255) / 256, 256, 0, s>>>(av, a.n, b.coef, b.hkey, b.hval, b.hcap, 0, part);
+        MWB_DISPATCH_K(a.mra->k, L_DIFF)
+#undef L_DIFF
+        k_sum_array<<<1, 1024, 0, s>>>(part, a.n, d);
+        count(ctx, 2);
+    }
+    if (b.n > 0) {
+#define L_DIFF(KK) k_diff_nodes<KK><<<(b.n * 32 + 255) / 256, 256, 0, s>>>(bv, b.n, a.coef, a.hkey, a.hval, a.hcap, 1, part);
+        MWB_DISPATCH_K(a.mra->k, L_DIFF)
+#undef L_DIFF
+        k_sum_array<<<1, 1024, 0, s>>>(part, b.n, d + 1);
+        count(ctx, 2);
+    }
+    MWB_CUDA(cudaGetLastError());
+    double h[2] = {0.0, 0.0};
+    MWB_CUDA(cudaMemcpyAsync(h, d, sizeof(double) * 2, cudaMemcpyDeviceToHost, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
+    dfree(ctx, part);
+    dfree(ctx, d);
+    return std::sqrt(h[0] + h[1]);
 }
 
 // host copies of the key helpers for the driver

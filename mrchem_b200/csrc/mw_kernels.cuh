@@ -34,6 +34,8 @@ struct InView {
 void launch_transform_nodes(Tree& t, int mode, const int* d_nodes, int nnodes, const FuncDesc* f, cudaStream_t s,
                             int begin = 0);
 void launch_node_norms(Tree& t, int begin, int end, cudaStream_t s);
+// sum-up top-down, compress bottom-up and/or node norms of several trees, one launch per level
+void trees_finish(const std::vector<Tree*>& ts, bool sumup, bool compress, bool norms, cudaStream_t s);
 void launch_hash_reset(Tree& t, cudaStream_t s);
 void launch_hash_insert(Tree& t, int begin, int end, cudaStream_t s);
 // flags[i - begin] = sqrt(wnorm2[i]) > thr(depth) for i in [begin, end); returns number of splits
@@ -52,11 +54,14 @@ void reduce_norms_many(const std::vector<Tree*>& ts, std::vector<double>& leaf2,
                        cudaStream_t s);
 void launch_rescale(Tree& t, double c, cudaStream_t s);
 double launch_dot(Tree& a, Tree& b, cudaStream_t s);
+double launch_distance(Tree& a, Tree& b, cudaStream_t s);
 
 // tree bookkeeping shared by the drivers (mw_api.cu)
 void tree_reserve(Tree& t, int need);
 void tree_make_roots(Tree& t);
 void tree_compress_bottom_up(Tree& t);
+// split the nodes of the last level whose wavelet norm exceeds thr; returns the number of new nodes
+int tree_refine_last_level(Tree& t, double thr);
 
 // one refinement pass of a batched apply (mw_apply.cu)
 struct BatchTree {

@@ -329,6 +329,22 @@ void multiply_batched(double prec, int n, Tree** out, const double* c, Tree** a,
         bool any = false;
         for (int i = 0; i < n; ++i) {
             Tree& o = *out[i];
+            if (work[i].empty()) continue;
+            // work = the whole last level (always so when the product grows from the roots): split on
+            // the device, children appended as the next level
+            const int L = o.levels();
+            const int lb = o.level_begin[L - 1], le = o.level_begin[L];
+            if ((int)work[i].size() == le - lb && work[i].front() == lb && work[i].back() == le - 1) {
+                const int added = tree_refine_last_level(o, mul_split_threshold(prec, std::sqrt(leaf2[i]), L - 1));
+                work[i].clear();
+                if (added > 0) {
+                    any = true;
+                    for (int q = le; q < le + added; ++q) work[i].push_back(q);
+                    keys[i].clear();  // host keys are refreshed when the general path needs them
+                }
+                continue;
+            }
+            if (keys[i].size() != (size_t)o.n) keys[i] = host_keys(o, s);
             std::vector<double> w2(o.n);
             MWB_CUDA(cudaMemcpyAsync(w2.data(), o.wnorm2, sizeof(double) * o.n, cudaMemcpyDeviceToHost, s));
             MWB_CUDA(cudaStreamSynchronize(s));
@@ -352,10 +368,7 @@ void multiply_batched(double prec, int n, Tree** out, const double* c, Tree** a,
         if (!any) break;
     }
     dfree(ctx, d_trees);
-    for (int i = 0; i < n; ++i) {
-        tree_compress_bottom_up(*out[i]);
-        launch_node_norms(*out[i], 0, out[i]->n, s);
-    }
+    trees_finish(std::vector<Tree*>(out, out + n), false, true, true, s);
     MWB_CUDA(cudaStreamSynchronize(s));
 }
 

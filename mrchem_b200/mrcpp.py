@@ -46,6 +46,7 @@ SYMBOLS = [
     ("mw_ctx_create", ctypes.c_int, [ctypes.c_int, _vp, _vpp]),
     ("mw_ctx_destroy", ctypes.c_int, [_vp]),
     ("mw_ctx_synchronize", ctypes.c_int, [_vp]),
+    ("mw_ctx_reserve", ctypes.c_int, [_vp, ctypes.c_ulonglong]),
     ("mw_ctx_profile", ctypes.c_int, [_vp, ctypes.c_int]),
     ("mw_ctx_profile_read", ctypes.c_int, [_vp, _lp, _lp, _dp]),
     ("mw_mra_create", ctypes.c_int, [_vp, ctypes.c_int, _ip, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vpp]),
@@ -63,6 +64,7 @@ SYMBOLS = [
     ("mw_project", ctypes.c_int, [ctypes.c_double, _vp, ctypes.c_int, ctypes.c_int, _dp]),
     ("mw_dot", ctypes.c_int, [_vp, _vp, _dp]),
     ("mw_nalloc_dot", ctypes.c_int, [_vp, _vp, _dp]),
+    ("mw_tree_distance", ctypes.c_int, [_vp, _vp, _dp]),
     ("mw_op_create_poisson", ctypes.c_int, [_vp, ctypes.c_double, _vpp]),
     ("mw_op_create_helmholtz", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _vpp]),
     ("mw_op_destroy", ctypes.c_int, [_vp]),
@@ -145,6 +147,10 @@ class Context:
 
     def synchronize(self):
         _check(_lib.mw_ctx_synchronize(self._h))
+
+    def reserve(self, nbytes):
+        """Grow the device memory pool to at least nbytes up front (see mw_ctx_reserve)."""
+        _check(_lib.mw_ctx_reserve(self._h, int(nbytes)))
 
     def profile(self, enable=True):
         """Reset and (de)activate the kernel counters."""
@@ -279,6 +285,13 @@ def project(prec, tree: FunctionTree, func):
 def dot(a: FunctionTree, b: FunctionTree):
     v = ctypes.c_double()
     _check(_lib.mw_dot(a._h, b._h, ctypes.byref(v)))
+    return v.value
+
+
+def distance(a: FunctionTree, b: FunctionTree):
+    """||a - b|| from the coefficient differences (no cancellation)"""
+    v = ctypes.c_double()
+    _check(_lib.mw_tree_distance(a._h, b._h, ctypes.byref(v)))
     return v.value
 
 

@@ -1,6 +1,8 @@
 // Drop-in check of the C++ front-end: the calls below have the shapes of the reference's call sites
 // (src/mrenv.cpp:52-66, src/scf_solver/HelmholtzVector.cpp:169-180, src/SCFDriver.cpp:279,
-// src/qmoperators/two_electron/CoulombPotential.cpp:80-85) and run on the GPU through libmwb200.so.
+// src/qmoperators/two_electron/CoulombPotential.cpp:80-85, src/qmfunctions/qmfunction_utils.cpp:209-217,
+// src/qmoperators/two_electron/ExchangePotential.cpp:131-137, src/qmfunctions/density_utils.cpp:73-74)
+// and run on the GPU through libmwb200.so.
 #include <cmath>
 #include <cstdio>
 
@@ -37,5 +39,22 @@ int main() {
     mrcpp::FunctionTree<3> V(MRA);
     mrcpp::apply(abs_prec, V, P, phi);
     std::printf("poisson nodes %d norm2 %.15e dot %.15e\n", V.getNNodes(), V.getSquareNorm(), mrcpp::dot(V, phi));
+
+    // ExchangePotential: phi_ip = phi_i^* phi_p on the union grid (multiply_real with prec < 0), then
+    // V_ip = P[phi_ip]
+    mrcpp::FunctionTree<3> phi_ip(MRA);
+    mrcpp::build_grid(phi_ip, phi);
+    mrcpp::build_grid(phi_ip, out);
+    mrcpp::multiply(-1.0, phi_ip, 1.0, phi, out, 0);
+    mrcpp::FunctionTree<3> V_ip(MRA);
+    mrcpp::apply(prec, V_ip, P, phi_ip);
+    std::printf("exchange nodes %d norm2 %.15e dot %.15e\n", V_ip.getNNodes(), V_ip.getSquareNorm(),
+                mrcpp::dot(V_ip, phi));
+
+    // density_utils::compute: copy_grid, then square
+    mrcpp::FunctionTree<3> rho(MRA);
+    mrcpp::copy_grid(rho, phi);
+    mrcpp::square(prec, rho, phi);
+    std::printf("density nodes %d norm2 %.15e dot %.15e\n", rho.getNNodes(), rho.getSquareNorm(), mrcpp::dot(rho, phi));
     return 0;
 }

@@ -34,7 +34,17 @@ def test_cpp_frontend_matches_python(gpu_mod, tmp_path):
     out_h.rescale(-1.0 / (2 * np.pi))
     V = G.FunctionTree(m)
     G.apply(prec / np.sqrt(phi.square_norm()), V, G.PoissonOperator(m, prec), phi)
-    for key, t in (("helmholtz", out_h), ("poisson", V)):
+    P = G.PoissonOperator(m, prec)
+    phi_ip = G.FunctionTree(m)
+    G.build_grid(phi_ip, phi)
+    G.build_grid(phi_ip, out_h)
+    G.multiply(-1.0, phi_ip, 1.0, phi, out_h, 0)
+    V_ip = G.FunctionTree(m)
+    G.apply(prec, V_ip, P, phi_ip)
+    rho = G.FunctionTree(m)
+    G.copy_grid(rho, phi)
+    G.square(prec, rho, phi)
+    for key, t in (("helmholtz", out_h), ("poisson", V), ("exchange", V_ip), ("density", rho)):
         n, n2, d = vals[key]
         assert n == t.nnodes()
         assert abs(n2 - t.square_norm()) <= 1e-12 * t.square_norm()

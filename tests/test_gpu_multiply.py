@@ -155,3 +155,22 @@ def test_multiply_errors(gpu_mod):
     G.project(1e-3, b, gauss(G, A2, C2))
     with pytest.raises(G.MWError):
         G.multiply(1e-3, G.FunctionTree(mg), 1.0, a, b)  # different worlds
+
+
+def test_tree_distance(gpu_mod):
+    """||a - b|| from coefficient differences: zero for a tree and itself, equal to the norm identity
+    for well-separated trees, symmetric, and exact for a rescaled copy on the same grid"""
+    G = gpu_mod
+    mg = G.MultiResolutionAnalysis(*WORLD, 5, 14)
+    a, b = G.FunctionTree(mg), G.FunctionTree(mg)
+    G.project(1e-4, a, gauss(G, A1, C1))
+    G.project(1e-4, b, gauss(G, A2, C2))
+    assert G.distance(a, a) == 0.0
+    d = G.distance(a, b)
+    ident = np.sqrt(a.square_norm() + b.square_norm() - 2 * G.dot(a, b))
+    assert abs(d - ident) < 1e-10 * ident
+    assert abs(G.distance(b, a) - d) < 1e-14 * d
+    c = G.FunctionTree(mg)
+    G.project(1e-4, c, gauss(G, A1, C1))
+    c.rescale(1.0 + 1e-9)
+    assert abs(G.distance(a, c) - 1e-9 * np.sqrt(a.square_norm())) < 1e-3 * 1e-9 * np.sqrt(a.square_norm())
