@@ -259,7 +259,7 @@ def run_gpu(args):
         step_ms.append([evs[q].elapsed_time(evs[q + 1]) for q in range(args.steps)])
         barrier()
         ms_ = ev0.elapsed_time(ev1)
-        prof = ctx.profile_read()
+        prof = ctx.profile_read() + (ctx.profile_ctas(),)
         ctx.profile(False)
         if world > 1:
             tt = torch.tensor([ms_], device=f"cuda:{local}", dtype=torch.float64)
@@ -300,7 +300,7 @@ def run_gpu(args):
         return st["triples"]
 
     ms, triples, prof32, clocks = timed(run_learned)
-    launches, apply_launches, apply_ms = prof32
+    launches, apply_launches, apply_ms, apply_ctas = prof32
     # error of the mixed + learned result against the FP64 one: ||g - g64|| / ||g64|| per orbital
     # (from the coefficient differences, mw_tree_distance: no cancellation)
     rel_err = 0.0
@@ -344,11 +344,13 @@ def run_gpu(args):
     flops = triples * flops_per_triple(k)
     achieved = flops / (apply_ms / 1e3) / 1e12 if apply_ms > 0 else None
     peak = float(peaks.get("bf16_tflops", 1590.0))
+    # DRAM traffic per contraction launch: bytes per CTA measured by ncu on an 8-orbital batch
+    # (profiles/k_gapply_fp32_k10_traffic.json) times this step's CTAs per launch
     traffic = None
-    prof_file = os.path.join(ROOT, "profiles", "k_apply_fp64_traffic.json")
-    if os.path.exists(prof_file):
+    prof_file = os.path.join(ROOT, "profiles", "k_gapply_fp32_k10_traffic.json")
+    if os.path.exists(prof_file) and k == 10 and apply_launches > 0:
         try:
-            traffic = json.load(open(prof_file)).get("dram_bytes_per_launch")
+            traffic = json.load(open(prof_file))["dram_bytes_per_cta"] * apply_ctas / apply_launches
         except Exception:
             traffic = None
 
@@ -389,7 +391,9 @@ def run_gpu(args):
                          else "fallback", "fp32_simt_peak_nominal": FP32_PEAK_NOMINAL,
                          "frac_fp32_simt_nominal": (achieved / FP32_PEAK_NOMINAL) if achieved else None,
                          "flops_per_triple": flops_per_triple(k), "triples_per_step": triples // max(1, args.steps),
-                         "kernel_ms_per_step": apply_ms / args.steps, "kernel_launches": apply_launches},
+                         "kernel_ms_per_step": apply_ms / args.steps, "kernel_launches": apply_launches,
+                         "traffic_unit": "DRAM bytes per launch (ncu bytes per CTA x CTAs per launch)",
+                         "block_write_bytes_per_launch": apply_ctas * (2 * k) ** 3 * 8 / max(1, apply_launches)},
             "cpu_baseline": cpu,
             "gpu_launches": int(launches),
             "clocks": clocks,

@@ -53,6 +53,9 @@ int mw_ctx_reserve(mw_ctx ctx, unsigned long long bytes);
  * kernels this library launched, and number and CUDA-event time (ms) of contraction-kernel launches. */
 int mw_ctx_profile(mw_ctx ctx, int enable);
 int mw_ctx_profile_read(mw_ctx ctx, long long* launches, long long* apply_launches, double* apply_ms);
+/* CTAs (chunks of <= 48 triples of one output node) of the contraction launches counted since
+ * mw_ctx_profile(ctx, 1): the unit the contraction's DRAM traffic scales with */
+int mw_ctx_profile_ctas(mw_ctx ctx, long long* ctas);
 
 /* World and basis.  Replaces BoundingBox<3>(min_scale, corner, boxes) +
  * InterpolatingBasis(order) / LegendreBasis(order) + MultiResolutionAnalysis<3>(world, basis,

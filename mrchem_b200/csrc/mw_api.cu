@@ -927,7 +927,15 @@ int mw_ctx_profile(mw_ctx ctx, int enable) {
         ctx->prof = enable != 0;
         ctx->launches = 0;
         ctx->apply_launches = 0;
+        ctx->apply_ctas = 0;
         ctx->apply_ms = 0.0;
+    })
+}
+
+int mw_ctx_profile_ctas(mw_ctx ctx, long long* ctas) {
+    MW_TRY({
+        MW_ARG(ctx && ctas, "null pointer");
+        *ctas = ctx->apply_ctas;
     })
 }
 

@@ -1320,6 +1320,7 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     if (ctx->prof) MWB_CUDA(cudaEventRecord(ctx->ev1, s));
     count(ctx);
     ctx->apply_launches++;
+    ctx->apply_ctas += nchunks;
     if (nslots > 0) {
         int* d_mflags = (int*)dalloc(ctx, sizeof(int) * (ni + 1));
         int* d_mpos = (int*)dalloc(ctx, sizeof(int) * (ni + 1));

@@ -41,6 +41,7 @@ struct Ctx {
     bool prof = false;
     long long launches = 0;
     long long apply_launches = 0;
+    long long apply_ctas = 0;  // CTAs (chunks) of those launches
     double apply_ms = 0.0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };

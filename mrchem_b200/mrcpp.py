@@ -49,6 +49,7 @@ SYMBOLS = [
     ("mw_ctx_reserve", ctypes.c_int, [_vp, ctypes.c_ulonglong]),
     ("mw_ctx_profile", ctypes.c_int, [_vp, ctypes.c_int]),
     ("mw_ctx_profile_read", ctypes.c_int, [_vp, _lp, _lp, _dp]),
+    ("mw_ctx_profile_ctas", ctypes.c_int, [_vp, _lp]),
     ("mw_mra_create", ctypes.c_int, [_vp, ctypes.c_int, _ip, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vpp]),
     ("mw_mra_destroy", ctypes.c_int, [_vp]),
     ("mw_mra_filter", ctypes.c_int, [_vp, _dp]),
@@ -155,6 +156,12 @@ class Context:
     def profile(self, enable=True):
         """Reset and (de)activate the kernel counters."""
         _check(_lib.mw_ctx_profile(self._h, int(enable)))
+
+    def profile_ctas(self):
+        """contraction CTAs launched since profile()"""
+        v = ctypes.c_longlong()
+        _check(_lib.mw_ctx_profile_ctas(self._h, ctypes.byref(v)))
+        return v.value
 
     def profile_read(self):
         """(kernels launched, contraction launches, contraction CUDA-event ms) since profile()."""
