@@ -1112,25 +1112,27 @@ int mw_tree_upload(mw_tree t, int n, const int* depth, const long long* trans, c
             key[i] = host_make_key(depth[i], trans[3 * i], trans[3 * i + 1], trans[3 * i + 2]);
             maxd = std::max(maxd, depth[i]);
         }
+        // nodes already in (depth, Morton) order -- every tree this library exports -- are copied
+        // straight from the caller's buffers (pinned buffers: one DMA each); otherwise the blocks are
+        // copied as given and reordered on the device
+        const bool sorted = std::is_sorted(key.begin(), key.end());
         std::vector<int> ord(n);
         std::iota(ord.begin(), ord.end(), 0);
-        std::sort(ord.begin(), ord.end(), [&](int a, int b) { return key[a] < key[b]; });
+        if (!sorted) std::sort(ord.begin(), ord.end(), [&](int a, int b) { return key[a] < key[b]; });
         std::vector<int> pos(n);
         for (int i = 0; i < n; ++i) pos[ord[i]] = i;
         int nroot = (int)((long long)m.boxes[0] * m.boxes[1] * m.boxes[2]);
         std::vector<uint64_t> k2(n);
         std::vector<int> p2(n), c2(n);
-        std::vector<double> coef2((size_t)n * m.bsize());
         std::vector<int> lb(maxd + 2, 0);
         int roots = 0;
         for (int i = 0; i < n; ++i) {
             const int o = ord[i];
+            MW_ARG(parent[o] >= -1 && parent[o] < n && child0[o] >= -1 && child0[o] < n, "bad parent/child index");
             k2[i] = key[o];
             p2[i] = parent[o] < 0 ? -1 : pos[parent[o]];
             c2[i] = child0[o] < 0 ? -1 : pos[child0[o]];
             if (depth[o] == 0) ++roots;
-            MW_ARG(parent[o] < n && child0[o] < n, "bad parent/child index");
-            std::memcpy(&coef2[(size_t)i * m.bsize()], coef + (size_t)o * m.bsize(), sizeof(double) * m.bsize());
             lb[depth[o] + 1]++;
         }
         MW_ARG(roots == nroot, "tree must contain every root box");
@@ -1145,10 +1147,21 @@ int mw_tree_upload(mw_tree t, int n, const int* depth, const long long* trans, c
         for (int d = 1; d < (int)lb.size(); ++d) lb[d] += lb[d - 1];
         t->n = 0;
         tree_reserve(*t, n);
+        const size_t BS = m.bsize();
         MWB_CUDA(cudaMemcpyAsync(t->key, k2.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s));
         MWB_CUDA(cudaMemcpyAsync(t->parent, p2.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
         MWB_CUDA(cudaMemcpyAsync(t->child0, c2.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
-        MWB_CUDA(cudaMemcpyAsync(t->coef, coef2.data(), sizeof(double) * coef2.size(), cudaMemcpyHostToDevice, s));
+        if (sorted) {
+            MWB_CUDA(cudaMemcpyAsync(t->coef, coef, sizeof(double) * BS * n, cudaMemcpyHostToDevice, s));
+        } else {
+            double* stage = (double*)dalloc(m.ctx, sizeof(double) * BS * n);
+            int* d_ord = (int*)dalloc(m.ctx, sizeof(int) * n);
+            MWB_CUDA(cudaMemcpyAsync(stage, coef, sizeof(double) * BS * n, cudaMemcpyHostToDevice, s));
+            MWB_CUDA(cudaMemcpyAsync(d_ord, ord.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+            launch_gather_blocks(stage, d_ord, n, BS, t->coef, s);
+            dfree(m.ctx, stage);
+            dfree(m.ctx, d_ord);
+        }
         t->n = n;
         t->level_begin = lb;
         launch_hash_reset(*t, s);

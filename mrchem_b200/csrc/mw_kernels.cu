@@ -694,6 +694,21 @@ double launch_distance(Tree& a, Tree& b, cudaStream_t s) {
     return std::sqrt(h[0] + h[1]);
 }
 
+// dst[i] = src[perm[i]] for blocks of bs doubles
+__global__ void k_gather_blocks(const double* __restrict__ src, const int* __restrict__ perm, int n, size_t bs,
+                                double* __restrict__ dst) {
+    const int i = blockIdx.x;
+    if (i >= n) return;
+    const double* a = src + (size_t)perm[i] * bs;
+    double* b = dst + (size_t)i * bs;
+    for (size_t e = threadIdx.x; e < bs; e += blockDim.x) b[e] = a[e];
+}
+void launch_gather_blocks(const double* src, const int* perm, int n, size_t bs, double* dst, cudaStream_t s) {
+    if (n <= 0) return;
+    k_gather_blocks<<<n, 256, 0, s>>>(src, perm, n, bs, dst);
+    MWB_CUDA(cudaGetLastError());
+}
+
 // host copies of the key helpers for the driver
 uint64_t host_make_key(int depth, long long tx, long long ty, long long tz) { return make_key(depth, tx, ty, tz); }
 void host_key_trans(uint64_t k, long long t[3]) { key_trans(k, t); }

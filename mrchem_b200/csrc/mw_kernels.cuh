@@ -55,6 +55,8 @@ void reduce_norms_many(const std::vector<Tree*>& ts, std::vector<double>& leaf2,
 void launch_rescale(Tree& t, double c, cudaStream_t s);
 double launch_dot(Tree& a, Tree& b, cudaStream_t s);
 double launch_distance(Tree& a, Tree& b, cudaStream_t s);
+// dst[i] = src[perm[i]] for n blocks of bs doubles
+void launch_gather_blocks(const double* src, const int* perm, int n, size_t bs, double* dst, cudaStream_t s);
 
 // tree bookkeeping shared by the drivers (mw_api.cu)
 void tree_reserve(Tree& t, int need);

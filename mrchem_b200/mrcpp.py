@@ -248,6 +248,23 @@ class FunctionTree:
                                      _d(coef) if with_coefs else None))
         return dict(depth=depth, trans=trans, parent=parent, child0=child0, coef=coef)
 
+    def export_into(self, bufs):
+        """Download into caller-owned arrays (e.g. pinned host memory reused across calls): `bufs` has
+        int32 'depth', 'parent', 'child0' (>= n), int64 'trans' (>= n x 3) and float64 'coef'
+        (>= n x (2k)^3), all C-contiguous; returns n.  Nothing is allocated."""
+        n = self.nnodes()
+        k = self.mra.k
+        need = {"depth": (np.int32, n), "parent": (np.int32, n), "child0": (np.int32, n), "trans": (np.int64, 3 * n),
+                "coef": (np.float64, n * (2 * k) ** 3)}
+        for name, (dt, size) in need.items():
+            a = bufs[name]
+            if a.dtype != dt or not a.flags.c_contiguous or a.size < size:
+                raise MWError(f"export_into: buffer '{name}' must be C-contiguous {np.dtype(dt).name} of >= {size}")
+        _check(_lib.mw_tree_download(self._h, bufs["depth"].ctypes.data_as(_ip), bufs["trans"].ctypes.data_as(_lp),
+                                     bufs["parent"].ctypes.data_as(_ip), bufs["child0"].ctypes.data_as(_ip),
+                                     _d(bufs["coef"])))
+        return n
+
     def load(self, depth, trans, parent, child0, coef):
         depth = np.ascontiguousarray(depth, np.int32)
         trans = np.ascontiguousarray(trans, np.int64)

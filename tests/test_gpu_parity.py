@@ -233,6 +233,30 @@ def test_upload_download_roundtrip(gpu_mod, oracle_mod):
     assert abs(tg.square_norm() - to.square_norm()) < 1e-13 * to.square_norm()
 
 
+def test_ordered_upload_and_export_into(gpu_mod):
+    """A tree in the library's own node order is uploaded without reordering; export_into fills
+    caller-owned buffers with exactly what export() returns"""
+    G = gpu_mod
+    m = G.MultiResolutionAnalysis(*WORLD, 7, 14)
+    a = G.FunctionTree(m)
+    G.project(1e-5, a, two_gaussians(G))
+    ea = a.export()
+    b = G.FunctionTree(m)
+    b.load(ea["depth"], ea["trans"], ea["parent"], ea["child0"], ea["coef"])
+    eb = b.export()
+    for key in ("depth", "trans", "parent", "child0", "coef"):
+        assert np.array_equal(ea[key], eb[key])
+    n = a.nnodes()
+    bufs = {"depth": np.zeros(n + 5, np.int32), "parent": np.zeros(n + 5, np.int32), "child0": np.zeros(n + 5, np.int32),
+            "trans": np.zeros(3 * (n + 5), np.int64), "coef": np.zeros(ea["coef"].size + 10)}
+    assert b.export_into(bufs) == n
+    assert np.array_equal(bufs["coef"][:ea["coef"].size], ea["coef"].ravel())
+    assert np.array_equal(bufs["trans"][:3 * n], ea["trans"].ravel())
+    assert np.array_equal(bufs["child0"][:n], ea["child0"])
+    with pytest.raises(G.MWError):
+        b.export_into(dict(bufs, coef=np.zeros(5)))
+
+
 def test_rescale_and_dot(gpu_mod, oracle_mod):
     G, O = gpu_mod, oracle_mod
     mg, mo = pair(G, O, 5)
