@@ -48,9 +48,10 @@ def parse():
     p.add_argument("--tau", type=float, default=0.97, help="proposal threshold of the learned apply")
     p.add_argument("--reserve-gib", type=int, default=64,
                    help="device memory pool reserved up front (GiB): the working set of the step")
-    p.add_argument("--workload", default="helmholtz", choices=["helmholtz", "exchange"],
+    p.add_argument("--workload", default="helmholtz", choices=["helmholtz", "exchange", "density_sweep"],
                    help="helmholtz: 32-orbital Helmholtz batch (the headline); exchange: 16 orbitals -> 136 "
-                        "pair products, each followed by a Poisson apply")
+                        "pair products, each followed by a Poisson apply; density_sweep: Poisson potential of "
+                        "a 20-atom density at orders 7/9/11 x prec 1e-5/1e-6/1e-7, FP64 and mixed")
     return p.parse_args()
 
 
@@ -514,12 +515,84 @@ def run_exchange(args):
         print(json.dumps(line), flush=True)
 
 
+def run_density_sweep(args):
+    """Poisson potential of a 20-atom density (4 normalised Gaussians per atom, exponents
+    log-U[0.3, 1e3], atoms in a 12 Bohr box) at interpolating orders 7/9/11 and precisions
+    1e-5/1e-6/1e-7: FP64 and mixed (FP32 products, FP64 accumulation) applies on the GPU, each timed
+    over --steps steps after --warmup, with the relative error of the mixed potential against FP64
+    (coefficient differences) and the CPU restatement's time for one apply at order 7, prec 1e-5."""
+    import torch
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    from mrchem_b200 import mrcpp as G
+    from mrchem_b200 import workloads as W
+
+    stream = torch.cuda.Stream()
+    ctx = G.Context(local, stream=stream.cuda_stream)
+    ctx.reserve(args.reserve_gib << 30)
+    rho_f = W.density_20_atoms()
+    rows = []
+    for order in (7, 9, 11):
+        m = G.MultiResolutionAnalysis(W.WORLD["min_scale"], W.WORLD["corner"], W.WORLD["boxes"], order, 15, ctx=ctx)
+        for prec in (1e-5, 1e-6, 1e-7):
+            rho = G.FunctionTree(m)
+            G.project(prec, rho, rho_f)
+            P = G.PoissonOperator(m, prec)
+            row = {"order": order, "k": order + 1, "prec": prec, "input_nodes": rho.nnodes()}
+            outs = {}
+            for name, fl in (("fp64", G.APPLY_FP64), ("mixed", G.APPLY_FP32)):
+                out = G.FunctionTree(m)
+                for _ in range(args.warmup):
+                    G.apply(prec, out, P, rho, fl)
+                torch.cuda.synchronize()
+                ctx.profile(True)
+                ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                ev0.record(stream)
+                for _ in range(args.steps):
+                    st = G.apply(prec, out, P, rho, fl)
+                ev1.record(stream)
+                torch.cuda.synchronize()
+                kms = ctx.profile_read()[2] / args.steps
+                ctx.profile(False)
+                row[name] = {"ms": ev0.elapsed_time(ev1) / args.steps, "kernel_ms": kms, "triples": st[0],
+                             "out_nodes": out.nnodes(),
+                             "tflops": st[0] * flops_per_triple(order + 1) / (kms / 1e3) / 1e12 if kms > 0 else None}
+                outs[name] = out
+            row["rel_error_mixed"] = G.distance(outs["mixed"], outs["fp64"]) / np.sqrt(outs["fp64"].square_norm())
+            row["same_nodes"] = outs["mixed"].nnodes() == outs["fp64"].nnodes()
+            row["speedup_mixed"] = row["fp64"]["ms"] / row["mixed"]["ms"]
+            rows.append(row)
+            print(json.dumps(row), file=sys.stderr, flush=True)
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        mo = O.MultiResolutionAnalysis(W.WORLD["min_scale"], W.WORLD["corner"], W.WORLD["boxes"], 7, 15)
+        ro = O.FunctionTree(mo)
+        O.project(1e-5, ro, rho_f)
+        Po = O.PoissonOperator(mo, 1e-5)
+        vo = O.FunctionTree(mo)
+        O.apply(1e-5, vo, Po, ro)  # operator tables are built on first use
+        t0 = time.perf_counter()
+        O.apply(1e-5, vo, Po, ro)
+        cpu = {"order": 7, "prec": 1e-5, "s_per_apply": time.perf_counter() - t0,
+               "cores": O.lib().oracle_num_threads(), "kind": "port"}
+    if rank == 0:
+        print(json.dumps({"metric": "Poisson apply of a 20-atom density: orders x precisions, FP64 and mixed",
+                          "workload": "density_20_atoms_sweep", "data": "synthetic", "steps": args.steps,
+                          "warmup": args.warmup, "rows": rows, "cpu_baseline": cpu,
+                          "not_built": ["split-TF32", "BF16x3"]}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "exchange":
         run_exchange(args)
+    elif args.workload == "density_sweep":
+        run_density_sweep(args)
     else:
         run_gpu(args)
 
