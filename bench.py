@@ -127,17 +127,18 @@ class Clocks:
 
 
 def dist_env():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from mrchem_b200.replicas import dist_env as de
+
+    return de()
 
 
 def workload(rank, n, seed=2):
     """Config-2 orbitals and Helmholtz mu for a rank (weak scaling: every rank its own batch)."""
     from mrchem_b200 import workloads as W
 
-    return W.orbitals(n, seed=seed + 1000 * rank), W.helmholtz_mus(n, seed=seed + 1000 * rank)
+    from mrchem_b200.replicas import rank_seed
+
+    return W.orbitals(n, seed=rank_seed(seed, rank)), W.helmholtz_mus(n, seed=rank_seed(seed, rank))
 
 
 def flops_per_triple(k):
@@ -209,6 +210,7 @@ def run_gpu(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from mrchem_b200 import mrcpp as G
     from mrchem_b200 import workloads as W
+    from mrchem_b200.replicas import max_over_ranks
 
     stream = torch.cuda.Stream()
     ctx = G.Context(local, stream=stream.cuda_stream)
@@ -262,10 +264,7 @@ def run_gpu(args):
         ms_ = ev0.elapsed_time(ev1)
         prof = ctx.profile_read() + (ctx.profile_ctas(),)
         ctx.profile(False)
-        if world > 1:
-            tt = torch.tensor([ms_], device=f"cuda:{local}", dtype=torch.float64)
-            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-            ms_ = float(tt.item())
+        ms_ = max_over_ranks(ms_, device=f"cuda:{local}")
         return ms_, trip, prof, clk.summary()
 
     # learned tree proposal: trained (untimed) on plain applies of a disjoint seeded orbital set
@@ -356,10 +355,7 @@ def run_gpu(args):
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     gc.enable()
-    if world > 1:
-        tt = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = max_over_ranks(e2e_s, device=f"cuda:{local}")
     e2e_val = args.orbitals * n_e2e * world / e2e_s
 
     peaks = measured_peaks()
@@ -461,6 +457,7 @@ def run_exchange(args):
     torch.cuda.set_device(local)
     from mrchem_b200 import mrcpp as G
     from mrchem_b200 import workloads as W
+    from mrchem_b200.replicas import rank_seed
 
     stream = torch.cuda.Stream()
     ctx = G.Context(local, stream=stream.cuda_stream)
@@ -468,7 +465,7 @@ def run_exchange(args):
     m = G.MultiResolutionAnalysis(W.WORLD["min_scale"], W.WORLD["corner"], W.WORLD["boxes"], args.order, 15, ctx=ctx)
     norb = 16
     phis = []
-    for f in W.orbitals(norb, seed=2 + 1000 * rank):
+    for f in W.orbitals(norb, seed=rank_seed(2, rank)):
         t = G.FunctionTree(m)
         G.project(args.prec, t, f)
         phis.append(t)

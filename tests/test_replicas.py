@@ -1,0 +1,72 @@
+"""Host logic of the multi-GPU runs, on CPU: the balanced contiguous split of a batch over ranks, the
+per-rank batches of the weak-scaling runs, and the max-over-ranks step time, the last over a real
+2-process `gloo` group (the same collective the GPU runs make over NCCL)."""
+import json
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from mrchem_b200.replicas import max_over_ranks, rank_seed, shard_ranges
+
+
+def test_shard_ranges_cover_and_balance():
+    rng = np.random.default_rng(0)
+    for world in (1, 2, 3, 4, 8):
+        for n in (0, 1, 5, 32, 136):
+            w = rng.integers(500, 5000, n).tolist()
+            r = shard_ranges(w, world)
+            assert len(r) == world
+            assert r[0][0] == 0 and r[-1][1] == n
+            for (a, b), (c, d) in zip(r, r[1:]):
+                assert b == c and a <= b
+            if n >= 4 * world:
+                loads = [sum(w[a:b]) for a, b in r]
+                assert max(loads) <= sum(w) / world + max(w)
+    assert shard_ranges([1.0] * 8, 4) == [(0, 2), (2, 4), (4, 6), (6, 8)]
+    with pytest.raises(ValueError):
+        shard_ranges([1.0], 0)
+
+
+def test_rank_batches_differ():
+    from mrchem_b200 import workloads as W
+
+    a = W.orbitals(4, seed=rank_seed(2, 0))
+    b = W.orbitals(4, seed=rank_seed(2, 1))
+    assert not np.array_equal(a[0][1], b[0][1])
+    assert rank_seed(2, 0) == 2
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, outdir):
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        step_ms = [12.5, 40.25][rank]
+        got = max_over_ranks(step_ms)
+        ranges = shard_ranges([3, 1, 4, 1, 5, 9, 2, 6], world)
+        with open(os.path.join(outdir, f"rank{rank}.json"), "w") as f:
+            json.dump({"max": got, "range": ranges[rank]}, f)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_gloo_two_processes(tmp_path):
+    import torch.multiprocessing as mp
+
+    port = _free_port()
+    mp.start_processes(_rank_main, args=(2, port, str(tmp_path)), nprocs=2, join=True, start_method="spawn")
+    res = [json.load(open(tmp_path / f"rank{r}.json")) for r in range(2)]
+    assert res[0]["max"] == res[1]["max"] == 40.25
+    assert res[0]["range"][1] == res[1]["range"][0] and res[0]["range"][0] == 0 and res[1]["range"][1] == 8
+    assert max_over_ranks(7.0) == 7.0  # no process group: the value itself
