@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <memory>
+#include <tuple>
 #include <vector>
 
 #include "mwb200.h"
@@ -217,6 +218,24 @@ inline void multiply(double prec, FunctionTree<3>& out, double c, FunctionTree<3
 // out = a^2 (reference src/qmfunctions/density_utils.cpp:74)
 inline void square(double prec, FunctionTree<3>& out, FunctionTree<3>& a, int maxIter = -1) {
     detail::check(mw_square(prec, out.handle(), a.handle(), maxIter), "square");
+}
+
+// out = sum_i c_i f_i over (c_i, f_i) pairs (reference qmfunction_utils.cpp:170-177, KAIN.cpp:180)
+template <int D> using FunctionTreeVector = std::vector<std::tuple<double, FunctionTree<D>*>>;
+inline void add(double prec, FunctionTree<3>& out, FunctionTreeVector<3>& vec, int maxIter = -1) {
+    std::vector<double> c;
+    std::vector<mw_tree> f;
+    for (auto& t : vec) {
+        c.push_back(std::get<0>(t));
+        f.push_back(std::get<1>(t)->handle());
+    }
+    detail::check(mw_add(prec, out.handle(), (int)f.size(), c.data(), f.data(), maxIter), "add");
+}
+// out = a A + b B
+inline void add(double prec, FunctionTree<3>& out, double a, FunctionTree<3>& A, double b, FunctionTree<3>& B,
+                int maxIter = -1) {
+    FunctionTreeVector<3> vec{{a, &A}, {b, &B}};
+    add(prec, out, vec, maxIter);
 }
 
 // grid helpers (reference qmfunction_utils.cpp:211-212, density_utils.cpp:73)

@@ -154,6 +154,13 @@ int mw_multiply(double prec, mw_tree out, double c, mw_tree a, mw_tree b, int ma
 int mw_multiply_batched(int n, double prec, mw_tree* out, const double* c, mw_tree* a, mw_tree* b, int max_iter);
 /* out = a^2: mrcpp::square(prec, out, a), reference src/qmfunctions/density_utils.cpp:74 */
 int mw_square(double prec, mw_tree out, mw_tree a, int max_iter);
+/* Linear combination out = sum_i c[i] f[i] of n <= 256 trees on one world.  Replaces
+ * mrcpp::add(prec, out, vec[, maxIter]) with vec = {(c_i, f_i)}: reference
+ * src/qmfunctions/qmfunction_utils.cpp:170-177 (qmfunction::linear_combination), density_utils.cpp:87,
+ * src/mrdft/XCFunctional.cpp:713, src/scf_solver/KAIN.cpp:180,192.  Grid and refinement as
+ * mw_multiply: the union-grid form is mw_tree_build_grid for every f_i, then prec < 0 (or
+ * max_iter = 0).  `out` is left compressed with valid norms. */
+int mw_add(double prec, mw_tree out, int n, const double* c, mw_tree* f, int max_iter);
 /* Grids.  mw_tree_build_grid extends the grid of `out` by that of `inp` (new nodes have zero blocks;
  * mrcpp::build_grid, reference qmfunction_utils.cpp:211-212); mw_tree_copy_grid = clear + build_grid
  * (mrcpp::copy_grid, density_utils.cpp:73); mw_tree_clear empties a tree. */

@@ -201,6 +201,65 @@ __global__ void __launch_bounds__(kMulThreads) k_mul(const MulItem* __restrict__
     }
 }
 
+// linear combination: one input function of a sum
+struct AddIn {
+    const uint64_t* hk;
+    const int* hv;
+    uint32_t hcap;
+    const double* coef;
+    double c;
+};
+struct AddOut {
+    const uint64_t* key;
+    double* coef;
+    double* norm2;
+    double* wnorm2;
+};
+constexpr int kAddMaxTerms = 256;
+
+// block of sum_i c_i f_i at one output node: compressed blocks are linear in the function, so the
+// inputs' blocks (own, or generated below the deepest ancestor) are combined as they are
+template <int K>
+__global__ void __launch_bounds__(kMulThreads) k_add(const MulItem* __restrict__ items, AddOut out,
+                                                     const AddIn* __restrict__ in, int nin,
+                                                     const double* __restrict__ FTg) {
+    using G = Geo<K>;
+    constexpr int K2 = G::K2;
+    extern __shared__ __align__(16) double asm_[];
+    double* ACC = asm_;
+    double* T = ACC + G::VOL;
+    double* FT = T + G::VOL;
+    double* unused = FT + K2 * K2;
+    double* red = unused + K2 * K2;
+    int* slot = reinterpret_cast<int*>(red + 64);
+    const int node = items[blockIdx.x].node;
+    for (int i = threadIdx.x; i < K2 * K2; i += blockDim.x) FT[i] = FTg[i];
+    for (int e = threadIdx.x; e < G::VOL; e += blockDim.x) ACC[e] = 0.0;
+    const uint64_t key = out.key[node];
+    __syncthreads();
+    for (int q = 0; q < nin; ++q) {
+        const AddIn f = in[q];
+        mul_fetch<K>(T, FT, f.hk, f.hv, f.hcap, f.coef, key, slot);
+        __syncthreads();
+        for (int e = threadIdx.x; e < G::VOL; e += blockDim.x) ACC[e] = fma(f.c, T[e], ACC[e]);
+        __syncthreads();
+    }
+    double* dst = out.coef + (size_t)node * G::BS;
+    double n2 = 0.0, w2 = 0.0;
+    for (int e = threadIdx.x; e < G::BS; e += blockDim.x) {
+        const int a = e % K2, b = (e / K2) % K2, c = e / (K2 * K2);
+        const double v = ACC[G::at(a, b, c)];
+        dst[e] = v;
+        n2 += v * v;
+        if (!(a < K && b < K && c < K)) w2 += v * v;
+    }
+    block_sum2(n2, w2, red);
+    if (threadIdx.x == 0) {
+        out.norm2[node] = n2;
+        out.wnorm2[node] = w2;
+    }
+}
+
 #define MWB_MUL_DISPATCH_K(k, F)                                                                \
     switch (k) {                                                                                \
         case 4: F(4); break;                                                                    \
@@ -268,20 +327,15 @@ void build_grid(Tree& out, Tree& inp) {
     tree_add_keys(out, add, s);
 }
 
-// out[i] = c[i] a[i] b[i], lock-step passes over the batch
-void multiply_batched(double prec, int n, Tree** out, const double* c, Tree** a, Tree** b, int max_iter) {
-    const Mra* m = a[0]->mra;
+// Refinement passes shared by the product and the linear combination: every pass computes the work
+// nodes of all output trees with one launch (`launch(items, d_items)`), then, unless prec <= 0 or the
+// pass limit is reached, splits the computed nodes whose wavelet norm exceeds prec ||out|| 2^{-depth/2}
+// and makes their children the next work.  Finally every tree is compressed bottom-up with its norms.
+template <typename LaunchF>
+void refine_passes(double prec, int n, Tree** out, int max_iter, LaunchF&& launch) {
+    const Mra* m = out[0]->mra;
     Ctx* ctx = m->ctx;
     cudaStream_t s = ctx->stream;
-    const int K = m->k;
-    for (int i = 0; i < n; ++i) {
-        if (!out[i] || !a[i] || !b[i]) throw Error(MW_ERR_ARG, "null tree");
-        if (out[i]->mra != m || a[i]->mra != m || b[i]->mra != m) throw Error(MW_ERR_ARG, "trees on different worlds");
-        if (a[i]->n == 0 || b[i]->n == 0) throw Error(MW_ERR_STATE, "empty input tree");
-        for (int j = 0; j < n; ++j)
-            if (j != i && out[j] == out[i]) throw Error(MW_ERR_ARG, "output tree listed twice");
-        if (out[i] == a[i] || out[i] == b[i]) throw Error(MW_ERR_ARG, "output tree is also an input");
-    }
     // work: the current leaves of every output tree (roots for an empty tree)
     std::vector<std::vector<int>> work(n);
     std::vector<std::vector<uint64_t>> keys(n);
@@ -294,35 +348,19 @@ void multiply_batched(double prec, int n, Tree** out, const double* c, Tree** a,
             if (c0[q] < 0) work[i].push_back(q);
         keys[i] = host_keys(*out[i], s);
     }
-    std::vector<MulTree> mt(n);
-    MulTree* d_trees = (MulTree*)dalloc(ctx, sizeof(MulTree) * n);
     for (int iter = 0;; ++iter) {
         std::vector<MulItem> items;
-        for (int i = 0; i < n; ++i) {
-            Tree& o = *out[i];
-            mt[i] = MulTree{o.key, o.coef, o.norm2, o.wnorm2, a[i]->hkey, a[i]->hval, a[i]->hcap, a[i]->coef,
-                            b[i]->hkey, b[i]->hval, b[i]->hcap, b[i]->coef, c ? c[i] : 1.0};
+        for (int i = 0; i < n; ++i)
             for (int q : work[i]) items.push_back({i, q});
-        }
         if (items.empty()) break;
-        MWB_CUDA(cudaMemcpyAsync(d_trees, mt.data(), sizeof(MulTree) * n, cudaMemcpyHostToDevice, s));
         MulItem* d_items = (MulItem*)dalloc(ctx, sizeof(MulItem) * items.size());
         MWB_CUDA(cudaMemcpyAsync(d_items, items.data(), sizeof(MulItem) * items.size(), cudaMemcpyHostToDevice, s));
-#define L_MUL(KK)                                                                                                 \
-    {                                                                                                             \
-        const size_t smem = MulCfg<KK>::SMEM;                                                                     \
-        MWB_CUDA(cudaFuncSetAttribute(k_mul<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));        \
-        k_mul<KK><<<(unsigned)items.size(), kMulThreads, smem, s>>>(d_items, d_trees, m->d_MV, m->d_PF, m->d_FT, \
-                                                                     m->n0);                                      \
-    }
-        MWB_MUL_DISPATCH_K(K, L_MUL)
-#undef L_MUL
+        launch(items, d_items);
         MWB_CUDA(cudaGetLastError());
         ctx->launches++;
         MWB_CUDA(cudaStreamSynchronize(s));  // the item list leaves scope
         dfree(ctx, d_items);
         if (prec <= 0.0 || (max_iter >= 0 && iter >= max_iter)) break;
-        // split the computed nodes whose wavelet norm exceeds prec ||out|| 2^{-depth/2}
         std::vector<Tree*> ts(out, out + n);
         std::vector<double> leaf2, max2;
         reduce_norms_many(ts, leaf2, max2, s);
@@ -330,7 +368,7 @@ void multiply_batched(double prec, int n, Tree** out, const double* c, Tree** a,
         for (int i = 0; i < n; ++i) {
             Tree& o = *out[i];
             if (work[i].empty()) continue;
-            // work = the whole last level (always so when the product grows from the roots): split on
+            // work = the whole last level (always so when the tree grows from the roots): split on
             // the device, children appended as the next level
             const int L = o.levels();
             const int lb = o.level_begin[L - 1], le = o.level_begin[L];
@@ -367,8 +405,78 @@ void multiply_batched(double prec, int n, Tree** out, const double* c, Tree** a,
         }
         if (!any) break;
     }
-    dfree(ctx, d_trees);
     trees_finish(std::vector<Tree*>(out, out + n), false, true, true, s);
+    MWB_CUDA(cudaStreamSynchronize(s));
+}
+
+// out[i] = c[i] a[i] b[i], lock-step passes over the batch
+void multiply_batched(double prec, int n, Tree** out, const double* c, Tree** a, Tree** b, int max_iter) {
+    const Mra* m = a[0]->mra;
+    Ctx* ctx = m->ctx;
+    cudaStream_t s = ctx->stream;
+    const int K = m->k;
+    for (int i = 0; i < n; ++i) {
+        if (!out[i] || !a[i] || !b[i]) throw Error(MW_ERR_ARG, "null tree");
+        if (out[i]->mra != m || a[i]->mra != m || b[i]->mra != m) throw Error(MW_ERR_ARG, "trees on different worlds");
+        if (a[i]->n == 0 || b[i]->n == 0) throw Error(MW_ERR_STATE, "empty input tree");
+        for (int j = 0; j < n; ++j)
+            if (j != i && out[j] == out[i]) throw Error(MW_ERR_ARG, "output tree listed twice");
+        if (out[i] == a[i] || out[i] == b[i]) throw Error(MW_ERR_ARG, "output tree is also an input");
+    }
+    std::vector<MulTree> mt(n);
+    MulTree* d_trees = (MulTree*)dalloc(ctx, sizeof(MulTree) * n);
+    refine_passes(prec, n, out, max_iter, [&](const std::vector<MulItem>& items, const MulItem* d_items) {
+        for (int i = 0; i < n; ++i) {  // output arrays may have moved (growth) since the last pass
+            Tree& o = *out[i];
+            mt[i] = MulTree{o.key, o.coef, o.norm2, o.wnorm2, a[i]->hkey, a[i]->hval, a[i]->hcap, a[i]->coef,
+                            b[i]->hkey, b[i]->hval, b[i]->hcap, b[i]->coef, c ? c[i] : 1.0};
+        }
+        MWB_CUDA(cudaMemcpyAsync(d_trees, mt.data(), sizeof(MulTree) * n, cudaMemcpyHostToDevice, s));
+#define L_MUL(KK)                                                                                                 \
+    {                                                                                                             \
+        const size_t smem = MulCfg<KK>::SMEM;                                                                     \
+        MWB_CUDA(cudaFuncSetAttribute(k_mul<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));        \
+        k_mul<KK><<<(unsigned)items.size(), kMulThreads, smem, s>>>(d_items, d_trees, m->d_MV, m->d_PF, m->d_FT, \
+                                                                     m->n0);                                      \
+    }
+        MWB_MUL_DISPATCH_K(K, L_MUL)
+#undef L_MUL
+    });
+    dfree(ctx, d_trees);
+    MWB_CUDA(cudaStreamSynchronize(s));
+}
+
+// out = sum_i c[i] f[i] on one world
+void add_trees(double prec, Tree* out, int n, const double* c, Tree** f, int max_iter) {
+    if (!out || n <= 0 || !f || !c) throw Error(MW_ERR_ARG, "null tree or empty sum");
+    if (n > kAddMaxTerms) throw Error(MW_ERR_ARG, "at most 256 functions per sum");
+    const Mra* m = out->mra;
+    Ctx* ctx = m->ctx;
+    cudaStream_t s = ctx->stream;
+    std::vector<AddIn> in(n);
+    for (int i = 0; i < n; ++i) {
+        if (!f[i]) throw Error(MW_ERR_ARG, "null tree");
+        if (f[i]->mra != m) throw Error(MW_ERR_ARG, "trees on different worlds");
+        if (f[i]->n == 0) throw Error(MW_ERR_STATE, "empty input tree");
+        if (f[i] == out) throw Error(MW_ERR_ARG, "output tree is also an input");
+        in[i] = AddIn{f[i]->hkey, f[i]->hval, f[i]->hcap, f[i]->coef, c[i]};
+    }
+    AddIn* d_in = (AddIn*)dalloc(ctx, sizeof(AddIn) * n);
+    MWB_CUDA(cudaMemcpyAsync(d_in, in.data(), sizeof(AddIn) * n, cudaMemcpyHostToDevice, s));
+    const int K = m->k;
+    Tree* outs[1] = {out};
+    refine_passes(prec, 1, outs, max_iter, [&](const std::vector<MulItem>& items, const MulItem* d_items) {
+        const AddOut ao{out->key, out->coef, out->norm2, out->wnorm2};
+#define L_ADD(KK)                                                                                                   \
+    {                                                                                                               \
+        const size_t smem = MulCfg<KK>::SMEM;                                                                       \
+        MWB_CUDA(cudaFuncSetAttribute(k_add<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));          \
+        k_add<KK><<<(unsigned)items.size(), kMulThreads, smem, s>>>(d_items, ao, d_in, n, m->d_FT);               \
+    }
+        MWB_MUL_DISPATCH_K(K, L_ADD)
+#undef L_ADD
+    });
+    dfree(ctx, d_in);
     MWB_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -420,6 +528,16 @@ int mw_multiply_batched(int n, double prec, mw_tree* out, const double* c, mw_tr
 }
 
 int mw_square(double prec, mw_tree out, mw_tree a, int max_iter) { return mw_multiply(prec, out, 1.0, a, a, max_iter); }
+
+int mw_add(double prec, mw_tree out, int n, const double* c, mw_tree* f, int max_iter) {
+    MWM_TRY({
+        MWM_ARG(out && f && c && n > 0, "null pointer or empty sum");
+        MWB_CUDA(cudaSetDevice(out->mra->ctx->device));
+        std::vector<mwb::Tree*> v(n);
+        for (int q = 0; q < n; ++q) v[q] = f[q];
+        mwb::add_trees(prec, out, n, c, v.data(), max_iter);
+    })
+}
 
 int mw_tree_build_grid(mw_tree out, mw_tree inp) {
     MWM_TRY({

@@ -78,6 +78,7 @@ SYMBOLS = [
     ("mw_multiply_batched", ctypes.c_int, [ctypes.c_int, ctypes.c_double, _vpp, _dp, _vpp, _vpp, ctypes.c_int]),
     ("mw_square", ctypes.c_int, [ctypes.c_double, _vp, _vp, ctypes.c_int]),
     ("mw_tree_build_grid", ctypes.c_int, [_vp, _vp]),
+    ("mw_add", ctypes.c_int, [ctypes.c_double, _vp, ctypes.c_int, _dp, _vpp, ctypes.c_int]),
     ("mw_tree_copy_grid", ctypes.c_int, [_vp, _vp]),
     ("mw_tree_clear", ctypes.c_int, [_vp]),
     ("mw_mlp_create", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_uint, _vpp]),
@@ -420,6 +421,18 @@ def multiply_batched(prec, outs, coefs, a_trees, b_trees, max_iter=-1):
 def square(prec, out: FunctionTree, a: FunctionTree, max_iter=-1):
     """out = a^2: mrcpp::square (reference src/qmfunctions/density_utils.cpp:74)"""
     _check(_lib.mw_square(float(prec), out._h, a._h, int(max_iter)))
+
+
+def add(prec, out: FunctionTree, coefs, trees, max_iter=-1):
+    """out = sum_i coefs[i] trees[i]: mrcpp::add(prec, out, vec, maxIter) (reference
+    src/qmfunctions/qmfunction_utils.cpp:170-177); union-grid form: build_grid(out, t) for every tree,
+    then prec < 0 or max_iter = 0"""
+    n = len(trees)
+    if n != len(coefs):
+        raise MWError("coefficient and tree lists must have equal length")
+    c = np.ascontiguousarray(coefs, dtype=np.float64)
+    arr = (ctypes.c_void_p * n)(*[t._h.value for t in trees])
+    _check(_lib.mw_add(float(prec), out._h, n, _d(c), arr, int(max_iter)))
 
 
 def build_grid(out: FunctionTree, inp: FunctionTree):

@@ -1311,6 +1311,48 @@ void multiply(double prec, Tree& out, double c, const Tree& a, const Tree& b, in
     compress_bottom_up(out);
 }
 
+// out = sum_i c_i f_i (mrcpp::add(prec, out, vec[, maxIter]) contract: reference
+// src/qmfunctions/qmfunction_utils.cpp:170-177, src/qmfunctions/density_utils.cpp:87,
+// src/mrdft/XCFunctional.cpp:713, src/scf_solver/KAIN.cpp:180,192).  Compressed blocks are linear in
+// the function, so a node's block is the combination of the inputs' blocks at that node (their own, or
+// generated below their deepest ancestor); grid and refinement as in multiply().
+void add(double prec, Tree& out, const std::vector<double>& c, const std::vector<const Tree*>& f, int max_iter) {
+    const MRA& mra = *f[0]->mra;
+    const size_t BS = mra.bsize();
+    out.mra = f[0]->mra;
+    if (out.nodes.empty()) out.make_roots();
+    std::vector<int> work;
+    for (int i : out.level_order())
+        if (out.nodes[i].child0 < 0) work.push_back(i);
+    for (int iter = 0; !work.empty(); ++iter) {
+#pragma omp parallel for schedule(dynamic, 4)
+        for (size_t q = 0; q < work.size(); ++q) {
+            Node& nd = out.nodes[work[q]];
+            std::vector<double> blk(BS);
+            std::fill(nd.c.begin(), nd.c.end(), 0.0);
+            for (size_t i = 0; i < f.size(); ++i) {
+                block_at(*f[i], nd.depth, nd.t, blk.data());
+                for (size_t e = 0; e < BS; ++e) nd.c[e] += c[i] * blk[e];
+            }
+        }
+        if (prec <= 0.0 || (max_iter >= 0 && iter >= max_iter)) break;
+        const double ref = std::sqrt(out.square_norm());
+        std::vector<int> next;
+        for (int i : work) {
+            const Node& nd = out.nodes[i];
+            if (nd.depth >= mra.max_depth) continue;
+            const double w = std::sqrt(wavelet_sq_norm(nd.c.data(), mra.k()));
+            if (w > split_threshold(prec, ref, nd.depth)) {
+                out.split(i);
+                const int c0 = out.nodes[i].child0;
+                for (int ch = 0; ch < 8; ++ch) next.push_back(c0 + ch);
+            }
+        }
+        work.swap(next);
+    }
+    compress_bottom_up(out);
+}
+
 // extend the grid of `out` by the grid of `inp` (union; new nodes have zero blocks)
 void build_grid(Tree& out, const Tree& inp) {
     out.mra = inp.mra;
@@ -1479,6 +1521,14 @@ int oracle_apply(double prec, void* out, void* op, void* inp, long long* stats) 
 // out = c a b (mrcpp::multiply contract); returns the number of output nodes
 int oracle_multiply(double prec, void* out, double c, void* a, void* b, int max_iter) {
     multiply(prec, *(Tree*)out, c, *(Tree*)a, *(Tree*)b, max_iter);
+    return (int)((Tree*)out)->nodes.size();
+}
+// out = sum_i c[i] f[i] (mrcpp::add contract); returns the number of output nodes
+int oracle_add(double prec, void* out, int n, const double* c, void* const* f, int max_iter) {
+    std::vector<double> cv(c, c + n);
+    std::vector<const Tree*> fv;
+    for (int i = 0; i < n; ++i) fv.push_back((const Tree*)f[i]);
+    add(prec, *(Tree*)out, cv, fv, max_iter);
     return (int)((Tree*)out)->nodes.size();
 }
 // union of grids (mrcpp::build_grid contract); returns the number of nodes of `out`

@@ -64,6 +64,7 @@ def lib():
         L.oracle_apply.argtypes = [ctypes.c_double, _vp, _vp, _vp, _lp]
         L.oracle_multiply.argtypes = [ctypes.c_double, _vp, ctypes.c_double, _vp, _vp, ctypes.c_int]
         L.oracle_build_grid.argtypes = [_vp, _vp]
+        L.oracle_add.argtypes = [ctypes.c_double, _vp, ctypes.c_int, _dp, ctypes.POINTER(_vp), ctypes.c_int]
         _lib = L
     return _lib
 
@@ -246,3 +247,12 @@ def multiply(prec, out: FunctionTree, c, a: FunctionTree, b: FunctionTree, max_i
 def build_grid(out: FunctionTree, inp: FunctionTree):
     """extend the grid of `out` by that of `inp` (mrcpp::build_grid, qmfunction_utils.cpp:211-212)"""
     return lib().oracle_build_grid(out._h, inp._h)
+
+
+def add(prec, out: FunctionTree, coefs, trees, max_iter=-1):
+    """out = sum_i coefs[i] trees[i] (mrcpp::add contract, qmfunction_utils.cpp:170-177); returns the
+    number of output nodes"""
+    n = len(trees)
+    c = np.ascontiguousarray(coefs, dtype=np.float64)
+    arr = (_vp * n)(*[t._h for t in trees])
+    return lib().oracle_add(float(prec), out._h, n, _d(c), arr, int(max_iter))

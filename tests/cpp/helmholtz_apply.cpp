@@ -56,5 +56,10 @@ int main() {
     mrcpp::copy_grid(rho, phi);
     mrcpp::square(prec, rho, phi);
     std::printf("density nodes %d norm2 %.15e dot %.15e\n", rho.getNNodes(), rho.getSquareNorm(), mrcpp::dot(rho, phi));
+
+    // HelmholtzVector::apply's argument V phi + psi (HelmholtzVector.cpp:133-135): an adaptive sum
+    mrcpp::FunctionTree<3> arg(MRA);
+    mrcpp::add(prec, arg, 1.0, out, -2.0, phi);
+    std::printf("sum nodes %d norm2 %.15e dot %.15e\n", arg.getNNodes(), arg.getSquareNorm(), mrcpp::dot(arg, phi));
     return 0;
 }

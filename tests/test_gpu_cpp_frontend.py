@@ -44,7 +44,9 @@ def test_cpp_frontend_matches_python(gpu_mod, tmp_path):
     rho = G.FunctionTree(m)
     G.copy_grid(rho, phi)
     G.square(prec, rho, phi)
-    for key, t in (("helmholtz", out_h), ("poisson", V), ("exchange", V_ip), ("density", rho)):
+    arg = G.FunctionTree(m)
+    G.add(prec, arg, [1.0, -2.0], [out_h, phi])
+    for key, t in (("helmholtz", out_h), ("poisson", V), ("exchange", V_ip), ("density", rho), ("sum", arg)):
         n, n2, d = vals[key]
         assert n == t.nnodes()
         assert abs(n2 - t.square_norm()) <= 1e-12 * t.square_norm()
