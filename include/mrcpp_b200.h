@@ -190,6 +190,34 @@ public:
     }
 };
 
+// first derivative with flux parameters a, b (reference src/SCFDriver.cpp:282-283)
+template <int D> class DerivativeOperator;
+template <> class DerivativeOperator<3> {
+public:
+    DerivativeOperator(const DerivativeOperator&) = delete;
+    DerivativeOperator& operator=(const DerivativeOperator&) = delete;
+    ~DerivativeOperator() {
+        if (h_) mw_op_destroy(h_);
+    }
+    mw_op handle() const { return h_; }
+
+protected:
+    DerivativeOperator() = default;
+    mw_op h_ = nullptr;
+};
+template <int D> class ABGVOperator;
+template <> class ABGVOperator<3> : public DerivativeOperator<3> {
+public:
+    ABGVOperator(const MultiResolutionAnalysis<3>& mra, double a, double b) {
+        detail::check(mw_op_create_abgv(mra.handle(), a, b, &h_), "ABGVOperator");
+    }
+};
+// out = d/dx_dir inp on the input's grid (reference NablaOperator.cpp:35)
+template <int D> void apply(FunctionTree<D>& out, DerivativeOperator<D>& op, FunctionTree<D>& inp, int dir);
+template <> inline void apply<3>(FunctionTree<3>& out, DerivativeOperator<3>& op, FunctionTree<3>& inp, int dir) {
+    detail::check(mw_apply_derivative(out.handle(), op.handle(), inp.handle(), dir, MW_APPLY_FP64), "apply");
+}
+
 // out = op * inp, adaptive to relative precision prec
 template <int D> void apply(double prec, FunctionTree<D>& out, ConvolutionOperator<D>& op, FunctionTree<D>& inp);
 template <> inline void apply<3>(double prec, FunctionTree<3>& out, ConvolutionOperator<3>& op, FunctionTree<3>& inp) {

@@ -122,6 +122,14 @@ int mw_nalloc_dot(mw_tree a, mw_tree b, double* out);
  * (reference src/scf_solver/HelmholtzVector.cpp:171).  Kernels 1/|r| and exp(-mu|r|)/|r|. */
 int mw_op_create_poisson(mw_mra mra, double prec, mw_op* out);
 int mw_op_create_helmholtz(mw_mra mra, double mu, double prec, mw_op* out);
+/* First-derivative operator with numerical flux parameters a, b in [0, 1] (Alpert, Beylkin, Gines &
+ * Vozovoi 2002; a = b = 0: the cell-local derivative, a = b = 1/2: central flux).  Replaces
+ * mrcpp::ABGVOperator<3>(MRA, a, b): reference src/SCFDriver.cpp:282-283, src/mrdft/XCFunctional.cpp:67. */
+int mw_op_create_abgv(mw_mra mra, double a, double b, mw_op* out);
+/* out = d/dx_dir inp (dir 0, 1, 2 = x, y, z) on the input's grid (no refinement).  Replaces
+ * mrcpp::apply(out, D, inp, dir): reference src/qmoperators/one_electron/NablaOperator.cpp:35,40,
+ * MomentumOperator.cpp:35,41.  `out` is overwritten and left compressed with valid norms. */
+int mw_apply_derivative(mw_tree out, mw_op op, mw_tree inp, int dir, int flags);
 int mw_op_destroy(mw_op op);
 int mw_op_nterms(mw_op op, int* n);
 int mw_op_terms(mw_op op, double* alpha, double* beta);

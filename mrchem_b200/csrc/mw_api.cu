@@ -287,15 +287,92 @@ static double bound3(double beta, const double* t, const double* x, bool root) {
     return beta * std::sqrt(v);
 }
 
+// Tables of a first-derivative operator along `dir` at one depth: one term (beta = 1) whose factor
+// along `dir` is the derivative's NS matrix for the offset and the identity along the other two
+// directions; offsets -1, 0, 1 along `dir`.  The NS matrix of offset l at scale n is
+// F [[T(2l) T(2l-1)]; [T(2l+1) T(2l)]] F^T with T(d) = 2^{n+1} T_unit(d) at the children's scale.
+static void derivative_depth(Op& op, int depth, int dir, OpDepth& od, std::vector<double>& mbeta) {
+    const Mra& m = *op.mra;
+    const int k = m.k, K2 = 2 * k;
+    const double fac = std::ldexp(1.0, m.n0 + depth + 1);
+    auto Tc = [&](int d, int i, int j) -> double {  // children-scale block T(d)[i][j]
+        return (d < -1 || d > 1) ? 0.0 : fac * op.dT[d + 1][(size_t)i * k + j];
+    };
+    std::vector<double> ident((size_t)K2 * K2, 0.0);
+    for (int a = 0; a < K2; ++a) ident[(size_t)a * K2 + a] = 1.0;
+    od.mats = ident;  // matrix 0: identity
+    double tn[3], xn[3];
+    const double ti = (double)k, xi = (double)k;  // identity: k ones in the s-s block, k elsewhere
+    for (int l = -1; l <= 1; ++l) {
+        std::vector<double> C((size_t)K2 * K2, 0.0), tmp((size_t)K2 * K2, 0.0), NS((size_t)K2 * K2, 0.0);
+        for (int co = 0; co < 2; ++co)
+            for (int ci = 0; ci < 2; ++ci)
+                for (int i = 0; i < k; ++i)
+                    for (int j = 0; j < k; ++j) C[(size_t)(co * k + i) * K2 + ci * k + j] = Tc(2 * l + co - ci, i, j);
+        for (int a = 0; a < K2; ++a)
+            for (int c = 0; c < K2; ++c) {
+                double v = 0.0;
+                for (int b = 0; b < K2; ++b) v += m.F[(size_t)a * K2 + b] * C[(size_t)b * K2 + c];
+                tmp[(size_t)a * K2 + c] = v;
+            }
+        double t2 = 0.0, x2 = 0.0;
+        for (int a = 0; a < K2; ++a)
+            for (int c = 0; c < K2; ++c) {
+                double v = 0.0;
+                for (int b = 0; b < K2; ++b) v += tmp[(size_t)a * K2 + b] * m.F[(size_t)c * K2 + b];
+                NS[(size_t)a * K2 + c] = v;
+                (a < k && c < k ? t2 : x2) += v * v;
+            }
+        tn[l + 1] = t2;
+        xn[l + 1] = x2;
+        od.mats.insert(od.mats.end(), NS.begin(), NS.end());  // matrix 2 + l
+    }
+    const bool root = depth == 0;
+    std::vector<std::pair<DeltaRec, TermRec>> rows;
+    for (int l = -1; l <= 1; ++l) {
+        double t[3], x[3];
+        for (int d = 0; d < 3; ++d) {
+            t[d] = d == dir ? tn[l + 1] : ti;
+            x[d] = d == dir ? xn[l + 1] : xi;
+        }
+        const double bd = bound3(1.0, t, x, root);
+        if (!(bd > 0.0)) continue;
+        DeltaRec dr{};
+        dr.d[dir] = l;
+        dr.maxb = bd;
+        TermRec tr{};
+        tr.m = 0;
+        tr.mx = dir == 0 ? 2 + l : 0;
+        tr.my = dir == 1 ? 2 + l : 0;
+        tr.mz = dir == 2 ? 2 + l : 0;
+        tr.beta = 1.0;
+        tr.bound = bd;
+        rows.emplace_back(dr, tr);
+    }
+    std::stable_sort(rows.begin(), rows.end(), [](const auto& a, const auto& b) { return a.first.maxb > b.first.maxb; });
+    for (auto& r : rows) {
+        r.first.t0 = (int)od.terms.size();
+        od.terms.push_back(r.second);
+        r.first.t1 = (int)od.terms.size();
+        od.deltas.push_back(r.first);
+    }
+    mbeta.assign(4, 1.0);
+}
+
 // build (once) and upload the tables of one depth
-static const OpDepth& op_depth(Op& op, int depth) {
+static const OpDepth& op_depth(Op& op, int depth, int dir = 0) {
     std::lock_guard<std::mutex> g(op.mtx);
-    auto it = op.depths.find(depth);
+    const int ckey = op.kind == 1 ? 3 * depth + dir : depth;
+    auto it = op.depths.find(ckey);
     if (it != op.depths.end()) return *it->second;
     const Mra& m = *op.mra;
     const int K2 = 2 * m.k;
-    std::vector<BandTmp> bs = op_bands(op, depth);
     auto od = std::make_unique<OpDepth>();
+    std::vector<double> mbeta;  // the term weight of every stored matrix (z-step tables)
+    if (op.kind == 1) {
+        derivative_depth(op, depth, dir, *od, mbeta);
+    } else {
+    std::vector<BandTmp> bs = op_bands(op, depth);
     std::vector<int> base(bs.size(), -1);
     for (size_t mi = 0; mi < bs.size(); ++mi) {
         if (!bs[mi].active) continue;
@@ -362,6 +439,12 @@ static const OpDepth& op_depth(Op& op, int depth) {
         r.first.t1 = (int)od->terms.size();
         od->deltas.push_back(r.first);
     }
+    mbeta.assign(od->mats.size() / ((size_t)K2 * K2), 0.0);
+    for (size_t mi = 0; mi < bs.size(); ++mi) {
+        if (!bs[mi].active) continue;
+        for (int q = 0; q < 2 * bs[mi].L + 1; ++q) mbeta[base[mi] + q] = op.terms[mi].beta;
+    }
+    }
     Ctx* ctx = m.ctx;
     cudaStream_t s = ctx->stream;
     od->d_mats = (double*)dalloc(ctx, sizeof(double) * std::max<size_t>(1, od->mats.size()));
@@ -372,11 +455,7 @@ static const OpDepth& op_depth(Op& op, int depth) {
     od->d_matsb32 = (float*)dalloc(ctx, sizeof(float) * std::max<size_t>(1, od->mats.size()));
     std::vector<float> m32(od->mats.begin(), od->mats.end());
     std::vector<double> mb(od->mats.size());
-    for (size_t mi = 0; mi < bs.size(); ++mi) {
-        if (!bs[mi].active) continue;
-        const size_t b0 = (size_t)base[mi] * K2 * K2, n = (size_t)(2 * bs[mi].L + 1) * K2 * K2;
-        for (size_t q = 0; q < n; ++q) mb[b0 + q] = op.terms[mi].beta * od->mats[b0 + q];
-    }
+    for (size_t q = 0; q < od->mats.size(); ++q) mb[q] = mbeta[q / ((size_t)K2 * K2)] * od->mats[q];
     std::vector<float> mb32(mb.begin(), mb.end());
     // transposed, zero-padded copies for the GEMM-tiled contraction
     const int KP = (K2 + 3) / 4 * 4;
@@ -410,7 +489,7 @@ static const OpDepth& op_depth(Op& op, int depth) {
     if (!od->terms.empty())
         MWB_CUDA(cudaMemcpyAsync(od->d_terms, od->terms.data(), sizeof(TermRec) * od->terms.size(), cudaMemcpyHostToDevice, s));
     MWB_CUDA(cudaStreamSynchronize(s));
-    return *op.depths.emplace(depth, std::move(od)).first->second;
+    return *op.depths.emplace(ckey, std::move(od)).first->second;
 }
 
 static void op_init(Op& op, Mra* m, double mu, double prec) {
@@ -475,6 +554,8 @@ static void add_children_many(const std::vector<Tree*>& ts, const std::vector<st
 // run in lock-step over the batch (one launch per stage for all trees of a depth).
 static void apply_batched(double prec, int n, Tree** out, Op** op, Tree** inp, int precision) {
     if (n <= 0) throw Error(MW_ERR_ARG, "empty batch");
+    for (int i = 0; i < n; ++i)
+        if (op[i] && op[i]->kind != 0) throw Error(MW_ERR_ARG, "derivative operators are applied with mw_apply_derivative");
     if (n > 128) throw Error(MW_ERR_ARG, "at most 128 trees per batch");
     const Mra* m = inp[0]->mra;
     for (int i = 0; i < n; ++i) {
@@ -568,7 +649,7 @@ struct Entry {
 };
 static long long run_entries(double prec, int precision, const std::vector<Entry>& ents, Tree** out, Op** op,
                              Tree** inp, const std::vector<double>& fnorm, const std::vector<double>& nu_max,
-                             const std::vector<double>& g0) {
+                             const std::vector<double>& g0, int dir = 0) {
     long long trip = 0;
     cudaStream_t s = out[0]->mra->ctx->stream;
     for (size_t e0 = 0; e0 < ents.size(); e0 += 128) {
@@ -580,7 +661,7 @@ static long long run_entries(double prec, int precision, const std::vector<Entry
             BatchTree bt;
             bt.out = out[i];
             bt.inp = inp[i];
-            bt.tab = &op_depth(*op[i], en.depth);
+            bt.tab = &op_depth(*op[i], en.depth, dir);
             bt.obegin = en.begin;
             bt.oend = en.end;
             bt.prec = prec;
@@ -622,6 +703,8 @@ static void apply_learned(double prec, int n, Tree** out, Op** op, Tree** inp, i
                 throw Error(MW_ERR_ARG, "output trees must be distinct from each other and from the inputs");
     }
     if (!(prec > 0.0)) throw Error(MW_ERR_ARG, "the learned apply needs prec > 0");
+    for (int i = 0; i < n; ++i)
+        if (op[i]->kind != 0) throw Error(MW_ERR_ARG, "derivative operators are applied with mw_apply_derivative");
     Ctx* ctx = m->ctx;
     cudaStream_t s = ctx->stream;
     const float logit_tau = std::log(tau / (1.0f - tau));
@@ -817,6 +900,48 @@ static void apply_learned(double prec, int n, Tree** out, Op** op, Tree** inp, i
         stats[4] = missed;
         stats[5] = nout;
     }
+}
+
+// out = d/dx_dir inp on the input's grid (no refinement, no screening): the output takes the input's
+// nodes, every level is one entry of a single pass set, then sum-up, compression and norms.
+static void apply_derivative(Tree* out, Op* op, Tree* inp, int dir, int precision) {
+    if (!out || !op || !inp) throw Error(MW_ERR_ARG, "null tree or operator");
+    if (op->kind != 1) throw Error(MW_ERR_ARG, "not a derivative operator");
+    if (dir < 0 || dir > 2) throw Error(MW_ERR_ARG, "direction must be 0, 1 or 2");
+    if (out->mra != inp->mra || op->mra != inp->mra) throw Error(MW_ERR_ARG, "trees and operator on different worlds");
+    if (inp->n == 0) throw Error(MW_ERR_STATE, "input tree is empty");
+    if (out == inp) throw Error(MW_ERR_ARG, "output tree is also the input");
+    Ctx* ctx = inp->mra->ctx;
+    cudaStream_t s = ctx->stream;
+    // grid of the input
+    out->n = 0;
+    tree_reserve(*out, inp->n);
+    MWB_CUDA(cudaMemcpyAsync(out->key, inp->key, sizeof(uint64_t) * inp->n, cudaMemcpyDeviceToDevice, s));
+    MWB_CUDA(cudaMemcpyAsync(out->parent, inp->parent, sizeof(int) * inp->n, cudaMemcpyDeviceToDevice, s));
+    MWB_CUDA(cudaMemcpyAsync(out->child0, inp->child0, sizeof(int) * inp->n, cudaMemcpyDeviceToDevice, s));
+    out->n = inp->n;
+    out->level_begin = inp->level_begin;
+    launch_hash_reset(*out, s);
+    launch_hash_insert(*out, 0, out->n, s);
+    std::vector<Tree*> ins{inp};
+    std::vector<double> l2, m2;
+    reduce_norms_many(ins, l2, m2, s);
+    std::vector<double> fnorm{std::sqrt(l2[0])}, nu_max{std::sqrt(m2[0])}, g0{0.0};
+    std::vector<Entry> ents;
+    for (int d = 0; d < out->levels(); ++d)
+        if (out->level_begin[d + 1] > out->level_begin[d]) ents.push_back(Entry{0, d, out->level_begin[d], out->level_begin[d + 1]});
+    Tree* o[1] = {out};
+    Op* p[1] = {op};
+    Tree* i1[1] = {inp};
+    const long long trip = run_entries(0.0, precision, ents, o, p, i1, fnorm, nu_max, g0, dir);
+    trees_finish(std::vector<Tree*>{out}, true, true, true, s);
+    MWB_CUDA(cudaStreamSynchronize(s));
+    out->g0 = 0.0;
+    out->prec = 0.0;
+    out->stats[0] = trip;
+    out->stats[1] = trip;
+    out->stats[2] = (long long)((ents.size() + 127) / 128);
+    out->stats[3] = out->n;
 }
 
 // features and labels (split or not) of the non-root nodes of an applied output tree
@@ -1267,6 +1392,30 @@ int mw_op_create_helmholtz(mw_mra m, double mu, double prec, mw_op* out) {
             throw;
         }
         *out = op;
+    })
+}
+
+int mw_op_create_abgv(mw_mra m, double a, double b, mw_op* out) {
+    MW_TRY({
+        MW_ARG(m && out, "null pointer");
+        MW_ARG(a >= 0.0 && a <= 1.0 && b >= 0.0 && b <= 1.0, "flux parameters must lie in [0, 1]");
+        MWB_CUDA(cudaSetDevice(m->ctx->device));
+        auto* op = new mw_op_s();
+        op->mra = m;
+        op->kind = 1;
+        op->da = a;
+        op->db = b;
+        derivative_blocks(m->basis, a, b, op->dT);
+        *out = op;
+    })
+}
+
+int mw_apply_derivative(mw_tree out, mw_op op, mw_tree inp, int dir, int flags) {
+    MW_TRY({
+        MW_ARG(out && op && inp, "null pointer");
+        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32, "unknown apply flags");
+        MWB_CUDA(cudaSetDevice(inp->mra->ctx->device));
+        apply_derivative(out, op, inp, dir, flags);
     })
 }
 

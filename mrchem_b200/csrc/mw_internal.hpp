@@ -97,6 +97,9 @@ struct OpDepth {
 
 struct Op {
     Mra* mra = nullptr;
+    int kind = 0;                  // 0: separated-Gaussian convolution; 1: first derivative (ABGV)
+    double da = 0.0, db = 0.0;     // derivative flux parameters
+    std::vector<double> dT[3];     // derivative unit-scale blocks T(-1), T(0), T(1), k x k
     double mu = 0.0, prec = 0.0, eps = 0.0;
     std::vector<GaussTerm> terms;
     std::unique_ptr<GaussianOperatorBuilder> builder;

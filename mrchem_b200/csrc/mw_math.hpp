@@ -64,6 +64,19 @@ inline void leg01(double t, int np, double* out) {
     }
 }
 
+// d/dt of the normalised shifted Legendre polynomials Pt_p(t) = sqrt(2p+1) P_p(2t - 1) on [0,1],
+// from P'_{p+1} = P'_{p-1} + (2p + 1) P_p
+inline void leg01_deriv(double t, int np, double* out) {
+    const double z = 2.0 * t - 1.0;
+    std::vector<double> P(np + 1), dP(np + 1, 0.0);
+    P[0] = 1.0;
+    if (np > 0) P[1] = z;
+    for (int p = 1; p < np; ++p) P[p + 1] = ((2.0 * p + 1.0) * z * P[p] - p * P[p - 1]) / (p + 1.0);
+    if (np > 1) dP[1] = 1.0;
+    for (int p = 1; p + 1 < np; ++p) dP[p + 1] = dP[p - 1] + (2.0 * p + 1.0) * P[p];
+    for (int p = 0; p < np; ++p) out[p] = 2.0 * std::sqrt(2.0 * p + 1.0) * dP[p];
+}
+
 struct ScalingBasis {
     int type = 0;  // 0 interpolating (Gauss-Legendre nodes), 1 Legendre
     int k = 0;
@@ -91,7 +104,51 @@ struct ScalingBasis {
             out[j] = v * std::sqrt(qw[j]);
         }
     }
+    // first derivatives of all k scaling functions at x in [0,1]
+    void derivs(double x, double* out) const {
+        std::vector<double> L(k);
+        leg01_deriv(x, k, L.data());
+        if (type == 1) {
+            for (int j = 0; j < k; ++j) out[j] = L[j];
+            return;
+        }
+        for (int j = 0; j < k; ++j) {
+            double v = 0.0;
+            for (int i = 0; i < k; ++i) v += lq[j * k + i] * L[i];
+            out[j] = v * std::sqrt(qw[j]);
+        }
+    }
 };
+
+// Unit-scale blocks of the first-derivative operator with numerical flux parameters (a, b)
+// (Alpert, Beylkin, Gines & Vozovoi 2002).  On a cell, integrating phi_i f' by parts with the value
+// of f at the right interface taken as (1-a) f_left + a f_right and at the left interface as
+// b f_left + (1-b) f_right gives, for output cell l and input cell l - delta:
+//   T(0)[i][j]  = (1-a) phi_i(1) phi_j(1) - (1-b) phi_i(0) phi_j(0) - int phi_i' phi_j
+//   T(-1)[i][j] = a phi_i(1) phi_j(0)        (input cell l + 1)
+//   T(+1)[i][j] = -b phi_i(0) phi_j(1)       (input cell l - 1)
+// a = b = 0: the cell-local derivative; a = b = 1/2: the central flux.  At scale n the blocks scale
+// with 2^n.  T[delta + 1] holds T(delta), k x k row-major.
+inline void derivative_blocks(const ScalingBasis& B, double a, double b, std::vector<double> T[3]) {
+    const int k = B.k;
+    std::vector<double> p0(k), p1(k), dq(k), pq(k);
+    B.values(0.0, p0.data());
+    B.values(1.0, p1.data());
+    for (int d = 0; d < 3; ++d) T[d].assign((size_t)k * k, 0.0);
+    std::vector<double> I(k * k, 0.0);  // int phi_i' phi_j (k-point rule exact: degree 2k - 3)
+    for (int q = 0; q < k; ++q) {
+        B.derivs(B.qx[q], dq.data());
+        B.values(B.qx[q], pq.data());
+        for (int i = 0; i < k; ++i)
+            for (int j = 0; j < k; ++j) I[i * k + j] += B.qw[q] * dq[i] * pq[j];
+    }
+    for (int i = 0; i < k; ++i)
+        for (int j = 0; j < k; ++j) {
+            T[1][i * k + j] = (1.0 - a) * p1[i] * p1[j] - (1.0 - b) * p0[i] * p0[j] - I[i * k + j];
+            T[0][i * k + j] = a * p1[i] * p0[j];
+            T[2][i * k + j] = -b * p0[i] * p1[j];
+        }
+}
 
 // Two-scale filter F = [[H0 H1];[G0 G1]] (2k x 2k, row-major).  H by exact 2k-point quadrature;
 // G rows: orthonormal complement built from [e_j, -e_j]/sqrt2 by twice-repeated Gram-Schmidt.

@@ -68,6 +68,8 @@ SYMBOLS = [
     ("mw_tree_distance", ctypes.c_int, [_vp, _vp, _dp]),
     ("mw_op_create_poisson", ctypes.c_int, [_vp, ctypes.c_double, _vpp]),
     ("mw_op_create_helmholtz", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _vpp]),
+    ("mw_op_create_abgv", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_double, _vpp]),
+    ("mw_apply_derivative", ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int]),
     ("mw_op_destroy", ctypes.c_int, [_vp]),
     ("mw_op_nterms", ctypes.c_int, [_vp, _ip]),
     ("mw_op_terms", ctypes.c_int, [_vp, _dp, _dp]),
@@ -369,6 +371,28 @@ class HelmholtzOperator(ConvolutionOperator):
         if not mu > 0.0:
             raise MWError("mu must be positive")
         super().__init__(mra, mu, prec)
+
+
+class ABGVOperator:
+    """First derivative with flux parameters a, b (mrcpp::ABGVOperator<3>(MRA, a, b), reference
+    src/SCFDriver.cpp:282-283)."""
+
+    def __init__(self, mra, a, b):
+        self.mra = mra
+        h = ctypes.c_void_p()
+        _check(load_library().mw_op_create_abgv(mra._h, float(a), float(b), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.mw_op_destroy(self._h)
+            self._h = None
+
+
+def apply_derivative(out: FunctionTree, op: ABGVOperator, inp: FunctionTree, direction, flags=APPLY_FP64):
+    """out = d/dx_dir inp on the input's grid: mrcpp::apply(out, D, inp, dir) (reference
+    src/qmoperators/one_electron/NablaOperator.cpp:35)."""
+    _check(_lib.mw_apply_derivative(out._h, op._h, inp._h, int(direction), int(flags)))
 
 
 def apply_batched(prec, outs, ops, inps, flags=APPLY_FP64):

@@ -87,6 +87,23 @@ void gauss_legendre01(int n, std::vector<double>& x, std::vector<double>& w) {
     }
 }
 
+// d/dt Pt_p(t) for p < np, from (1 - z^2) P_p'(z) = p (P_{p-1}(z) - z P_p(z)) away from the ends and
+// P_p'(+-1) = (+-1)^{p+1} p (p + 1) / 2 at them
+inline void legendre01_deriv(double t, int np, double* out) {
+    const double z = 2.0 * t - 1.0;
+    std::vector<double> P(np + 1);
+    P[0] = 1.0;
+    if (np > 0) P[1] = z;
+    for (int p = 1; p < np; ++p) P[p + 1] = ((2.0 * p + 1.0) * z * P[p] - p * P[p - 1]) / (p + 1.0);
+    for (int p = 0; p < np; ++p) {
+        double d;
+        if (p == 0) d = 0.0;
+        else if (std::fabs(1.0 - z * z) < 1e-12) d = (z > 0 ? 1.0 : ((p + 1) % 2 == 0 ? 1.0 : -1.0)) * 0.5 * p * (p + 1.0);
+        else d = p * (P[p - 1] - z * P[p]) / (1.0 - z * z);
+        out[p] = 2.0 * std::sqrt(2.0 * p + 1.0) * d;
+    }
+}
+
 // Orthonormal shifted Legendre polynomials Pt_p(t) = sqrt(2p+1) P_p(2t-1) on [0,1], p < np.
 inline void legendre01(double t, int np, double* out) {
     double z = 2.0 * t - 1.0;
@@ -126,6 +143,17 @@ struct Basis {
     }
     void phi_all(double x, double* out) const {
         for (int j = 0; j < k; ++j) out[j] = phi(j, x);
+    }
+    // phi_j'(x) on [0,1]
+    double dphi(int j, double x) const {
+        std::vector<double> L(k);
+        legendre01_deriv(x, k, L.data());
+        if (type == 1) return L[j];
+        std::vector<double> Lj(k);
+        legendre01(qx[j], k, Lj.data());
+        double v = 0.0;
+        for (int i = 0; i < k; ++i) v += Lj[i] * L[i];
+        return v * std::sqrt(qw[j]);
     }
 
     void build(int type_, int order) {
@@ -1311,6 +1339,124 @@ void multiply(double prec, Tree& out, double c, const Tree& a, const Tree& b, in
     compress_bottom_up(out);
 }
 
+// ---------------------------------------------------------------------------------------------
+// First-derivative operator (Alpert, Beylkin, Gines & Vozovoi 2002), contract of
+// mrcpp::ABGVOperator<3>(MRA, a, b) + mrcpp::apply(out, D, inp, dir) (reference src/SCFDriver.cpp:282,
+// src/qmoperators/one_electron/NablaOperator.cpp:35).  Flux: at the right interface of a cell
+// f = (1-a) f_left + a f_right, at the left interface f = b f_left + (1-b) f_right; integrating
+// phi_i f' by parts on the cell gives the unit-scale blocks for output cell l, input cell l - d:
+//   T(0) = (1-a) phi(1) phi(1)^T - (1-b) phi(0) phi(0)^T - <phi', phi>,
+//   T(-1) = a phi(1) phi(0)^T,  T(+1) = -b phi(0) phi(1)^T,  scaled by 2^n at scale n.
+// The apply is the non-standard form on the input's grid: for each node, the derivative's NS matrix
+// of the offset along dir (identity along the other directions) on the input blocks of the same
+// scale (own or generated), the s->s block removed below the root, then sum-up and compression.
+// ---------------------------------------------------------------------------------------------
+void derivative_unit_blocks(const Basis& B, double a, double b, std::vector<double> T[3]) {
+    const int k = B.k;
+    std::vector<double> p0(k), p1(k);
+    for (int j = 0; j < k; ++j) {
+        p0[j] = B.phi(j, 0.0);
+        p1[j] = B.phi(j, 1.0);
+    }
+    for (int d = 0; d < 3; ++d) T[d].assign((size_t)k * k, 0.0);
+    for (int i = 0; i < k; ++i)
+        for (int j = 0; j < k; ++j) {
+            double I = 0.0;
+            for (int q = 0; q < k; ++q) I += B.qw[q] * B.dphi(i, B.qx[q]) * B.phi(j, B.qx[q]);
+            T[1][i * k + j] = (1.0 - a) * p1[i] * p1[j] - (1.0 - b) * p0[i] * p0[j] - I;
+            T[0][i * k + j] = a * p1[i] * p0[j];
+            T[2][i * k + j] = -b * p0[i] * p1[j];
+        }
+}
+
+// NS matrix of the derivative at depth, offset l: F [[T(2l) T(2l-1)]; [T(2l+1) T(2l)]] F^T with the
+// children-scale blocks 2^{n+1} T_unit
+std::vector<double> derivative_ns(const MRA& mra, const std::vector<double> T[3], int depth, int l) {
+    const int k = mra.k(), K2 = 2 * k;
+    const double fac = std::ldexp(1.0, mra.n0 + depth + 1);
+    std::vector<double> C((size_t)K2 * K2, 0.0), NS((size_t)K2 * K2, 0.0), tmp((size_t)K2 * K2, 0.0);
+    for (int co = 0; co < 2; ++co)
+        for (int ci = 0; ci < 2; ++ci) {
+            const int d = 2 * l + co - ci;
+            if (d < -1 || d > 1) continue;
+            for (int i = 0; i < k; ++i)
+                for (int j = 0; j < k; ++j) C[(size_t)(co * k + i) * K2 + ci * k + j] = fac * T[d + 1][i * k + j];
+        }
+    const std::vector<double>& F = mra.basis.F;
+    for (int a = 0; a < K2; ++a)
+        for (int c = 0; c < K2; ++c)
+            for (int b = 0; b < K2; ++b) tmp[(size_t)a * K2 + c] += F[(size_t)a * K2 + b] * C[(size_t)b * K2 + c];
+    for (int a = 0; a < K2; ++a)
+        for (int c = 0; c < K2; ++c)
+            for (int b = 0; b < K2; ++b) NS[(size_t)a * K2 + c] += tmp[(size_t)a * K2 + b] * F[(size_t)c * K2 + b];
+    return NS;
+}
+
+void derivative_apply(Tree& out, const Tree& inp, double a, double b, int dir) {
+    const MRA& mra = *inp.mra;
+    const int k = mra.k(), K2 = 2 * k;
+    const size_t BS = mra.bsize(), SS = (size_t)k * k * k;
+    std::vector<double> T[3];
+    derivative_unit_blocks(mra.basis, a, b, T);
+    // the input's grid
+    out.mra = inp.mra;
+    out.clear();
+    for (const Node& nd : inp.nodes) {
+        Node c;
+        c.depth = nd.depth;
+        for (int d = 0; d < 3; ++d) c.t[d] = nd.t[d];
+        c.parent = nd.parent;
+        c.child0 = nd.child0;
+        c.c.assign(BS, 0.0);
+        out.nodes.push_back(std::move(c));
+        out.index[node_key(nd.depth, nd.t)] = (int)out.nodes.size() - 1;
+    }
+    std::map<std::pair<int, int>, std::vector<double>> ns;  // (depth, l) -> NS matrix
+    int maxd = out.max_depth_present();
+    for (int d = 0; d <= maxd; ++d)
+        for (int l = -1; l <= 1; ++l) ns[{d, l}] = derivative_ns(mra, T, d, l);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (size_t q = 0; q < out.nodes.size(); ++q) {
+        Node& o = out.nodes[q];
+        std::vector<double> blk(BS), t1(BS), sin(SS), u1(SS);
+        const long long ext = (long long)mra.boxes[dir] << o.depth;
+        for (int l = -1; l <= 1; ++l) {
+            int64_t ti[3] = {o.t[0], o.t[1], o.t[2]};
+            ti[dir] -= l;
+            if (ti[dir] < 0 || ti[dir] >= ext) continue;
+            block_at(inp, o.depth, ti, blk.data());
+            const std::vector<double>& M = ns[{o.depth, l}];
+            mode_product(M.data(), K2, K2, K2, dir, blk.data(), K2, K2, K2, t1.data());
+            for (size_t i = 0; i < BS; ++i) o.c[i] += t1[i];
+            if (o.depth > 0) {  // remove the scaling->scaling block
+                for (int z = 0; z < k; ++z)
+                    for (int y = 0; y < k; ++y)
+                        for (int x = 0; x < k; ++x) sin[x + k * (y + k * z)] = blk[x + K2 * (y + K2 * z)];
+                mode_product(M.data(), K2, k, k, dir, sin.data(), k, k, k, u1.data());
+                for (int z = 0; z < k; ++z)
+                    for (int y = 0; y < k; ++y)
+                        for (int x = 0; x < k; ++x) o.c[x + K2 * (y + K2 * z)] -= u1[x + k * (y + k * z)];
+            }
+        }
+    }
+    // sum-up top-down, then compression
+    std::vector<double> rec(BS);
+    for (int i : out.level_order()) {
+        Node& nd = out.nodes[i];
+        if (nd.child0 < 0) continue;
+        transform3(mra.basis.F, k, true, nd.c.data(), rec.data());
+        for (int c = 0; c < 8; ++c) {
+            Node& ch = out.nodes[nd.child0 + c];
+            int cx = c & 1, cy = (c >> 1) & 1, cz = (c >> 2) & 1;
+            for (int z = 0; z < k; ++z)
+                for (int y = 0; y < k; ++y)
+                    for (int x = 0; x < k; ++x)
+                        ch.c[x + K2 * (y + K2 * z)] += rec[(cx * k + x) + K2 * ((cy * k + y) + K2 * (cz * k + z))];
+        }
+    }
+    compress_bottom_up(out);
+}
+
 // out = sum_i c_i f_i (mrcpp::add(prec, out, vec[, maxIter]) contract: reference
 // src/qmfunctions/qmfunction_utils.cpp:170-177, src/qmfunctions/density_utils.cpp:87,
 // src/mrdft/XCFunctional.cpp:713, src/scf_solver/KAIN.cpp:180,192).  Compressed blocks are linear in
@@ -1529,6 +1675,11 @@ int oracle_add(double prec, void* out, int n, const double* c, void* const* f, i
     std::vector<const Tree*> fv;
     for (int i = 0; i < n; ++i) fv.push_back((const Tree*)f[i]);
     add(prec, *(Tree*)out, cv, fv, max_iter);
+    return (int)((Tree*)out)->nodes.size();
+}
+// out = d/dx_dir inp on the input's grid (ABGV first derivative, flux parameters a, b)
+int oracle_derivative(void* out, void* inp, double a, double b, int dir) {
+    derivative_apply(*(Tree*)out, *(Tree*)inp, a, b, dir);
     return (int)((Tree*)out)->nodes.size();
 }
 // union of grids (mrcpp::build_grid contract); returns the number of nodes of `out`

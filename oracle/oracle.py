@@ -64,6 +64,7 @@ def lib():
         L.oracle_apply.argtypes = [ctypes.c_double, _vp, _vp, _vp, _lp]
         L.oracle_multiply.argtypes = [ctypes.c_double, _vp, ctypes.c_double, _vp, _vp, ctypes.c_int]
         L.oracle_build_grid.argtypes = [_vp, _vp]
+        L.oracle_derivative.argtypes = [_vp, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_int]
         L.oracle_add.argtypes = [ctypes.c_double, _vp, ctypes.c_int, _dp, ctypes.POINTER(_vp), ctypes.c_int]
         _lib = L
     return _lib
@@ -256,3 +257,8 @@ def add(prec, out: FunctionTree, coefs, trees, max_iter=-1):
     c = np.ascontiguousarray(coefs, dtype=np.float64)
     arr = (_vp * n)(*[t._h for t in trees])
     return lib().oracle_add(float(prec), out._h, n, _d(c), arr, int(max_iter))
+
+
+def derivative(out: FunctionTree, inp: FunctionTree, a, b, direction):
+    """out = d/dx_dir inp on the input's grid (ABGV derivative, mrcpp::apply(out, D, inp, dir) contract)"""
+    return lib().oracle_derivative(out._h, inp._h, float(a), float(b), int(direction))

@@ -61,5 +61,11 @@ int main() {
     mrcpp::FunctionTree<3> arg(MRA);
     mrcpp::add(prec, arg, 1.0, out, -2.0, phi);
     std::printf("sum nodes %d norm2 %.15e dot %.15e\n", arg.getNNodes(), arg.getSquareNorm(), mrcpp::dot(arg, phi));
+
+    // QMNabla::apply: ABGVOperator<3>(MRA, 0.5, 0.5) along y (SCFDriver.cpp:283, NablaOperator.cpp:35)
+    mrcpp::ABGVOperator<3> D(MRA, 0.5, 0.5);
+    mrcpp::FunctionTree<3> dphi(MRA);
+    mrcpp::apply(dphi, D, phi, 1);
+    std::printf("derivative nodes %d norm2 %.15e dot %.15e\n", dphi.getNNodes(), dphi.getSquareNorm(), mrcpp::dot(dphi, phi));
     return 0;
 }

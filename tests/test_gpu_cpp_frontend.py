@@ -46,7 +46,10 @@ def test_cpp_frontend_matches_python(gpu_mod, tmp_path):
     G.square(prec, rho, phi)
     arg = G.FunctionTree(m)
     G.add(prec, arg, [1.0, -2.0], [out_h, phi])
-    for key, t in (("helmholtz", out_h), ("poisson", V), ("exchange", V_ip), ("density", rho), ("sum", arg)):
+    dphi = G.FunctionTree(m)
+    G.apply_derivative(dphi, G.ABGVOperator(m, 0.5, 0.5), phi, 1)
+    for key, t in (("helmholtz", out_h), ("poisson", V), ("exchange", V_ip), ("density", rho), ("sum", arg),
+                   ("derivative", dphi)):
         n, n2, d = vals[key]
         assert n == t.nnodes()
         assert abs(n2 - t.square_norm()) <= 1e-12 * t.square_norm()
