@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <memory>
+#include <string>
 #include <tuple>
 #include <vector>
 
@@ -126,6 +127,9 @@ public:
     void rescale(double c) { detail::check(mw_tree_rescale(h_, c), "rescale"); }
     const MultiResolutionAnalysis<3>& getMRA() const { return *mra_; }
     mw_tree handle() const { return h_; }
+    // checkpoint files (reference src/qmfunctions/Orbital.cpp:128,170)
+    void saveTree(const std::string& file) { detail::check(mw_tree_save(h_, file.c_str()), "saveTree"); }
+    void loadTree(const std::string& file) { detail::check(mw_tree_load(h_, file.c_str()), "loadTree"); }
 
 private:
     const MultiResolutionAnalysis<3>* mra_;

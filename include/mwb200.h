@@ -81,6 +81,18 @@ int mw_tree_upload(mw_tree tree, int n, const int* depth, const long long* trans
 int mw_tree_download(mw_tree tree, int* depth, long long* trans, int* parent, int* child0, double* coef);
 /* device pointers of the node arrays (coef: n*(2k)^3 doubles, key: n uint64, norm2: n doubles) */
 int mw_tree_device_arrays(mw_tree tree, void** coef, void** key, void** norm2);
+/* Flat byte image of a tree: a 64-byte header (magic "MWB2TREE", format version, k, basis type, root
+ * scale, corner[3], boxes[3], node count) then int64 trans[3n], float64 coef[n (2k)^3], int32 depth[n],
+ * parent[n], child0[n] in the layout above; it is the checkpoint file of mw_tree_save and the payload
+ * a caller sends between processes.  Replaces FunctionTree::saveTree / loadTree (reference
+ * src/qmfunctions/Orbital.cpp:118-190) and the payload of mrcpp::send_tree / recv_tree
+ * (src/parallel.cpp:208-232).  Deserializing checks that the image was written on the same world and
+ * basis. */
+int mw_tree_serialized_size(mw_tree tree, unsigned long long* bytes);
+int mw_tree_serialize(mw_tree tree, void* buf, unsigned long long cap);
+int mw_tree_deserialize(mw_tree tree, const void* buf, unsigned long long len);
+int mw_tree_save(mw_tree tree, const char* path);
+int mw_tree_load(mw_tree tree, const char* path);
 /* rescale(c): reference src/scf_solver/HelmholtzVector.cpp:81 (out[i].rescale(-1/2pi)) */
 int mw_tree_rescale(mw_tree tree, double c);
 

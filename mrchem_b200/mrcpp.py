@@ -62,6 +62,11 @@ SYMBOLS = [
     ("mw_tree_download", ctypes.c_int, [_vp, _ip, _lp, _ip, _ip, _dp]),
     ("mw_tree_device_arrays", ctypes.c_int, [_vp, _vpp, _vpp, _vpp]),
     ("mw_tree_rescale", ctypes.c_int, [_vp, ctypes.c_double]),
+    ("mw_tree_serialized_size", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_ulonglong)]),
+    ("mw_tree_serialize", ctypes.c_int, [_vp, _vp, ctypes.c_ulonglong]),
+    ("mw_tree_deserialize", ctypes.c_int, [_vp, _vp, ctypes.c_ulonglong]),
+    ("mw_tree_save", ctypes.c_int, [_vp, ctypes.c_char_p]),
+    ("mw_tree_load", ctypes.c_int, [_vp, ctypes.c_char_p]),
     ("mw_project", ctypes.c_int, [ctypes.c_double, _vp, ctypes.c_int, ctypes.c_int, _dp]),
     ("mw_dot", ctypes.c_int, [_vp, _vp, _dp]),
     ("mw_nalloc_dot", ctypes.c_int, [_vp, _vp, _dp]),
@@ -250,6 +255,27 @@ class FunctionTree:
                                      parent.ctypes.data_as(_ip), child0.ctypes.data_as(_ip),
                                      _d(coef) if with_coefs else None))
         return dict(depth=depth, trans=trans, parent=parent, child0=child0, coef=coef)
+
+    def serialize(self):
+        """flat byte image of the tree (numpy uint8): checkpoint / message payload"""
+        n = ctypes.c_ulonglong()
+        _check(_lib.mw_tree_serialized_size(self._h, ctypes.byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        _check(_lib.mw_tree_serialize(self._h, buf.ctypes.data_as(ctypes.c_void_p), n.value))
+        return buf
+
+    def deserialize(self, buf):
+        """replace the tree by a byte image written on the same world and basis"""
+        b = np.ascontiguousarray(buf, dtype=np.uint8)
+        _check(_lib.mw_tree_deserialize(self._h, b.ctypes.data_as(ctypes.c_void_p), b.size))
+
+    def save_tree(self, path):
+        """FunctionTree::saveTree (reference src/qmfunctions/Orbital.cpp:128)"""
+        _check(_lib.mw_tree_save(self._h, os.fsencode(path)))
+
+    def load_tree(self, path):
+        """FunctionTree::loadTree (reference src/qmfunctions/Orbital.cpp:170)"""
+        _check(_lib.mw_tree_load(self._h, os.fsencode(path)))
 
     def export_into(self, bufs):
         """Download into caller-owned arrays (e.g. pinned host memory reused across calls): `bufs` has

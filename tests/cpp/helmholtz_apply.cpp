@@ -5,6 +5,7 @@
 // and run on the GPU through libmwb200.so.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 
 #include "mrcpp_b200.h"
 
@@ -67,5 +68,14 @@ int main() {
     mrcpp::FunctionTree<3> dphi(MRA);
     mrcpp::apply(dphi, D, phi, 1);
     std::printf("derivative nodes %d norm2 %.15e dot %.15e\n", dphi.getNNodes(), dphi.getSquareNorm(), mrcpp::dot(dphi, phi));
+
+    // Orbital::saveOrbital / loadOrbital (Orbital.cpp:128,170): checkpoint round trip
+    const char* ckpt = std::getenv("MWB200_CKPT");
+    if (ckpt) {
+        out.saveTree(ckpt);
+        mrcpp::FunctionTree<3> back(MRA);
+        back.loadTree(ckpt);
+        std::printf("checkpoint nodes %d norm2 %.15e dot %.15e\n", back.getNNodes(), back.getSquareNorm(), mrcpp::dot(back, phi));
+    }
     return 0;
 }

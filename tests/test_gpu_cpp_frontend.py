@@ -19,7 +19,8 @@ def test_cpp_frontend_matches_python(gpu_mod, tmp_path):
     subprocess.check_call(["g++", "-std=c++17", "-O2", "-I" + os.path.join(ROOT, "include"),
                            os.path.join(ROOT, "tests", "cpp", "helmholtz_apply.cpp"), "-L" + libdir, "-lmwb200",
                            "-Wl,-rpath," + libdir, "-o", str(exe)])
-    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    env = dict(os.environ, MWB200_CKPT=str(tmp_path / "out_h.tree"))
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True, env=env).stdout
     vals = {}
     for line in out.splitlines():
         m = re.match(r"(\w+) nodes (\d+) norm2 (\S+) dot (\S+)", line)
@@ -49,7 +50,7 @@ def test_cpp_frontend_matches_python(gpu_mod, tmp_path):
     dphi = G.FunctionTree(m)
     G.apply_derivative(dphi, G.ABGVOperator(m, 0.5, 0.5), phi, 1)
     for key, t in (("helmholtz", out_h), ("poisson", V), ("exchange", V_ip), ("density", rho), ("sum", arg),
-                   ("derivative", dphi)):
+                   ("derivative", dphi), ("checkpoint", out_h)):
         n, n2, d = vals[key]
         assert n == t.nnodes()
         assert abs(n2 - t.square_norm()) <= 1e-12 * t.square_norm()
