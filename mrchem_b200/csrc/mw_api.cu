@@ -205,6 +205,8 @@ Op::~Op() {
         dfree(c, kv.second->d_matsT32);
         dfree(c, kv.second->d_matsbT);
         dfree(c, kv.second->d_matsbT32);
+        dfree(c, kv.second->d_matsI);
+        dfree(c, kv.second->d_matsbI);
         dfree(c, kv.second->d_deltas);
         dfree(c, kv.second->d_terms);
     }
@@ -472,6 +474,32 @@ static const OpDepth& op_depth(Op& op, int depth, int dir = 0) {
     od->d_matsT32 = (float*)dalloc(ctx, sizeof(float) * std::max<size_t>(1, mT.size()));
     od->d_matsbT = (double*)dalloc(ctx, sizeof(double) * std::max<size_t>(1, mT.size()));
     od->d_matsbT32 = (float*)dalloc(ctx, sizeof(float) * std::max<size_t>(1, mT.size()));
+    // split-TF32 images: three TF32 pieces per entry (hi, mid, lo: each the TF32 rounding of what the
+    // previous pieces leave of the FP64 value)
+    const int KP8 = (K2 + 7) / 8 * 8;
+    const size_t isz = (size_t)3 * KP8 * KP8;
+    std::vector<float> mI(nmat * isz, 0.0f), mbI(nmat * isz, 0.0f);
+    auto put3 = [&](std::vector<float>& img, size_t mi, int o, int k, double v) {
+        const size_t w = mi * isz + (size_t)(o + 3 * KP8 * (k / 4)) * 4 + k % 4;  // row o of the hi block
+        const float h = tf32_round((float)v);
+        const float md = tf32_round((float)(v - (double)h));
+        const float l = tf32_round((float)(v - (double)h - (double)md));
+        img[w] = h;
+        img[w + 4 * (size_t)KP8] = md;  // row KP8 + o
+        img[w + 8 * (size_t)KP8] = l;   // row 2 KP8 + o
+    };
+    for (size_t mi = 0; mi < nmat; ++mi)
+        for (int o = 0; o < K2; ++o)
+            for (int k = 0; k < K2; ++k) {
+                put3(mI, mi, o, k, od->mats[mi * K2 * K2 + (size_t)o * K2 + k]);
+                put3(mbI, mi, o, k, mb[mi * K2 * K2 + (size_t)o * K2 + k]);
+            }
+    od->d_matsI = (float*)dalloc(ctx, sizeof(float) * std::max<size_t>(1, mI.size()));
+    od->d_matsbI = (float*)dalloc(ctx, sizeof(float) * std::max<size_t>(1, mI.size()));
+    if (!mI.empty()) {
+        MWB_CUDA(cudaMemcpyAsync(od->d_matsI, mI.data(), sizeof(float) * mI.size(), cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(od->d_matsbI, mbI.data(), sizeof(float) * mbI.size(), cudaMemcpyHostToDevice, s));
+    }
     if (!mT.empty()) {
         MWB_CUDA(cudaMemcpyAsync(od->d_matsT, mT.data(), sizeof(double) * mT.size(), cudaMemcpyHostToDevice, s));
         MWB_CUDA(cudaMemcpyAsync(od->d_matsT32, mT32.data(), sizeof(float) * mT.size(), cudaMemcpyHostToDevice, s));
@@ -1413,7 +1441,7 @@ int mw_op_create_abgv(mw_mra m, double a, double b, mw_op* out) {
 int mw_apply_derivative(mw_tree out, mw_op op, mw_tree inp, int dir, int flags) {
     MW_TRY({
         MW_ARG(out && op && inp, "null pointer");
-        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32, "unknown apply flags");
+        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3, "unknown apply flags");
         MWB_CUDA(cudaSetDevice(inp->mra->ctx->device));
         apply_derivative(out, op, inp, dir, flags);
     })
@@ -1445,7 +1473,7 @@ int mw_op_terms(mw_op op, double* alpha, double* beta) {
 int mw_apply(double prec, mw_tree out, mw_op op, mw_tree inp, int flags) {
     MW_TRY({
         MW_ARG(out && op && inp, "null pointer");
-        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32, "unknown apply flags");
+        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3, "unknown apply flags");
         MWB_CUDA(cudaSetDevice(inp->mra->ctx->device));
         Tree* o = out;
         Op* p = op;
@@ -1457,7 +1485,7 @@ int mw_apply(double prec, mw_tree out, mw_op op, mw_tree inp, int flags) {
 int mw_apply_batched(int n, double prec, mw_tree* out, mw_op* ops, mw_tree* inp, int flags) {
     MW_TRY({
         MW_ARG(n > 0 && out && ops && inp, "null pointer or empty batch");
-        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32, "unknown apply flags");
+        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3, "unknown apply flags");
         MW_ARG(inp[0], "null input tree");
         MWB_CUDA(cudaSetDevice(inp[0]->mra->ctx->device));
         std::vector<Tree*> o(n), i(n);
@@ -1603,7 +1631,7 @@ int mw_apply_learned(int n, double prec, mw_tree* out, mw_op* ops, mw_tree* inp,
                      long long* stats) {
     MW_TRY({
         MW_ARG(n > 0 && out && ops && inp && mlp, "null pointer or empty batch");
-        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32, "unknown apply flags");
+        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3, "unknown apply flags");
         MW_ARG(tau > 0.0f && tau < 1.0f, "tau must be in (0, 1)");
         MW_ARG(inp[0], "null input tree");
         MWB_CUDA(cudaSetDevice(inp[0]->mra->ctx->device));

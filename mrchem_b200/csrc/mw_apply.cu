@@ -23,6 +23,7 @@
 #include "mw_device.cuh"
 #include "mw_kernels.cuh"
 #include "mw_tmem.cuh"
+#include "mw_umma.cuh"
 
 namespace mwb {
 
@@ -45,6 +46,8 @@ struct BTree {
     const float* matsT32;
     const double* matsbT;
     const float* matsbT32;
+    const float* matsI;  // split-TF32 operator images (tensor-core contraction)
+    const float* matsbI;
     int nprefix;
     int root;
     double theta;
@@ -1020,6 +1023,10 @@ __global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
     }
 }
 
+}  // namespace mwb
+#include "mw_tapply.cuh"
+namespace mwb {
+
 // add the partial blocks of a multi-chunk node in chunk order; write block and norms
 template <int K>
 __global__ void __launch_bounds__(256) k_breduce(const Chunk* __restrict__ chunks, const int* __restrict__ choff,
@@ -1169,6 +1176,8 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         d.matsT32 = b.tab->d_matsT32;
         d.matsbT = b.tab->d_matsbT;
         d.matsbT32 = b.tab->d_matsbT32;
+        d.matsI = b.tab->d_matsI;
+        d.matsbI = b.tab->d_matsbI;
         d.nprefix = b.nprefix;
         d.root = b.depth == 0;
         d.theta = b.theta;
@@ -1282,13 +1291,19 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     double* d_partials = (double*)dalloc(ctx, sizeof(double) * BS * std::max(1, nslots));
 
     // 5. contraction + reduction of multi-chunk nodes
-    unsigned long long* d_ntrip_tot = (unsigned long long*)dalloc(ctx, sizeof(unsigned long long));
-    MWB_CUDA(cudaMemsetAsync(d_ntrip_tot, 0, sizeof(unsigned long long), s));
+    unsigned long long* d_ntrip_tot = (unsigned long long*)dalloc(ctx, 2 * sizeof(unsigned long long));
+    int* d_kerr = reinterpret_cast<int*>(d_ntrip_tot + 1);  // set by the tensor-core kernel on a wait timeout
+    MWB_CUDA(cudaMemsetAsync(d_ntrip_tot, 0, 2 * sizeof(unsigned long long), s));
     if (ctx->prof) MWB_CUDA(cudaEventRecord(ctx->ev0, s));
     const bool pencil = contraction_pencil();
 #define L_AP(KK)                                                                                             \
     {                                                                                                        \
-        if (bp.precision == 1 && GCfg<KK, float>::FITS && !pencil) {                                          \
+        if (bp.precision == 2 && TCfg<KK>::FITS && !pencil) {                                                \
+            size_t smem = TCfg<KK>::SMEM;                                                                    \
+            MWB_CUDA(cudaFuncSetAttribute(k_tapply<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+            k_tapply<KK><<<nchunks, TCfg<KK>::NTHR, smem, s>>>(d_chunks, d_items, d_trees, d_cdelta, d_csrc,     \
+                                                               d_gblk, d_gnorm2, d_partials, d_ntrip_tot, d_kerr); \
+        } else if (bp.precision >= 1 && GCfg<KK, float>::FITS && !pencil) {                                  \
             size_t smem = GCfg<KK, float>::SMEM;                                                             \
             MWB_CUDA(cudaFuncSetAttribute(k_gapply<KK, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
             k_gapply<KK, float><<<nchunks, GCfg<KK, float>::NTHR, smem, s>>>(d_chunks, d_items, d_trees, d_cdelta, \
@@ -1300,7 +1315,7 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
             k_gapply<KK, double><<<nchunks, GCfg<KK, double>::NTHR, smem, s>>>(d_chunks, d_items, d_trees, d_cdelta, \
                                                                                 d_csrc, d_gblk, d_gnorm2, d_partials, \
                                                                                 d_ntrip_tot);                       \
-        } else if (bp.precision == 1) {                                                                      \
+        } else if (bp.precision >= 1) {                                                                      \
             size_t smem = ACfg<KK, float>::SMEM;                                                             \
             MWB_CUDA(cudaFuncSetAttribute(k_bapply<KK, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
             k_bapply<KK, float><<<nchunks, ACfg<KK, float>::NT, smem, s>>>(d_chunks, d_items, d_trees, d_cdelta,  \
@@ -1338,15 +1353,17 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         dfree(ctx, d_mpos);
         dfree(ctx, d_mlist);
     }
-    unsigned long long ntot = 0;
-    MWB_CUDA(cudaMemcpyAsync(&ntot, d_ntrip_tot, sizeof(ntot), cudaMemcpyDeviceToHost, s));
+    unsigned long long ntot[2] = {0, 0};
+    MWB_CUDA(cudaMemcpyAsync(ntot, d_ntrip_tot, sizeof(ntot), cudaMemcpyDeviceToHost, s));
     MWB_CUDA(cudaStreamSynchronize(s));
+    if ((ntot[1] & 0xffffffffull) != 0)
+        throw Error(-2, "tensor-core contraction: an MMA completion wait exceeded its time limit");
     if (ctx->prof) {
         float ms = 0.0f;
         MWB_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
         ctx->apply_ms += ms;
     }
-    bp.triples = (long long)ntot;
+    bp.triples = (long long)ntot[0];
 
     // 6. root norms (g0 per root entry), then split lists per entry
     bool any_root = false;

@@ -91,6 +91,12 @@ struct OpDepth {
     float* d_matsT32 = nullptr;
     double* d_matsbT = nullptr;
     float* d_matsbT32 = nullptr;
+    // split-TF32 operator images for the tensor-core contraction: per matrix one K-major FP32 image of
+    // 3 KP8 rows and KP8 columns (KP8 = 2k rounded up to a multiple of 8, zero padding): rows o,
+    // KP8 + o, 2 KP8 + o = hi, mid, lo TF32 pieces of M[o][.]; entry (row n, k) at word
+    // 4 (n + 3 KP8 (k / 4)) + k % 4; plain and beta-scaled
+    float* d_matsI = nullptr;
+    float* d_matsbI = nullptr;
     DeltaRec* d_deltas = nullptr;
     TermRec* d_terms = nullptr;
 };

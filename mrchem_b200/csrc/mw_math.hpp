@@ -16,6 +16,18 @@
 
 namespace mwb {
 
+// FP32 -> TF32 (10 explicit mantissa bits) rounded to nearest with ties away from zero, the rounding
+// of the device's TF32 split; infinities and NaNs pass unchanged
+inline float tf32_round(float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+    float r;
+    std::memcpy(&r, &u, 4);
+    return r;
+}
+
+
 constexpr double kPi = 3.14159265358979323846;
 
 // Gauss-Legendre rule on [0,1], ascending nodes.
