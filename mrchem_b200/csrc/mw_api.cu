@@ -1005,6 +1005,35 @@ struct mw_tree_s : Tree {};
 struct mw_op_s : Op {};
 struct mw_mlp_s : Mlp {};
 
+// Handle lifetimes: a context or world destroyed while handles still point to it is freed when the
+// last of them goes, so the C-ABI's destroy calls may come in any order (e.g. from a garbage collector
+// finalising a reference cycle).
+static void ctx_free(mwb::Ctx* ctx) {
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    delete static_cast<mw_ctx_s*>(ctx);
+}
+static void ctx_release(mwb::Ctx* ctx) {
+    if (--ctx->refs == 0 && ctx->closed) ctx_free(ctx);
+}
+static void mra_free(mwb::Mra* m) {
+    mwb::Ctx* c = m->ctx;
+    cudaSetDevice(c->device);
+    mwb::dfree(c, m->d_F);
+    mwb::dfree(c, m->d_FT);
+    mwb::dfree(c, m->d_PF);
+    mwb::dfree(c, m->d_MV);
+    cudaStreamSynchronize(c->stream);
+    delete static_cast<mw_mra_s*>(m);
+    ctx_release(c);
+}
+static void mra_release(mwb::Mra* m) {
+    if (--m->refs == 0 && m->closed) mra_free(m);
+}
+
 #define MW_TRY(...)                                        \
     try {                                                  \
         __VA_ARGS__;                                       \
@@ -1104,12 +1133,9 @@ int mw_ctx_profile_read(mw_ctx ctx, long long* launches, long long* apply_launch
 int mw_ctx_destroy(mw_ctx ctx) {
     MW_TRY({
         if (!ctx) return MW_OK;
-        cudaSetDevice(ctx->device);
-        cudaStreamSynchronize(ctx->stream);
-        if (ctx->ev0) cudaEventDestroy(ctx->ev0);
-        if (ctx->ev1) cudaEventDestroy(ctx->ev1);
-        if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
-        delete ctx;
+        MW_ARG(!ctx->closed, "context destroyed twice");
+        ctx->closed = true;
+        if (ctx->refs == 0) ctx_free(ctx);
     })
 }
 
@@ -1184,6 +1210,7 @@ int mw_mra_create(mw_ctx ctx, int min_scale, const int* corner, const int* boxes
         MWB_CUDA(cudaMemcpyAsync(m->d_FT, FT.data(), sizeof(double) * K2 * K2, cudaMemcpyHostToDevice, s));
         MWB_CUDA(cudaMemcpyAsync(m->d_PF, PF.data(), sizeof(double) * K2 * K2, cudaMemcpyHostToDevice, s));
         MWB_CUDA(cudaStreamSynchronize(s));
+        ctx->refs++;
         *out = m;
     })
 }
@@ -1191,13 +1218,9 @@ int mw_mra_create(mw_ctx ctx, int min_scale, const int* corner, const int* boxes
 int mw_mra_destroy(mw_mra m) {
     MW_TRY({
         if (!m) return MW_OK;
-        cudaSetDevice(m->ctx->device);
-        dfree(m->ctx, m->d_F);
-        dfree(m->ctx, m->d_FT);
-        dfree(m->ctx, m->d_PF);
-        dfree(m->ctx, m->d_MV);
-        cudaStreamSynchronize(m->ctx->stream);
-        delete m;
+        MW_ARG(!m->closed, "world destroyed twice");
+        m->closed = true;
+        if (m->refs == 0) mra_free(m);
     })
 }
 
@@ -1221,13 +1244,17 @@ int mw_tree_create(mw_mra m, mw_tree* out) {
         MWB_CUDA(cudaSetDevice(m->ctx->device));
         auto* t = new mw_tree_s();
         t->mra = m;
+        m->refs++;
         *out = t;
     })
 }
 
 int mw_tree_destroy(mw_tree t) {
     MW_TRY({
-        if (t) delete t;
+        if (!t) return MW_OK;
+        Mra* m = t->mra;
+        delete t;
+        if (m) mra_release(m);
     })
 }
 
@@ -1403,6 +1430,7 @@ int mw_op_create_poisson(mw_mra m, double prec, mw_op* out) {
             delete op;
             throw;
         }
+        m->refs++;
         *out = op;
     })
 }
@@ -1419,6 +1447,7 @@ int mw_op_create_helmholtz(mw_mra m, double mu, double prec, mw_op* out) {
             delete op;
             throw;
         }
+        m->refs++;
         *out = op;
     })
 }
@@ -1434,6 +1463,7 @@ int mw_op_create_abgv(mw_mra m, double a, double b, mw_op* out) {
         op->da = a;
         op->db = b;
         derivative_blocks(m->basis, a, b, op->dT);
+        m->refs++;
         *out = op;
     })
 }
@@ -1449,7 +1479,10 @@ int mw_apply_derivative(mw_tree out, mw_op op, mw_tree inp, int dir, int flags) 
 
 int mw_op_destroy(mw_op op) {
     MW_TRY({
-        if (op) delete op;
+        if (!op) return MW_OK;
+        Mra* m = op->mra;
+        delete op;
+        if (m) mra_release(m);
     })
 }
 
@@ -1513,13 +1546,17 @@ int mw_mlp_create(mw_ctx ctx, int hidden_layers, int width, unsigned seed, mw_ml
         MWB_CUDA(cudaSetDevice(ctx->device));
         auto* M = new mw_mlp_s();
         mlp_init(*M, ctx, hidden_layers, width, seed);
+        ctx->refs++;
         *out = M;
     })
 }
 
 int mw_mlp_destroy(mw_mlp mlp) {
     MW_TRY({
-        if (mlp) delete mlp;
+        if (!mlp) return MW_OK;
+        Ctx* c = mlp->ctx;
+        delete mlp;
+        if (c) ctx_release(c);
     })
 }
 

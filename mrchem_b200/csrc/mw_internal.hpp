@@ -44,6 +44,9 @@ struct Ctx {
     long long apply_ctas = 0;  // CTAs (chunks) of those launches
     double apply_ms = 0.0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // handles that point here (worlds, networks); a destroyed context is freed with the last of them
+    int refs = 0;
+    bool closed = false;
 };
 
 struct Mra {
@@ -61,6 +64,9 @@ struct Mra {
     double* d_FT = nullptr;  // F^T
     double* d_PF = nullptr;  // projection matrix F * blkdiag(W, W)
     double* d_MV = nullptr;  // evaluation matrix blkdiag(E, E) * F^T (pointwise product)
+    // trees and operators that point here; a destroyed world is freed with the last of them
+    int refs = 0;
+    bool closed = false;
     size_t bsize() const { return (size_t)8 * k * k * k; }
 };
 
