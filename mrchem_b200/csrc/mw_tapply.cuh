@@ -38,7 +38,8 @@
 // Synchronisation per term: two mbarriers per step (the first half of the tiles, the rest), armed by
 // tcgen05.commit from the issuing thread and waited for by all threads with a time limit (a wait that
 // runs out sets the kernel's error word and every thread leaves through the same barriers), so that
-// the epilogue of the first tiles runs while the tensor core works on the others; every mbarrier
+// the epilogue of the first tiles runs while the tensor core works on the others (x and z steps; the
+// y epilogue writes over the y MMAs' own operand and waits for both); every mbarrier
 // completes once per term, so one phase bit serves all six.  A CTA barrier after each epilogue
 // publishes the new operand (fence.proxy.async) and orders the TMEM reads before the next MMAs
 // (tcgen05.fence::before_thread_sync / after_thread_sync).
@@ -415,12 +416,11 @@ __global__ void __launch_bounds__(256, 1)
             // ---- y
             if (tid == 0) issue(sth, stl, 1, C::T2, nks, &bars[2]);
             corr_y();
+            // the y epilogue overwrites the y MMAs' own operand (T) in place: all of them must be done
             if (!mbar_wait(&bars[2], ph, kWaitNs)) bad = 1;
-            tmem_fence_after_sync();
-            epi(std::integral_constant<int, S2>{}, 0, (C::T2 + 1) / 2, [](int ap, int bp) { return ap + S3 * bp; });
             if (!mbar_wait(&bars[3], ph, kWaitNs)) bad = 1;
             tmem_fence_after_sync();
-            epi(std::integral_constant<int, S2>{}, (C::T2 + 1) / 2, C::T2, [](int ap, int bp) { return ap + S3 * bp; });
+            epi(std::integral_constant<int, S2>{}, 0, C::T2, [](int ap, int bp) { return ap + S3 * bp; });
             tmem_fence_before_sync();
             cp_async_wait_all();
             fence_proxy_async_smem();
