@@ -233,10 +233,11 @@ def run_gpu(args):
 
     step_ms = []  # per timed region: device time of each step
 
-    def timed(run):
+    def timed(run, name):
         """W untimed + K timed steps of `run()` (returns the step's contracted triples).  The clock
         sampler starts before the warm-up steps, so that its start-up (NVML initialisation) is over
-        when the timed region begins."""
+        when the timed region begins.  The timed steps sit in an NVTX range `name` (a no-op unless a
+        profiler listens; `ncu --nvtx --nvtx-include name/` lists the launches of that region only)."""
         with Clocks(local) as clk:
             for _ in range(args.warmup):
                 run()
@@ -252,9 +253,11 @@ def run_gpu(args):
             trip = 0
             ev0.record(stream)
             evs[0].record(stream)
+            torch.cuda.nvtx.range_push(name)
             for q in range(args.steps):
                 trip += run()
                 evs[q + 1].record(stream)
+            torch.cuda.nvtx.range_pop()
             ev1.record(stream)
             torch.cuda.synchronize()
             clk.mark()
@@ -288,9 +291,9 @@ def run_gpu(args):
 
     # plain FP64 (the reference method on the GPU), the mixed path (FP32 products, FP64
     # accumulation) and mixed + learned proposal, same inputs, same operators
-    ms64, trip64, prof64, _ = timed(lambda: G.apply_batched(args.prec, outs, ops, inps, G.APPLY_FP64))
+    ms64, trip64, prof64, _ = timed(lambda: G.apply_batched(args.prec, outs, ops, inps, G.APPLY_FP64), "plain_fp64")
     outs32 = [G.FunctionTree(m) for _ in range(args.orbitals)]
-    ms32, trip32, prof32m, _ = timed(lambda: G.apply_batched(args.prec, outs32, ops, inps, G.APPLY_FP32))
+    ms32, trip32, prof32m, _ = timed(lambda: G.apply_batched(args.prec, outs32, ops, inps, G.APPLY_FP32), "mixed")
     outsL = [G.FunctionTree(m) for _ in range(args.orbitals)]
     lstats = {}
 
@@ -299,8 +302,12 @@ def run_gpu(args):
         lstats.update(st)
         return st["triples"]
 
-    ms, triples, prof32, clocks = timed(run_learned)
+    ms, triples, prof32, clocks = timed(run_learned, "mixed_learned")
     launches, apply_launches, apply_ms, apply_ctas = prof32
+    # the tensor-core contraction (split-TF32 on tcgen05) on the same batch, no learned proposal
+    outsT = [G.FunctionTree(m) for _ in range(args.orbitals)]
+    msT, tripT, profT, _ = timed(lambda: G.apply_batched(args.prec, outsT, ops, inps, G.APPLY_TF32X3), "tensor_core")
+    errT = [G.distance(a, b) / np.sqrt(b.square_norm()) for a, b in zip(outsT, outs)]
     # error of the mixed + learned result against the FP64 one: ||g - g64|| / ||g64|| per orbital
     # (from the coefficient differences, mw_tree_distance: no cancellation)
     rel_err = 0.0
@@ -394,7 +401,20 @@ def run_gpu(args):
                            "triples_per_step": trip64 // max(1, args.steps)},
             "mixed_no_learning": {"value": args.orbitals * args.steps * world / (ms32 / 1e3), "unit": "applies/s",
                                   "ms_per_step": ms32 / args.steps, "kernel_ms_per_step": prof32m[2] / args.steps},
-            "step_ms": {"plain_fp64": step_ms[0], "mixed_no_learning": step_ms[1], "mixed_learned": step_ms[2]},
+            "tensor_core_tf32x3": {
+                "value": args.orbitals * args.steps * world / (msT / 1e3), "unit": "applies/s",
+                "ms_per_step": msT / args.steps, "kernel": f"k_tapply<{m.k}>",
+                "kernel_ms_per_step": profT[2] / args.steps,
+                "achieved_tflops": (tripT * flops_per_triple(m.k) / (profT[2] / 1e3) / 1e12) if profT[2] > 0 else None,
+                "frac_of_measured_bf16_peak": ((tripT * flops_per_triple(m.k) / (profT[2] / 1e3) / 1e12)
+                                               / float(measured_peaks().get("bf16_tflops", 1590.0)))
+                if profT[2] > 0 else None,
+                "rel_error_vs_fp64_max": max(errT), "rel_error_vs_fp64_median": float(np.median(errT)),
+                "same_node_count_as_fp64": all(a.nnodes() == b.nnodes() for a, b in zip(outsT, outs)),
+                "products": "data 2 TF32 pieces x operators 3 pieces, 2 MMAs (N = 6k) per K step; "
+                            "compensated FP32-pair summation over terms"},
+            "step_ms": {"plain_fp64": step_ms[0], "mixed_no_learning": step_ms[1], "mixed_learned": step_ms[2],
+                        "tensor_core_tf32x3": step_ms[3]},
             "speedup_vs_plain_fp64": ms64 / ms,
             "rel_error_vs_fp64": rel_err,
             "rel_error_vs_fp64_mixed_no_learning": rel_err_mixed,
