@@ -665,10 +665,57 @@ struct GCfg {
 __device__ __forceinline__ float mfma(float a, float b, float c) { return fmaf(a, b, c); }
 __device__ __forceinline__ double mfma(double a, double b, double c) { return fma(a, b, c); }
 
+// packed FP32 pairs (sm_100 f32x2 arithmetic): two independent round-to-nearest FMAs per instruction,
+// bit-identical to two fmaf calls
+__device__ __forceinline__ unsigned long long fma_f32x2(unsigned long long a, unsigned long long b,
+                                                        unsigned long long c) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ unsigned long long pack_f32x2(float lo, float hi) {
+    unsigned long long d;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(lo), "f"(hi));
+    return d;
+}
+__device__ __forceinline__ void unpack_f32x2(unsigned long long v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+
 // c (+)= At^T B on a thread tile: c[i][j] (+)= sum_{k < kdim} At[k lda + o0 + i] B[k ldb + n0 + j]
 template <int MT, int NT, bool ACC, typename R, typename CT>
 __device__ __forceinline__ void gemm_tile(const R* __restrict__ At, int lda, const R* __restrict__ B, int ldb,
                                           int o0, int n0, int kdim, CT (&c)[MT][NT]) {
+    if constexpr (sizeof(R) == 4 && sizeof(CT) == 4 && NT % 2 == 0) {
+        // FP32 tile: column pairs in packed registers, one f32x2 FMA per pair and contracted index
+        constexpr int NP = NT / 2;
+        unsigned long long pc[MT][NP];
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NP; ++j) pc[i][j] = ACC ? pack_f32x2(c[i][2 * j], c[i][2 * j + 1]) : 0ull;
+        const R* ap = At + o0;
+        const R* bp = B + n0;
+#pragma unroll 2
+        for (int k = 0; k < kdim; ++k) {
+            unsigned long long a2[MT], b2[NP];
+#pragma unroll
+            for (int i = 0; i < MT; ++i) a2[i] = pack_f32x2(ap[i], ap[i]);
+#pragma unroll
+            for (int j = 0; j < NP; ++j) b2[j] = *reinterpret_cast<const unsigned long long*>(bp + 2 * j);
+#pragma unroll
+            for (int i = 0; i < MT; ++i)
+#pragma unroll
+                for (int j = 0; j < NP; ++j) pc[i][j] = fma_f32x2(a2[i], b2[j], pc[i][j]);
+            ap += lda;
+            bp += ldb;
+        }
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NP; ++j) unpack_f32x2(pc[i][j], c[i][2 * j], c[i][2 * j + 1]);
+        return;
+    }
     if (!ACC) {
 #pragma unroll
         for (int i = 0; i < MT; ++i)
