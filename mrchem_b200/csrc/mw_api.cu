@@ -824,90 +824,51 @@ static void apply_learned(double prec, int n, Tree** out, Op** op, Tree** inp, i
         trip += run_entries(prec, precision, ents, out, op, inp, fnorm, nu_max, g0);
         ++passes;
     }
-    // exact criterion on every computed node, top-down from the roots: nodes below a node the
-    // criterion does not split are dropped (they stay in the arrays until the final rebuild), splits
-    // without children are refined by further passes
-    std::vector<std::vector<char>> keeps(n);
-    std::vector<std::vector<uint64_t>> keys(n);
-    std::vector<long long> computed(n);
-    for (int i = 0; i < n; ++i) computed[i] = out[i]->n;
+    // exact criterion on every computed node (on the device): a node is kept when all its ancestors
+    // split; nodes below a node the criterion does not split are dropped at the final rebuild, kept
+    // splits without children (misses) are refined by further passes
+    std::vector<std::vector<double>> thr(n, std::vector<double>(64, INFINITY));
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 64; ++d) thr[i][d] = split_threshold(prec, g0[i], d);
+    unsigned char* d_keep = nullptr;
     for (;;) {
-        std::vector<std::vector<double>> w2(n);
-        std::vector<std::vector<int>> c0(n);
-        for (int i = 0; i < n; ++i) {
-            Tree& t = *out[i];
-            w2[i].resize(t.n);
-            c0[i].resize(t.n);
-            keys[i].resize(t.n);
-            MWB_CUDA(cudaMemcpyAsync(w2[i].data(), t.wnorm2, sizeof(double) * t.n, cudaMemcpyDeviceToHost, s));
-            MWB_CUDA(cudaMemcpyAsync(c0[i].data(), t.child0, sizeof(int) * t.n, cudaMemcpyDeviceToHost, s));
-            MWB_CUDA(cudaMemcpyAsync(keys[i].data(), t.key, sizeof(uint64_t) * t.n, cudaMemcpyDeviceToHost, s));
-        }
-        MWB_CUDA(cudaStreamSynchronize(s));
+        long long tot = 0;
+        for (int i = 0; i < n; ++i) tot += out[i]->n;
+        dfree(ctx, d_keep);
+        d_keep = (unsigned char*)dalloc(ctx, std::max<long long>(1, tot));
+        const std::vector<Miss> ms = verify_trees(all, thr, m->depth_limit, d_keep, s);
+        if (ms.empty()) break;
+        // per tree, in key order (depth-major): the appended children come out grouped by depth
+        std::vector<std::vector<std::pair<uint64_t, int>>> mk(n);
+        for (const Miss& q : ms) mk[q.tree].push_back({q.key, q.node});
         std::vector<std::vector<int>> lists(n);
-        std::vector<std::vector<uint64_t>> misses(n);
-        bool any = false;
         for (int i = 0; i < n; ++i) {
-            const Tree& t = *out[i];
-            keeps[i].assign(t.n, 0);
-            std::vector<int> stack;
-            for (int q = 0; q < t.level_begin[1]; ++q) stack.push_back(q);
-            while (!stack.empty()) {
-                const int q = stack.back();
-                stack.pop_back();
-                keeps[i][q] = 1;
-                const int d = (int)(keys[i][q] >> 59);
-                if (d < m->depth_limit && std::sqrt(w2[i][q]) > split_threshold(prec, g0[i], d)) {
-                    if (c0[i][q] >= 0)
-                        for (int c = 0; c < 8; ++c) stack.push_back(c0[i][q] + c);
-                    else
-                        lists[i].push_back(q);
-                }
-            }
-            // depth-major order: the appended children come out grouped by depth
-            std::sort(lists[i].begin(), lists[i].end(), [&](int a, int b) { return keys[i][a] < keys[i][b]; });
-            missed += (long long)lists[i].size();
-            any |= !lists[i].empty();
+            std::sort(mk[i].begin(), mk[i].end());
+            for (auto& kv : mk[i]) lists[i].push_back(kv.second);
         }
-        if (!any) break;
+        missed += (long long)ms.size();
         std::vector<int> base(n);
         for (int i = 0; i < n; ++i) base[i] = out[i]->n;
         add_children_many(all, lists);
         std::vector<Entry> next;
         for (int i = 0; i < n; ++i) {
             int b = base[i];
-            for (size_t q = 0; q < lists[i].size();) {
-                const int d = (int)(keys[i][lists[i][q]] >> 59) + 1;
+            for (size_t q = 0; q < mk[i].size();) {
+                const int d = (int)(mk[i][q].first >> 59) + 1;
                 size_t r = q;
-                while (r < lists[i].size() && (int)(keys[i][lists[i][r]] >> 59) + 1 == d) ++r;
+                while (r < mk[i].size() && (int)(mk[i][r].first >> 59) + 1 == d) ++r;
                 next.push_back(Entry{i, d, b, b + 8 * (int)(r - q)});
                 b += 8 * (int)(r - q);
                 q = r;
             }
-            computed[i] = out[i]->n;
         }
         trip += run_entries(prec, precision, next, out, op, inp, fnorm, nu_max, g0);
         ++passes;
     }
-    // one rebuild of every tree whose arrays hold dropped nodes or appended refinements
-    {
-        std::vector<Tree*> ts;
-        std::vector<std::vector<char>> kk;
-        std::vector<std::vector<uint64_t>> ky;
-        for (int i = 0; i < n; ++i) {
-            long long nk = 0;
-            for (char k : keeps[i]) nk += k;
-            pruned += computed[i] - nk;
-            const bool sorted_levels = nk == out[i]->n && (int)keys[i].size() == out[i]->n &&
-                                       std::is_sorted(keys[i].begin(), keys[i].end());
-            if (!sorted_levels) {
-                ts.push_back(out[i]);
-                kk.push_back(keeps[i]);
-                ky.push_back(keys[i]);
-            }
-        }
-        trees_rebuild(ts, kk, ky);
-    }
+    // one rebuild of every tree from its kept nodes, in key order (drops pruned nodes, puts the
+    // appended refinements in level order)
+    pruned += trees_rebuild_device(all, d_keep, s);
+    dfree(ctx, d_keep);
     trees_finish(std::vector<Tree*>(out, out + n), true, true, true, s);
     for (int i = 0; i < n; ++i) {
         out[i]->g0 = g0[i];

@@ -12,6 +12,7 @@
 // and nodes the criterion splits but the network did not are refined with further passes.  The
 // result is the plain apply's tree (node keys and coefficients) exactly.
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include <algorithm>
 #include <cmath>
@@ -517,6 +518,315 @@ double mlp_train(Mlp& M, int epochs, int batch, float lr, unsigned seed) {
     MWB_CUDA(cudaStreamSynchronize(s));
     for (void* q : {(void*)d_w, (void*)d_bx, (void*)d_by, (void*)d_bw, (void*)d_idx}) dfree(ctx, q);
     return last;
+}
+
+}  // namespace mwb
+
+namespace mwb {
+
+// ---------------------------------------------------------------------------------------------
+// exact criterion and rebuild on the device
+// ---------------------------------------------------------------------------------------------
+namespace {
+constexpr int kMaxLevels = 64;
+
+struct VTree {
+    const uint64_t* key;
+    const int* parent;
+    const int* child0;
+    const double* wnorm2;
+    int n;
+    long long off;
+};
+
+// one thread per node of tree blockIdx.y: keep = all strict ancestors split; a kept node that splits
+// without children is appended to the miss list
+__global__ void k_verify(const VTree* __restrict__ ts, const double* __restrict__ thr, int depth_limit,
+                         unsigned char* keep, int* nmiss, Miss* miss, int cap) {
+    const VTree T = ts[blockIdx.y];
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= T.n) return;
+    const double* th = thr + (size_t)blockIdx.y * kMaxLevels;
+    auto splits = [&](int p) {
+        const int d = key_depth(T.key[p]);
+        return d < depth_limit && sqrt(T.wnorm2[p]) > th[d];
+    };
+    unsigned char k = 1;
+    for (int p = T.parent[q]; p >= 0; p = T.parent[p])
+        if (!splits(p)) {
+            k = 0;
+            break;
+        }
+    keep[T.off + q] = k;
+    if (k && T.child0[q] < 0 && splits(q)) {
+        const int w = atomicAdd(nmiss, 1);
+        if (w < cap) miss[w] = Miss{(int)blockIdx.y, q, T.key[q]};
+    }
+}
+
+struct RTree {  // old arrays, new arrays and hash index of one tree being rebuilt
+    const uint64_t* okey;
+    const double* ocoef;
+    const double* on2;
+    const double* ow2;
+    uint64_t* nkey;
+    double* ncoef;
+    double* nn2;
+    double* nw2;
+    int* nparent;
+    int* nchild0;
+    const uint64_t* hkey;
+    const int* hval;
+    uint32_t hcap;
+    long long off;   // first global index of the tree's old nodes
+    long long noff;  // first position of the tree's kept nodes in the sorted list
+    int nn;
+};
+
+__global__ void k_gather_keys(const uint64_t* __restrict__ k, const long long* __restrict__ g, int n, uint64_t* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = k[g[i]];
+}
+
+// tree of each kept node (largest tree whose first global index is <= g[i]); kept nodes per tree
+__global__ void k_tree_of(const long long* __restrict__ g, int n, const long long* __restrict__ offs, int nt,
+                          unsigned* tid, int* cnt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int lo = 0, hi = nt - 1;  // last tree whose offset <= g[i]
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (offs[mid] <= g[i]) lo = mid;
+        else hi = mid - 1;
+    }
+    tid[i] = (unsigned)lo;
+    atomicAdd(&cnt[lo], 1);
+}
+
+// block j: kept node j of the sorted list (tree tid[j]) -> its new position
+__global__ void k_rebuild_gather(const long long* __restrict__ g, const unsigned* __restrict__ tid, int n,
+                                 const RTree* __restrict__ rt, size_t bs) {
+    const int j = blockIdx.x;
+    if (j >= n) return;
+    const RTree& R = rt[tid[j]];
+    const long long o = g[j] - R.off;
+    const long long d = j - R.noff;
+    const double* src = R.ocoef + (size_t)o * bs;
+    double* dst = R.ncoef + (size_t)d * bs;
+    for (size_t e = threadIdx.x; e < bs; e += blockDim.x) dst[e] = src[e];
+    if (threadIdx.x == 0) {
+        R.nkey[d] = R.okey[o];
+        R.nn2[d] = R.on2[o];
+        R.nw2[d] = R.ow2[o];
+    }
+}
+
+// parent and first child of every new node from the rebuilt hash index; level starts per tree
+__global__ void k_rebuild_links(const unsigned* __restrict__ tid, int n, const RTree* __restrict__ rt, int* lb) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const unsigned t = tid[j];
+    const RTree& R = rt[t];
+    const int d = (int)(j - R.noff);
+    const uint64_t k = R.nkey[d];
+    const int dep = key_depth(k);
+    long long tr[3];
+    key_trans(k, tr);
+    R.nparent[d] = dep > 0 ? hlookup(R.hkey, R.hval, R.hcap, make_key(dep - 1, tr[0] >> 1, tr[1] >> 1, tr[2] >> 1)) : -1;
+    R.nchild0[d] = hlookup(R.hkey, R.hval, R.hcap, make_key(dep + 1, 2 * tr[0], 2 * tr[1], 2 * tr[2]));
+    if (d == 0 || key_depth(R.nkey[d - 1]) != dep) lb[(size_t)t * (kMaxLevels + 1) + dep] = d;
+}
+}  // namespace
+
+std::vector<Miss> verify_trees(const std::vector<Tree*>& ts, const std::vector<std::vector<double>>& thr,
+                               int depth_limit, unsigned char* d_keep, cudaStream_t s) {
+    const int nt = (int)ts.size();
+    if (nt == 0) return {};
+    Ctx* ctx = ts[0]->mra->ctx;
+    std::vector<VTree> vt(nt);
+    std::vector<double> th((size_t)nt * kMaxLevels, INFINITY);
+    long long off = 0;
+    int maxn = 0;
+    for (int i = 0; i < nt; ++i) {
+        const Tree& t = *ts[i];
+        vt[i] = VTree{t.key, t.parent, t.child0, t.wnorm2, t.n, off};
+        off += t.n;
+        maxn = std::max(maxn, t.n);
+        for (int d = 0; d < kMaxLevels && d < (int)thr[i].size(); ++d) th[(size_t)i * kMaxLevels + d] = thr[i][d];
+    }
+    if (depth_limit > kMaxLevels) throw Error(-3, "depth limit beyond the verification table");
+    VTree* d_vt = (VTree*)dalloc(ctx, sizeof(VTree) * nt);
+    double* d_th = (double*)dalloc(ctx, sizeof(double) * th.size());
+    int cap = 4096;
+    std::vector<Miss> out;
+    for (;;) {
+        int* d_n = (int*)dalloc(ctx, sizeof(int));
+        Miss* d_m = (Miss*)dalloc(ctx, sizeof(Miss) * cap);
+        MWB_CUDA(cudaMemcpyAsync(d_vt, vt.data(), sizeof(VTree) * nt, cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(d_th, th.data(), sizeof(double) * th.size(), cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemsetAsync(d_n, 0, sizeof(int), s));
+        if (maxn > 0) {
+            k_verify<<<dim3((maxn + 255) / 256, nt), 256, 0, s>>>(d_vt, d_th, depth_limit, d_keep, d_n, d_m, cap);
+            MWB_CUDA(cudaGetLastError());
+        }
+        int nm = 0;
+        MWB_CUDA(cudaMemcpyAsync(&nm, d_n, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MWB_CUDA(cudaStreamSynchronize(s));
+        if (nm <= cap) {
+            out.resize(nm);
+            if (nm > 0) {
+                MWB_CUDA(cudaMemcpyAsync(out.data(), d_m, sizeof(Miss) * nm, cudaMemcpyDeviceToHost, s));
+                MWB_CUDA(cudaStreamSynchronize(s));
+            }
+            dfree(ctx, d_n);
+            dfree(ctx, d_m);
+            break;
+        }
+        dfree(ctx, d_n);
+        dfree(ctx, d_m);
+        cap = nm;  // the list did not fit: once more with room for all
+    }
+    dfree(ctx, d_vt);
+    dfree(ctx, d_th);
+    return out;
+}
+
+long long trees_rebuild_device(const std::vector<Tree*>& ts, const unsigned char* d_keep, cudaStream_t s) {
+    const int nt = (int)ts.size();
+    if (nt == 0) return 0;
+    Ctx* ctx = ts[0]->mra->ctx;
+    const size_t BS = ts[0]->mra->bsize();
+    std::vector<long long> offs(nt + 1, 0);
+    for (int i = 0; i < nt; ++i) offs[i + 1] = offs[i] + ts[i]->n;
+    const long long total = offs[nt];
+    if (total <= 0) return 0;
+    if (total > (1LL << 31) - 1) throw Error(-4, "too many nodes to rebuild at once");
+    const int N = (int)total;
+    // keys of all nodes, concatenated
+    uint64_t* d_k = (uint64_t*)dalloc(ctx, sizeof(uint64_t) * N);
+    for (int i = 0; i < nt; ++i)
+        if (ts[i]->n > 0)
+            MWB_CUDA(cudaMemcpyAsync(d_k + offs[i], ts[i]->key, sizeof(uint64_t) * ts[i]->n, cudaMemcpyDeviceToDevice, s));
+    // kept global indices, ascending (grouped by tree)
+    long long* d_g = (long long*)dalloc(ctx, sizeof(long long) * N);
+    int* d_nsel = (int*)dalloc(ctx, sizeof(int));
+    {
+        thrust::counting_iterator<long long> cnt(0);
+        size_t tmp = 0;
+        MWB_CUDA(cub::DeviceSelect::Flagged(nullptr, tmp, cnt, d_keep, d_g, d_nsel, N, s));
+        void* d_tmp = dalloc(ctx, std::max<size_t>(tmp, 1));
+        MWB_CUDA(cub::DeviceSelect::Flagged(d_tmp, tmp, cnt, d_keep, d_g, d_nsel, N, s));
+        dfree(ctx, d_tmp);
+    }
+    int n = 0;
+    MWB_CUDA(cudaMemcpyAsync(&n, d_nsel, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
+    // sort the kept nodes by key, then stably by tree: grouped by tree, key order inside a tree
+    uint64_t* d_kk = (uint64_t*)dalloc(ctx, sizeof(uint64_t) * std::max(1, n));
+    uint64_t* d_kk2 = (uint64_t*)dalloc(ctx, sizeof(uint64_t) * std::max(1, n));
+    long long* d_g2 = (long long*)dalloc(ctx, sizeof(long long) * std::max(1, n));
+    unsigned* d_tid = (unsigned*)dalloc(ctx, sizeof(unsigned) * std::max(1, n));
+    unsigned* d_tid2 = (unsigned*)dalloc(ctx, sizeof(unsigned) * std::max(1, n));
+    long long* d_offs = (long long*)dalloc(ctx, sizeof(long long) * (nt + 1));
+    int* d_cnt = (int*)dalloc(ctx, sizeof(int) * nt);
+    MWB_CUDA(cudaMemcpyAsync(d_offs, offs.data(), sizeof(long long) * (nt + 1), cudaMemcpyHostToDevice, s));
+    MWB_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(int) * nt, s));
+    k_gather_keys<<<(n + 255) / 256, 256, 0, s>>>(d_k, d_g, n, d_kk);
+    {
+        size_t tmp = 0;
+        MWB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, d_kk, d_kk2, d_g, d_g2, n, 0, 64, s));
+        void* d_tmp = dalloc(ctx, std::max<size_t>(tmp, 1));
+        MWB_CUDA(cub::DeviceRadixSort::SortPairs(d_tmp, tmp, d_kk, d_kk2, d_g, d_g2, n, 0, 64, s));
+        dfree(ctx, d_tmp);
+    }
+    k_tree_of<<<(n + 255) / 256, 256, 0, s>>>(d_g2, n, d_offs, nt, d_tid, d_cnt);
+    {
+        int bits = 1;
+        while ((1 << bits) < nt) ++bits;
+        size_t tmp = 0;
+        MWB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, d_tid, d_tid2, d_g2, d_g, n, 0, bits, s));
+        void* d_tmp = dalloc(ctx, std::max<size_t>(tmp, 1));
+        MWB_CUDA(cub::DeviceRadixSort::SortPairs(d_tmp, tmp, d_tid, d_tid2, d_g2, d_g, n, 0, bits, s));
+        dfree(ctx, d_tmp);
+    }
+    MWB_CUDA(cudaGetLastError());
+    std::vector<int> cnt(nt);
+    MWB_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int) * nt, cudaMemcpyDeviceToHost, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
+    // new arrays, gather, swap
+    std::vector<RTree> rt(nt);
+    long long noff = 0;
+    for (int i = 0; i < nt; ++i) {
+        Tree& t = *ts[i];
+        const int nn = cnt[i];
+        RTree& R = rt[i];
+        R.okey = t.key;
+        R.ocoef = t.coef;
+        R.on2 = t.norm2;
+        R.ow2 = t.wnorm2;
+        R.nkey = (uint64_t*)dalloc(ctx, sizeof(uint64_t) * std::max(1, nn));
+        R.ncoef = (double*)dalloc(ctx, sizeof(double) * BS * std::max(1, nn));
+        R.nn2 = (double*)dalloc(ctx, sizeof(double) * std::max(1, nn));
+        R.nw2 = (double*)dalloc(ctx, sizeof(double) * std::max(1, nn));
+        R.nparent = (int*)dalloc(ctx, sizeof(int) * std::max(1, nn));
+        R.nchild0 = (int*)dalloc(ctx, sizeof(int) * std::max(1, nn));
+        R.hkey = t.hkey;
+        R.hval = t.hval;
+        R.hcap = t.hcap;
+        R.off = offs[i];
+        R.noff = noff;
+        R.nn = nn;
+        noff += nn;
+    }
+    RTree* d_rt = (RTree*)dalloc(ctx, sizeof(RTree) * nt);
+    MWB_CUDA(cudaMemcpyAsync(d_rt, rt.data(), sizeof(RTree) * nt, cudaMemcpyHostToDevice, s));
+    if (n > 0) k_rebuild_gather<<<n, 256, 0, s>>>(d_g, d_tid2, n, d_rt, BS);
+    MWB_CUDA(cudaGetLastError());
+    for (int i = 0; i < nt; ++i) {
+        Tree& t = *ts[i];
+        RTree& R = rt[i];
+        dfree(ctx, t.key);
+        dfree(ctx, t.coef);
+        dfree(ctx, t.norm2);
+        dfree(ctx, t.wnorm2);
+        dfree(ctx, t.parent);
+        dfree(ctx, t.child0);
+        t.key = R.nkey;
+        t.coef = R.ncoef;
+        t.norm2 = R.nn2;
+        t.wnorm2 = R.nw2;
+        t.parent = R.nparent;
+        t.child0 = R.nchild0;
+        t.n = R.nn;
+        t.cap = std::max(1, R.nn);
+        launch_hash_reset(t, s);
+        launch_hash_insert(t, 0, t.n, s);
+    }
+    // links and level starts from the rebuilt hash indices
+    int* d_lb = (int*)dalloc(ctx, sizeof(int) * (size_t)nt * (kMaxLevels + 1));
+    MWB_CUDA(cudaMemsetAsync(d_lb, 0xff, sizeof(int) * (size_t)nt * (kMaxLevels + 1), s));
+    if (n > 0) k_rebuild_links<<<(n + 255) / 256, 256, 0, s>>>(d_tid2, n, d_rt, d_lb);
+    MWB_CUDA(cudaGetLastError());
+    std::vector<int> lb((size_t)nt * (kMaxLevels + 1));
+    MWB_CUDA(cudaMemcpyAsync(lb.data(), d_lb, sizeof(int) * lb.size(), cudaMemcpyDeviceToHost, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < nt; ++i) {
+        Tree& t = *ts[i];
+        const int* L = lb.data() + (size_t)i * (kMaxLevels + 1);
+        int maxd = 0;
+        for (int d = 0; d < kMaxLevels; ++d)
+            if (L[d] >= 0) maxd = d;
+        t.level_begin.assign(maxd + 2, 0);
+        for (int d = 0; d <= maxd; ++d) {
+            if (L[d] < 0) throw Error(-3, "rebuilt tree has an empty level");
+            t.level_begin[d] = L[d];
+        }
+        t.level_begin[maxd + 1] = t.n;
+    }
+    for (void* p : std::initializer_list<void*>{d_k, d_g, d_nsel, d_kk, d_kk2, d_g2, d_tid, d_tid2, d_offs, d_cnt, d_rt,
+                                                d_lb})
+        dfree(ctx, p);
+    return total - n;
 }
 
 }  // namespace mwb

@@ -43,6 +43,20 @@ void mlp_append(Mlp& M, const float* d_F, const std::vector<float>& y, cudaStrea
 float* features(Ctx* ctx, std::vector<FeatCtx>& fc, const std::vector<int2>& items, cudaStream_t s);
 void trees_rebuild(const std::vector<Tree*>& ts, const std::vector<std::vector<char>>& keeps,
                    const std::vector<std::vector<uint64_t>>& keys);
+// Exact criterion over every node of the trees, on the device: keep[off[i] + q] = 1 when every strict
+// ancestor of node q of tree i splits (sqrt(wnorm2) > thr[i][depth], depth < depth_limit); a kept node
+// that splits but has no children is a miss.  Returns the misses as (tree, node, key) triples in no
+// particular order.  d_keep must hold sum(n) bytes.
+struct Miss {
+    int tree, node;
+    uint64_t key;
+};
+std::vector<Miss> verify_trees(const std::vector<Tree*>& ts, const std::vector<std::vector<double>>& thr,
+                               int depth_limit, unsigned char* d_keep, cudaStream_t s);
+// Rebuild every tree from its kept nodes (d_keep as written by verify_trees for the same trees),
+// ordered by key (parents before children, level-contiguous), on the device; one synchronisation.
+// Returns the number of nodes dropped.
+long long trees_rebuild_device(const std::vector<Tree*>& ts, const unsigned char* d_keep, cudaStream_t s);
 uint64_t host_make_key(int depth, long long tx, long long ty, long long tz);
 void host_key_trans(uint64_t k, long long t[3]);
 
