@@ -1632,6 +1632,7 @@ int mw_apply_learned(int n, double prec, mw_tree* out, mw_op* ops, mw_tree* inp,
         MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3, "unknown apply flags");
         MW_ARG(tau > 0.0f && tau < 1.0f, "tau must be in (0, 1)");
         MW_ARG(inp[0], "null input tree");
+        MW_ARG(mlp->ctx == inp[0]->mra->ctx, "the network and the trees belong to different contexts");
         MWB_CUDA(cudaSetDevice(inp[0]->mra->ctx->device));
         std::vector<Tree*> o(n), i(n);
         std::vector<Op*> p(n);

@@ -126,3 +126,14 @@ def test_trained_network_saves_passes(gpu_mod):
     assert st["missed"] * 8 < 0.1 * total, st
     assert st["pruned"] < 0.2 * total, st
     assert st["passes"] < plain_passes, (st, plain_passes)
+
+
+def test_network_of_another_context_rejected(gpu_mod):
+    """Handles of different contexts (streams) are never mixed in one call."""
+    G = gpu_mod
+    prec = 1e-4
+    m = G.MultiResolutionAnalysis(*WORLD, 5, 12)
+    inps, ops = _setup(G, m, 3, 1, prec)
+    other = G.ProposalNet(ctx=G.Context(0), hidden_layers=1, width=16, seed=1)
+    with pytest.raises(G.MWError):
+        G.apply_learned(prec, [G.FunctionTree(m)], ops, inps, other, tau=0.5)
