@@ -46,7 +46,7 @@ def parse():
     p.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--tau", type=float, default=0.99, help="proposal threshold of the learned apply")
-    p.add_argument("--e2e-workers", type=int, default=2,
+    p.add_argument("--e2e-workers", type=int, default=3,
                    help="host threads (one context and stream each) sharing the batch in the e2e measurement")
     p.add_argument("--reserve-gib", type=int, default=64,
                    help="device memory pool reserved up front (GiB): the working set of the step")
@@ -325,7 +325,7 @@ def run_gpu(args):
     # pinned host memory, applies, and downloads the output trees into pinned host memory (buffers
     # allocated once, as a caller that streams batches would).  The batch is served by several workers,
     # each a host thread with its own context (stream), operators and copy of the network, taking
-    # a share of the orbitals (--e2e-workers, default 2): one worker's transfers overlap another's
+    # a share of the orbitals (--e2e-workers, default 3): one worker's transfers overlap another's
     # compute (the library releases the interpreter lock in every call).
     import threading
 
