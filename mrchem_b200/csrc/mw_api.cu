@@ -551,30 +551,7 @@ static void op_init(Op& op, Mra* m, double mu, double prec) {
 // append the 8 children of every listed node, for several trees, with one synchronisation
 static void add_children_many(const std::vector<Tree*>& ts, const std::vector<std::vector<int>>& lists) {
     if (ts.empty()) return;
-    Ctx* ctx = ts[0]->mra->ctx;
-    cudaStream_t s = ctx->stream;
-    size_t tot = 0;
-    for (auto& l : lists) tot += l.size();
-    if (tot == 0) return;
-    std::vector<int> flat;
-    flat.reserve(tot);
-    for (auto& l : lists) flat.insert(flat.end(), l.begin(), l.end());
-    int* d_list = (int*)dalloc(ctx, sizeof(int) * tot);
-    MWB_CUDA(cudaMemcpyAsync(d_list, flat.data(), sizeof(int) * tot, cudaMemcpyHostToDevice, s));
-    size_t off = 0;
-    for (size_t i = 0; i < ts.size(); ++i) {
-        Tree& t = *ts[i];
-        const int ns = (int)lists[i].size();
-        if (ns == 0) continue;
-        tree_reserve(t, t.n + 8 * ns);
-        launch_make_children(t, d_list + off, ns, s);
-        launch_hash_insert(t, t.n, t.n + 8 * ns, s);
-        t.n += 8 * ns;
-        t.level_begin.push_back(t.n);
-        off += ns;
-    }
-    MWB_CUDA(cudaStreamSynchronize(s));
-    dfree(ctx, d_list);
+    trees_add_children(ts, lists, ts[0]->mra->ctx->stream);
 }
 
 

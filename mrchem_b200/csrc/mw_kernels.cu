@@ -20,10 +20,8 @@ __global__ void k_hash_reset(uint64_t* hk, int* hv, uint32_t cap) {
         hv[i] = -1;
     }
 }
-__global__ void k_hash_insert(uint64_t* hk, int* hv, uint32_t cap, const uint64_t* keys, int begin, int end) {
-    const int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= end) return;
-    const uint64_t key = keys[i];
+// node i with key `key` into the open-addressing index (linear probing, at most cap probes)
+__device__ __forceinline__ void hash_insert_one(uint64_t* hk, int* hv, uint32_t cap, uint64_t key, int i) {
     const uint32_t mask = cap - 1;
     uint32_t h = hslot(key, mask);
     for (uint32_t p = 0; p < cap; ++p) {
@@ -35,6 +33,11 @@ __global__ void k_hash_insert(uint64_t* hk, int* hv, uint32_t cap, const uint64_
         }
         h = (h + 1) & mask;
     }
+}
+__global__ void k_hash_insert(uint64_t* hk, int* hv, uint32_t cap, const uint64_t* keys, int begin, int end) {
+    const int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= end) return;
+    hash_insert_one(hk, hv, cap, keys[i], i);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -316,6 +319,41 @@ __global__ void k_make_children(TView t, const int* __restrict__ list, int nspli
     }
 }
 
+// children of the split nodes of several trees in one launch: entry q of the flat list belongs to tree
+// tree_of[q]; its 8 children are appended after the tree's first nold nodes (in list order) and
+// entered into the tree's hash index
+struct ChildTree {
+    TView t;
+    uint64_t* hkey;
+    int* hval;
+    uint32_t hcap;
+    int nold;   // nodes before the appended children
+    int first;  // first list entry of this tree
+};
+__global__ void k_make_children_many(const ChildTree* __restrict__ ts, const int* __restrict__ tree_of,
+                                     const int* __restrict__ list, int ntot) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= ntot) return;
+    const ChildTree& T = ts[tree_of[q]];
+    const int p = list[q];
+    const int c0 = T.nold + 8 * (q - T.first);
+    T.t.child0[p] = c0;
+    long long tr[3];
+    const uint64_t key = T.t.key[p];
+    key_trans(key, tr);
+    const int d = key_depth(key) + 1;
+    for (int c = 0; c < 8; ++c) {
+        const int i = c0 + c;
+        const uint64_t ck = make_key(d, 2 * tr[0] + (c & 1), 2 * tr[1] + ((c >> 1) & 1), 2 * tr[2] + ((c >> 2) & 1));
+        T.t.key[i] = ck;
+        T.t.parent[i] = p;
+        T.t.child0[i] = -1;
+        T.t.norm2[i] = 0.0;
+        T.t.wnorm2[i] = 0.0;
+        hash_insert_one(T.hkey, T.hval, T.hcap, ck, i);
+    }
+}
+
 // deterministic single-block reductions (fixed summation order)
 __global__ void k_reduce_norm2(const double* __restrict__ norm2, const int* __restrict__ child0, int begin,
                                int end, int leaves_only, int want_max, double* out) {
@@ -581,6 +619,45 @@ int launch_internal_list(Tree& t, int begin, int end, int* d_list, cudaStream_t 
     int cnt = compact_flags(ctx, d_flags, n, begin, d_list, s);
     dfree(ctx, d_flags);
     return cnt;
+}
+
+void trees_add_children(const std::vector<Tree*>& ts, const std::vector<std::vector<int>>& lists, cudaStream_t s) {
+    size_t tot = 0;
+    for (auto& l : lists) tot += l.size();
+    if (tot == 0 || ts.empty()) return;
+    Ctx* ctx = ts[0]->mra->ctx;
+    std::vector<ChildTree> ct;
+    std::vector<int> buf(2 * tot);  // list entries, then their tree (index into ct)
+    size_t off = 0;
+    for (size_t i = 0; i < ts.size(); ++i) {
+        Tree& t = *ts[i];
+        const int ns = (int)lists[i].size();
+        if (ns == 0) continue;
+        tree_reserve(t, t.n + 8 * ns);  // may move the arrays and grow the hash index
+        ct.push_back(ChildTree{view(t), t.hkey, t.hval, t.hcap, t.n, (int)off});
+        for (int q = 0; q < ns; ++q) {
+            buf[off + q] = lists[i][q];
+            buf[tot + off + q] = (int)ct.size() - 1;
+        }
+        off += ns;
+    }
+    int* d_buf = (int*)dalloc(ctx, sizeof(int) * buf.size());
+    ChildTree* d_ct = (ChildTree*)dalloc(ctx, sizeof(ChildTree) * ct.size());
+    MWB_CUDA(cudaMemcpyAsync(d_buf, buf.data(), sizeof(int) * buf.size(), cudaMemcpyHostToDevice, s));
+    MWB_CUDA(cudaMemcpyAsync(d_ct, ct.data(), sizeof(ChildTree) * ct.size(), cudaMemcpyHostToDevice, s));
+    k_make_children_many<<<(int)((tot + 127) / 128), 128, 0, s>>>(d_ct, d_buf + tot, d_buf, (int)tot);
+    MWB_CUDA(cudaGetLastError());
+    count(ctx);
+    for (size_t i = 0; i < ts.size(); ++i) {
+        Tree& t = *ts[i];
+        const int ns = (int)lists[i].size();
+        if (ns == 0) continue;
+        t.n += 8 * ns;
+        t.level_begin.push_back(t.n);
+    }
+    MWB_CUDA(cudaStreamSynchronize(s));  // the host vectors and the staging buffers are released
+    dfree(ctx, d_buf);
+    dfree(ctx, d_ct);
 }
 
 void launch_make_children(Tree& t, const int* d_list, int nsplit, cudaStream_t s) {

@@ -44,6 +44,9 @@ int launch_split(Tree& t, int begin, int end, int depth, double thr, int depth_l
                  cudaStream_t s);
 // append 8 children for each node in d_list (n_split entries)
 void launch_make_children(Tree& t, const int* d_list, int nsplit, cudaStream_t s);
+// append 8 children for every node in lists[i] of tree ts[i] (one level per tree), enter them into the
+// hash indices and push the new level start; one launch for all trees
+void trees_add_children(const std::vector<Tree*>& ts, const std::vector<std::vector<int>>& lists, cudaStream_t s);
 // internal node list of [begin, end) (returns count)
 int launch_internal_list(Tree& t, int begin, int end, int* d_list, cudaStream_t s);
 // deterministic reductions: sum of norm2 over leaves (or over [begin,end) when all=true), max norm2
