@@ -12,7 +12,8 @@
 //      step x: rows (b, c),  slot  b + S1 c      D1[slot][a'] = sum_a X[slot][a] Mx[a'][a]
 //      step y: rows (c, a'), slot  c + S2 a'     D2[slot][b'] = sum_b T1[slot][b] My[b'][b]
 //      step z: rows (a', b'), slot a' + S3 b'    D3[slot][c'] = sum_c T2[slot][c] Mz[c'][c]
-// Every operand is K-major in shared memory (element (slot, k) at 16 (slot + MR (k / 4)) + 4 (k % 4)).
+// Every operand is K-major in shared memory (element (slot, k) at 16 (slot + MR (k / 4)) + 4 (k % 4),
+// with a chunk stride MR per operand).
 // The epilogue of a step reads its row of D from TMEM (thread = TMEM lane = slot), transposes 4 x 4
 // blocks inside each quad of lanes (four consecutive slots share the slow index and hold four
 // consecutive values of the next step's contracted index), splits the values into TF32 hi + lo and
@@ -66,10 +67,14 @@ struct TCfg {
     static constexpr int T1 = (R1 + 127) / 128, T2 = (R2 + 127) / 128, T3 = (R3 + 127) / 128;
     static constexpr int RMAX = R1 > R2 ? (R1 > R3 ? R1 : R3) : (R2 > R3 ? R2 : R3);
     static constexpr int NTM = (RMAX + 127) / 128;
-    // row stride of the K chunks: >= every slot written, and 4 mod 8 so that the two quads of lanes
-    // in one 8-lane store phase fall into different bank groups
+    // row strides of the K chunks (>= every slot written), chosen for the epilogue that writes the
+    // operand: the y epilogue (z operand) is conflict-free with a stride of 4 mod 8; the x epilogue (y
+    // operand) puts a quad's lanes j and j+2 in one bank group whatever the stride, and a stride of
+    // 2 mod 8 keeps the two quads of an 8-lane phase in different groups.  The input operand uses MR.
     static constexpr int MR = (RMAX + 3) / 8 * 8 + 4;
-    static constexpr int IMG = 16 * (MR * (NCH - 1) + 128 * NTM);  // bytes of one operand image
+    static constexpr int MRY = (R2 + 5) / 8 * 8 + 2;
+    static constexpr int MRMAX = MR > MRY ? MR : MRY;
+    static constexpr int IMG = 16 * (MRMAX * (NCH - 1) + 128 * NTM);  // bytes of one operand image
     static constexpr int NB = 12 * KP8;                             // rows of the shared operator image
     static constexpr int OPIMG = NB * KP8 * 4;                      // its bytes
     static constexpr int GOPB = 3 * KP8 * KP8 * 4;  // one global operator image (hi, mid, lo rows)
@@ -83,7 +88,7 @@ struct TCfg {
     static constexpr int TCOLS = TCOLS_NEED <= 128 ? 128 : TCOLS_NEED <= 256 ? 256 : 512;
     static constexpr size_t SMEM = 4 * (size_t)IMG + (size_t)OPIMG + 3 * (size_t)ATF * 4 + 3 * (size_t)KKK * 4;
     static constexpr bool FITS = SMEM + 1024 <= 232448 && TCOLS_NEED <= 512 && KK <= 128 && KP8 >= 16 &&
-                                 NMMA <= 256 && (size_t)IMG >= (size_t)KKK * 8 + 64 * 8 && MR < 16384;
+                                 NMMA <= 256 && (size_t)IMG >= (size_t)KKK * 8 + 64 * 8 && MRMAX < 16384;
 };
 
 template <int K>
@@ -93,7 +98,7 @@ __global__ void __launch_bounds__(256, 1)
              const double* __restrict__ gnorm2, double* partials, unsigned long long* ntrip_out, int* err_out) {
     using C = TCfg<K>;
     constexpr int NTHR = C::NTHR;
-    constexpr int K2 = C::K2, KP4 = C::KP4, KP8 = C::KP8, MR = C::MR, KK = C::KK, KKK = C::KKK;
+    constexpr int K2 = C::K2, KP4 = C::KP4, KP8 = C::KP8, MR = C::MR, MRY = C::MRY, KK = C::KK, KKK = C::KKK;
     constexpr int S1 = C::S1, S2 = C::S2, S3 = C::S3, ACCW = C::ACCW, IMG = C::IMG;
     constexpr int NB = C::NB, GOPB = C::GOPB, ATF = C::ATF, NG = C::NG, NGH = C::NGH, DSTR = C::DSTR;
     constexpr int BS = K2 * K2 * K2;
@@ -171,10 +176,10 @@ __global__ void __launch_bounds__(256, 1)
     // one step: every tile of 128 slots, every K step, two MMAs (A_hi against [hi; mid; lo], A_lo against
     // [0; hi; mid] of the operator); consecutive MMAs go to different tiles (independent accumulators);
     // the first half of the tiles commits to bar2[0], the rest to bar2[1]
-    auto issue = [&](uint32_t a_hi, uint32_t a_lo, int q, int ntiles, int nks, uint64_t* bar2) {
+    auto issue = [&](uint32_t a_hi, uint32_t a_lo, int mra, int q, int ntiles, int nks, uint64_t* bar2) {
         tmem_fence_after_sync();
         const uint32_t r0 = (uint32_t)(KP8 + 4 * KP8 * q);
-        const uint64_t ah0 = umma_sdesc(a_hi, 16u * MR, 128u), al0 = umma_sdesc(a_lo, 16u * MR, 128u);
+        const uint64_t ah0 = umma_sdesc(a_hi, 16u * mra, 128u), al0 = umma_sdesc(a_lo, 16u * mra, 128u);
         const uint64_t b1 = umma_sdesc(sops + 16u * r0, 16u * NB, 128u);
         const uint64_t b2 = umma_sdesc(sops + 16u * (r0 - KP8), 16u * NB, 128u);
         const int nfirst = (ntiles + 1) / 2;
@@ -184,10 +189,10 @@ __global__ void __launch_bounds__(256, 1)
                 const uint32_t acc = kk > 0 ? 1u : 0u;
                 const uint64_t bo = (uint64_t)(NB * 2 * kk);  // descriptor start addresses are in 16-byte units
                 for (int t = t0; t < t1; ++t)
-                    umma_tf32(tbase + (uint32_t)(C::COL_D + DSTR * t), ah0 + (uint64_t)(128 * t + MR * 2 * kk),
+                    umma_tf32(tbase + (uint32_t)(C::COL_D + DSTR * t), ah0 + (uint64_t)(128 * t + mra * 2 * kk),
                               b1 + bo, idesc, acc);
                 for (int t = t0; t < t1; ++t)
-                    umma_tf32(tbase + (uint32_t)(C::COL_D + DSTR * t), al0 + (uint64_t)(128 * t + MR * 2 * kk),
+                    umma_tf32(tbase + (uint32_t)(C::COL_D + DSTR * t), al0 + (uint64_t)(128 * t + mra * 2 * kk),
                               b2 + bo, idesc, 1u);
             }
             umma_commit(&bar2[part]);  // arrives when this part's MMAs (and all earlier ones) are done
@@ -196,7 +201,7 @@ __global__ void __launch_bounds__(256, 1)
     // epilogue of the x or y step: slot (fast, slow) with fast = slot % S, slow = slot / S holds the
     // values of output index `col`; the next operand takes slot next_slot(slow, col), K chunk fast / 4.
     // This warp takes the column groups g = half, half + 2, ...
-    auto epi = [&](auto s_tag, int t0, int t1, auto next_slot) {
+    auto epi = [&](auto s_tag, int mrn, int t0, int t1, auto next_slot) {
         constexpr int S = decltype(s_tag)::value;
         for (int t = t0; t < t1; ++t) {
             uint32_t r[12 * NGH];
@@ -228,7 +233,7 @@ __global__ void __launch_bounds__(256, 1)
                 quad_transpose(x, j4);
                 const int col = 4 * g + j4;
                 if (slow < K2 && col < K2) {
-                    const uint32_t off = 16u * (uint32_t)(next_slot(slow, col) + MR * chunk);
+                    const uint32_t off = 16u * (uint32_t)(next_slot(slow, col) + mrn * chunk);
                     uint32_t h[4], l[4];
 #pragma unroll
                     for (int q = 0; q < 4; ++q) split_tf32(x[q], h[q], l[q]);
@@ -399,14 +404,14 @@ __global__ void __launch_bounds__(256, 1)
             const bool has_next = ti + 1 < de.t1 && !(TR.terms[ti + 1].bound * nu < theta);
             const TermRec tn = has_next ? TR.terms[ti + 1] : tr;
             // ---- x
-            if (tid == 0) issue(sxh, sxl, 0, C::T1, nks, &bars[0]);
+            if (tid == 0) issue(sxh, sxl, MR, 0, C::T1, nks, &bars[0]);
             corr_x();
             if (!mbar_wait(&bars[0], ph, kWaitNs)) bad = 1;
             tmem_fence_after_sync();
-            epi(std::integral_constant<int, S1>{}, 0, (C::T1 + 1) / 2, [](int c, int ap) { return c + S2 * ap; });
+            epi(std::integral_constant<int, S1>{}, MRY, 0, (C::T1 + 1) / 2, [](int c, int ap) { return c + S2 * ap; });
             if (!mbar_wait(&bars[1], ph, kWaitNs)) bad = 1;
             tmem_fence_after_sync();
-            epi(std::integral_constant<int, S1>{}, (C::T1 + 1) / 2, C::T1, [](int c, int ap) { return c + S2 * ap; });
+            epi(std::integral_constant<int, S1>{}, MRY, (C::T1 + 1) / 2, C::T1, [](int c, int ap) { return c + S2 * ap; });
             tmem_fence_before_sync();
             cp_async_wait_all();
             fence_proxy_async_smem();
@@ -414,13 +419,13 @@ __global__ void __launch_bounds__(256, 1)
             if (bad) break;
             if (has_next) load_op(0, tn);  // the x MMAs and corr_x are done with the x rows
             // ---- y
-            if (tid == 0) issue(sth, stl, 1, C::T2, nks, &bars[2]);
+            if (tid == 0) issue(sth, stl, MRY, 1, C::T2, nks, &bars[2]);
             corr_y();
             // the y epilogue overwrites the y MMAs' own operand (T) in place: all of them must be done
             if (!mbar_wait(&bars[2], ph, kWaitNs)) bad = 1;
             if (!mbar_wait(&bars[3], ph, kWaitNs)) bad = 1;
             tmem_fence_after_sync();
-            epi(std::integral_constant<int, S2>{}, 0, C::T2, [](int ap, int bp) { return ap + S3 * bp; });
+            epi(std::integral_constant<int, S2>{}, MR, 0, C::T2, [](int ap, int bp) { return ap + S3 * bp; });
             tmem_fence_before_sync();
             cp_async_wait_all();
             fence_proxy_async_smem();
@@ -428,7 +433,7 @@ __global__ void __launch_bounds__(256, 1)
             if (bad) break;
             if (has_next) load_op(1, tn);
             // ---- z
-            if (tid == 0) issue(sth, stl, 2, C::T3, nks, &bars[4]);
+            if (tid == 0) issue(sth, stl, MR, 2, C::T3, nks, &bars[4]);
             corr_z();
             if (!mbar_wait(&bars[4], ph, kWaitNs)) bad = 1;
             tmem_fence_after_sync();
