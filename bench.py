@@ -608,9 +608,10 @@ def run_exchange(args):
 def run_density_sweep(args):
     """Poisson potential of a 20-atom density (4 normalised Gaussians per atom, exponents
     log-U[0.3, 1e3], atoms in a 12 Bohr box) at interpolating orders 7/9/11 and precisions
-    1e-5/1e-6/1e-7: FP64 and mixed (FP32 products, FP64 accumulation) applies on the GPU, each timed
-    over --steps steps after --warmup, with the relative error of the mixed potential against FP64
-    (coefficient differences) and the CPU restatement's time for one apply at order 7, prec 1e-5."""
+    1e-5/1e-6/1e-7: FP64, mixed (FP32 products, FP64 accumulation) and split-TF32 tensor-core applies
+    on the GPU, each timed over --steps steps after --warmup, with the relative errors of the mixed and
+    tensor-core potentials against FP64 (coefficient differences) and the CPU restatement's time for
+    one apply at order 7, prec 1e-5.  (At order 11, k = 12, the tensor-core flag runs the FP32 engine.)"""
     import torch
 
     world, rank, local = dist_env()
@@ -631,7 +632,7 @@ def run_density_sweep(args):
             P = G.PoissonOperator(m, prec)
             row = {"order": order, "k": order + 1, "prec": prec, "input_nodes": rho.nnodes()}
             outs = {}
-            for name, fl in (("fp64", G.APPLY_FP64), ("mixed", G.APPLY_FP32)):
+            for name, fl in (("fp64", G.APPLY_FP64), ("mixed", G.APPLY_FP32), ("tf32x3", G.APPLY_TF32X3)):
                 out = G.FunctionTree(m)
                 for _ in range(args.warmup):
                     G.apply(prec, out, P, rho, fl)
@@ -650,8 +651,11 @@ def run_density_sweep(args):
                              "tflops": st[0] * flops_per_triple(order + 1) / (kms / 1e3) / 1e12 if kms > 0 else None}
                 outs[name] = out
             row["rel_error_mixed"] = G.distance(outs["mixed"], outs["fp64"]) / np.sqrt(outs["fp64"].square_norm())
+            row["rel_error_tf32x3"] = G.distance(outs["tf32x3"], outs["fp64"]) / np.sqrt(outs["fp64"].square_norm())
             row["same_nodes"] = outs["mixed"].nnodes() == outs["fp64"].nnodes()
+            row["same_nodes_tf32x3"] = outs["tf32x3"].nnodes() == outs["fp64"].nnodes()
             row["speedup_mixed"] = row["fp64"]["ms"] / row["mixed"]["ms"]
+            row["speedup_tf32x3"] = row["fp64"]["ms"] / row["tf32x3"]["ms"]
             rows.append(row)
             print(json.dumps(row), file=sys.stderr, flush=True)
     cpu = None
@@ -669,10 +673,10 @@ def run_density_sweep(args):
         cpu = {"order": 7, "prec": 1e-5, "s_per_apply": time.perf_counter() - t0,
                "cores": O.lib().oracle_num_threads(), "kind": "port"}
     if rank == 0:
-        print(json.dumps({"metric": "Poisson apply of a 20-atom density: orders x precisions, FP64 and mixed",
+        print(json.dumps({"metric": "Poisson apply of a 20-atom density: orders x precisions, FP64, mixed, split-TF32",
                           "workload": "density_20_atoms_sweep", "data": "synthetic", "steps": args.steps,
                           "warmup": args.warmup, "rows": rows, "cpu_baseline": cpu,
-                          "not_built": ["split-TF32", "BF16x3"]}), flush=True)
+                          "not_built": ["BF16x3"]}), flush=True)
 
 
 def main():
