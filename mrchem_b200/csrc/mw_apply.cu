@@ -28,6 +28,7 @@
 namespace mwb {
 
 constexpr int kChunkTriples = 48;  // triples per contraction CTA (load balance vs partial traffic)
+constexpr double kTensorCoreMinPrec = 1e-6;  // finest prec served by the split-TF32 engine
 
 struct BTree {
     const uint64_t* okey;
@@ -1343,9 +1344,13 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     MWB_CUDA(cudaMemsetAsync(d_ntrip_tot, 0, 2 * sizeof(unsigned long long), s));
     if (ctx->prof) MWB_CUDA(cudaEventRecord(ctx->ev0, s));
     const bool pencil = contraction_pencil();
+    // the split-TF32 engine's error floor (about 2e-7 relative, data in two TF32 pieces) stays below the
+    // requested precision only from prec = 1e-6 up: finer requests take the FP32 engine
+    bool tc_prec_ok = true;
+    for (const BatchTree& b : bp.trees) tc_prec_ok &= !(b.prec > 0.0 && b.prec < kTensorCoreMinPrec);
 #define L_AP(KK)                                                                                             \
     {                                                                                                        \
-        if (bp.precision == 2 && TCfg<KK>::FITS && !pencil) {                                                \
+        if (bp.precision == 2 && TCfg<KK>::FITS && !pencil && tc_prec_ok) {                                  \
             size_t smem = TCfg<KK>::SMEM;                                                                    \
             MWB_CUDA(cudaFuncSetAttribute(k_tapply<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
             k_tapply<KK><<<nchunks, TCfg<KK>::NTHR, smem, s>>>(d_chunks, d_items, d_trees, d_cdelta, d_csrc,     \

@@ -113,3 +113,19 @@ def test_tf32x3_unknown_flag_rejected(gpu_mod):
     G.project(1e-3, inp, two_gaussians(G))
     with pytest.raises(G.MWError):
         G.apply(1e-3, G.FunctionTree(m), G.PoissonOperator(m, 1e-3), inp, 3)
+
+
+def test_tf32x3_fine_precision_takes_fp32_engine(gpu_mod):
+    """Below prec 1e-6 the split-TF32 error floor (about 2e-7) would exceed the request: the flag runs
+    the FP32 engine there, bit for bit."""
+    G = gpu_mod
+    prec = 1e-7
+    m = G.MultiResolutionAnalysis(*WORLD, 7, 14)
+    inp = G.FunctionTree(m)
+    G.project(prec, inp, two_gaussians(G))
+    op = G.PoissonOperator(m, prec)
+    o32, otc = G.FunctionTree(m), G.FunctionTree(m)
+    G.apply(prec, o32, op, inp, G.APPLY_FP32)
+    G.apply(prec, otc, op, inp, G.APPLY_TF32X3)
+    assert otc.nnodes() == o32.nnodes()
+    assert G.distance(otc, o32) == 0.0
