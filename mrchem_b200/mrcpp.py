@@ -38,7 +38,7 @@ FUNC_GAUSSIANS = 1
 FUNC_HYDROGEN_PRODUCTS = 2
 APPLY_FP64 = 0
 APPLY_FP32 = 1
-APPLY_TF32X3 = 2  # split-TF32 products on the tensor cores, compensated summation over terms
+APPLY_TF32X3 = 2  # split-TF32 tensor cores (k <= 10, prec >= 1e-6; otherwise the FP32 engine)
 
 # every symbol include/mwb200.h declares: (name, restype, argtypes)
 SYMBOLS = [
