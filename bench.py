@@ -542,8 +542,9 @@ def cpu_baseline(args, inps, mus):
 def run_exchange(args):
     """Exchange pair batch: 16 orbitals (the Helmholtz batch's orbital model), the 136 pair products
     phi_i phi_j (i <= j, adaptive multiply as at ExchangePotential.cpp:253,312), each followed by a
-    Poisson apply (ExchangePotential.cpp:137).  One step = all 136 products and applies; FP64 and mixed
-    applies (the products are FP64 in both); error per pair of the mixed potential against FP64."""
+    Poisson apply (ExchangePotential.cpp:137).  One step = all 136 products and applies; FP64, mixed and
+    split-TF32 tensor-core applies (the products are FP64 in all); error per pair of the mixed and
+    tensor-core potentials against FP64."""
     import torch
 
     world, rank, local = dist_env()
@@ -575,7 +576,7 @@ def run_exchange(args):
         return prods, outs
 
     res = {}
-    for name, flags in (("fp64", G.APPLY_FP64), ("mixed", G.APPLY_FP32)):
+    for name, flags in (("fp64", G.APPLY_FP64), ("mixed", G.APPLY_FP32), ("tf32x3", G.APPLY_TF32X3)):
         for _ in range(args.warmup):
             step(flags)
         torch.cuda.synchronize()
@@ -595,13 +596,17 @@ def run_exchange(args):
         res[name + "_outs"] = outs
     errs = [G.distance(a, b) / np.sqrt(b.square_norm()) for a, b in zip(res["mixed_outs"], res["fp64_outs"])]
     same = all(a.nnodes() == b.nnodes() for a, b in zip(res["mixed_outs"], res["fp64_outs"]))
+    errs_t = [G.distance(a, b) / np.sqrt(b.square_norm()) for a, b in zip(res["tf32x3_outs"], res["fp64_outs"])]
+    same_t = all(a.nnodes() == b.nnodes() for a, b in zip(res["tf32x3_outs"], res["fp64_outs"]))
     if rank == 0:
         line = {"metric": "exchange pair batch: 136 pair products + Poisson applies", "workload": "exchange_16orb_136pairs_k10_prec1e-6",
                 "value": res["mixed"]["pairs_per_s"], "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "order": args.order, "prec": args.prec, "data": "synthetic",
-                "fp64": res["fp64"], "mixed": res["mixed"],
+                "fp64": res["fp64"], "mixed": res["mixed"], "tf32x3": res["tf32x3"],
                 "rel_error_per_pair": {"max": max(errs), "median": float(np.median(errs)), "min": min(errs)},
-                "same_node_count_as_fp64": bool(same)}
+                "same_node_count_as_fp64": bool(same),
+                "rel_error_per_pair_tf32x3": {"max": max(errs_t), "median": float(np.median(errs_t)), "min": min(errs_t)},
+                "same_node_count_as_fp64_tf32x3": bool(same_t)}
         print(json.dumps(line), flush=True)
 
 

@@ -35,8 +35,8 @@ enum { MW_FUNC_GAUSSIANS = 1, MW_FUNC_HYDROGEN_PRODUCTS = 2 };
 /* apply flags: FP64 products (the plain apply), or FP32 products with every term's contribution
  * accumulated in FP64 (mixed precision), or split-TF32 products on the tensor cores (data in two TF32
  * pieces, operators in three; FP32 sums inside a term, compensated summation over terms; relative
- * error about 2e-7, so it serves orders k <= 10 at prec >= 1e-6, and other requests take the FP32
- * path); norms, screening and refinement are FP64 in all three */
+ * error 2e-7 .. 1e-6, so it serves orders k <= 10 at prec >= 1e-6 (where its error is at most about
+ * prec), and other requests take the FP32 path); norms, screening and refinement are FP64 in all three */
 enum { MW_APPLY_FP64 = 0, MW_APPLY_FP32 = 1, MW_APPLY_TF32X3 = 2 };
 
 const char* mw_last_error(void);
