@@ -291,6 +291,20 @@ def run_gpu(args):
     del tr_in, tr_out, tr_ops
     t_train = time.perf_counter() - t_train
 
+    # contraction work split per engine, tuned (untimed) on this batch: every engine gets the same
+    # treatment (mrchem_b200.autotune)
+    from mrchem_b200.autotune import tune_chunk_triples
+
+    tuning = {}
+    for name, fl in (("fp64", G.APPLY_FP64), ("fp32", G.APPLY_FP32), ("tf32x3", G.APPLY_TF32X3)):
+        tune_out = [G.FunctionTree(m) for _ in range(args.orbitals)]
+
+        def tune_run(fl=fl, tune_out=tune_out):
+            G.apply_batched(args.prec, tune_out, ops, inps, fl)
+
+        tuning[name] = tune_chunk_triples(ctx, tune_run, fl, reps=2, warmup=1)
+        del tune_out
+
     # plain FP64 (the reference method on the GPU), the mixed path (FP32 products, FP64
     # accumulation) and mixed + learned proposal, same inputs, same operators
     ms64, trip64, prof64, _ = timed(lambda: G.apply_batched(args.prec, outs, ops, inps, G.APPLY_FP64), "plain_fp64")
@@ -362,6 +376,7 @@ def run_gpu(args):
             self.ctx = G.Context(local, stream=self.stream.cuda_stream)
             self.m = G.MultiResolutionAnalysis(W.WORLD["min_scale"], W.WORLD["corner"], W.WORLD["boxes"], args.order,
                                                15, ctx=self.ctx)
+            self.ctx.set_chunk_triples(G.APPLY_FP32, ctx.chunk_triples(G.APPLY_FP32))
             self.net = G.ProposalNet(ctx=self.ctx, hidden_layers=3, width=128, seed=5)
             self.net.set_params(net_params)
             self.ops = [G.HelmholtzOperator(self.m, mus[i], args.prec) for i in idx]
@@ -508,6 +523,7 @@ def run_gpu(args):
                          "traffic_unit": "DRAM bytes per launch (ncu bytes per CTA x CTAs per launch)",
                          "block_write_bytes_per_launch": apply_ctas * (2 * k) ** 3 * 8 / max(1, apply_launches)},
             "cpu_baseline": cpu,
+            "autotune": {k: {"chunk_triples": v["best"], "ms_per_candidate": v["ms"]} for k, v in tuning.items()},
             "gpu_launches": int(launches),
             "clocks": clocks,
         }

@@ -51,12 +51,19 @@ int mw_ctx_synchronize(mw_ctx ctx);
  * threshold: unlimited); a pool that must still grow maps new memory inside the first calls that
  * need it, which makes their time vary.  Reserving the working set once removes that. */
 int mw_ctx_reserve(mw_ctx ctx, unsigned long long bytes);
+/* Contraction work per CTA of the context's applies under `flags` (one of MW_APPLY_*): each output
+ * node's (input node, term) pairs are cut into chunks of at most `triples` (1 .. 4096; default 48),
+ * one CTA each; more triples per CTA mean fewer partial blocks to reduce, fewer mean better load
+ * balance.  Results agree to FP64 rounding for any value (the partial sums are regrouped).  No
+ * reference counterpart (MRCPP schedules with OpenMP); set by mrchem_b200.autotune or the caller. */
+int mw_ctx_set_chunk_triples(mw_ctx ctx, int flags, int triples);
+int mw_ctx_get_chunk_triples(mw_ctx ctx, int flags, int* triples);
 /* Benchmark counters (no reference counterpart: the reference times with mrcpp::Timer around whole
  * calls, src/scf_solver/HelmholtzVector.cpp:68-82).  enable != 0 resets and starts them: number of
  * kernels this library launched, and number and CUDA-event time (ms) of contraction-kernel launches. */
 int mw_ctx_profile(mw_ctx ctx, int enable);
 int mw_ctx_profile_read(mw_ctx ctx, long long* launches, long long* apply_launches, double* apply_ms);
-/* CTAs (chunks of <= 48 triples of one output node) of the contraction launches counted since
+/* CTAs (chunks of <= chunk_triples triples of one output node) of the contraction launches counted since
  * mw_ctx_profile(ctx, 1): the unit the contraction's DRAM traffic scales with */
 int mw_ctx_profile_ctas(mw_ctx ctx, long long* ctas);
 

@@ -1023,6 +1023,23 @@ int mw_ctx_create(int device, void* stream, mw_ctx* out) {
     })
 }
 
+int mw_ctx_set_chunk_triples(mw_ctx ctx, int flags, int triples) {
+    MW_TRY({
+        MW_ARG(ctx, "null context");
+        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3, "unknown apply flags");
+        MW_ARG(triples >= 1 && triples <= 4096, "triples per CTA must be in [1, 4096]");
+        ctx->chunk_triples[flags] = triples;
+    })
+}
+
+int mw_ctx_get_chunk_triples(mw_ctx ctx, int flags, int* triples) {
+    MW_TRY({
+        MW_ARG(ctx && triples, "null pointer");
+        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3, "unknown apply flags");
+        *triples = ctx->chunk_triples[flags];
+    })
+}
+
 int mw_ctx_reserve(mw_ctx ctx, unsigned long long bytes) {
     MW_TRY({
         MW_ARG(ctx, "null context");

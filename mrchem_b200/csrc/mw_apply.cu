@@ -7,7 +7,8 @@
 //      up in the input tree's hash index (or its leaf ancestor -> generated node) and screens it;
 //   2. generated (scaling-only) input nodes are de-duplicated per tree and built once;
 //   3. per candidate, the number of terms that pass the screening (the triples it contributes);
-//   4. each output node's candidate list is cut into chunks of at most kChunkTriples triples;
+//   4. each output node's candidate list is cut into chunks of at most chunk_triples triples (a
+//      per-engine context setting, 48 unless tuned);
 //   5. the contraction kernel runs one CTA per chunk; multi-chunk nodes write partial blocks that
 //      a reduction kernel adds in chunk order (deterministic), single-chunk nodes write directly;
 //   6. norms and split flags; children are appended to each tree.
@@ -27,7 +28,6 @@
 
 namespace mwb {
 
-constexpr int kChunkTriples = 48;  // triples per contraction CTA (load balance vs partial traffic)
 constexpr double kTensorCoreMinPrec = 1e-6;  // finest prec served by the split-TF32 engine
 
 struct BTree {
@@ -263,9 +263,9 @@ __global__ void k_cand_item(const int* __restrict__ offs, int nitems, int* cand_
     if (w >= nitems) return;
     for (int c = offs[w] + threadIdx.x; c < offs[w + 1]; c += blockDim.x) cand_item[c] = w;
 }
-// greedy cut of each node's candidates into chunks of at most kChunkTriples triples (whole
+// greedy cut of each node's candidates into chunks of at most `limit` triples (whole
 // candidates; at least one chunk per node so that every output block gets written)
-__global__ void k_bchunks(const int* __restrict__ offs, int nitems, const int* __restrict__ ntrip, int fill,
+__global__ void k_bchunks(const int* __restrict__ offs, int nitems, const int* __restrict__ ntrip, int limit, int fill,
                           int* nchunk, const int* __restrict__ choff, const int* __restrict__ slotoff, Chunk* chunks) {
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= nitems) return;
@@ -274,7 +274,7 @@ __global__ void k_bchunks(const int* __restrict__ offs, int nitems, const int* _
     const int multi = fill ? (choff[w + 1] - choff[w] > 1) : 0;
     for (int c = c0; c < c1; ++c) {
         const int t = ntrip[c];
-        if (acc > 0 && acc + t > kChunkTriples) {
+        if (acc > 0 && acc + t > limit) {
             if (fill) chunks[choff[w] + nch] = Chunk{w, start, c, multi ? slotoff[w] + nch : -1};
             ++nch;
             acc = 0;
@@ -1327,13 +1327,15 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     int* d_slotoff = (int*)dalloc(ctx, sizeof(int) * (ni + 1));
     MWB_CUDA(cudaMemsetAsync(d_nchunk, 0, sizeof(int) * (ni + 1), s));
     MWB_CUDA(cudaMemsetAsync(d_nslot, 0, sizeof(int) * (ni + 1), s));
-    k_bchunks<<<(ni + 127) / 128, 128, 0, s>>>(d_offs, ni, d_ntrip, 0, d_nchunk, nullptr, nullptr, nullptr);
+    const int chunk_limit = ctx->chunk_triples[std::min(std::max(bp.precision, 0), 2)];
+    k_bchunks<<<(ni + 127) / 128, 128, 0, s>>>(d_offs, ni, d_ntrip, chunk_limit, 0, d_nchunk, nullptr, nullptr, nullptr);
     k_multi_slots<<<(ni + 127) / 128, 128, 0, s>>>(d_nchunk, ni, d_nslot);
     count(ctx, 2);
     const int nchunks = scan_total(ctx, d_nchunk, d_choff, ni);
     const int nslots = scan_total(ctx, d_nslot, d_slotoff, ni);
     Chunk* d_chunks = (Chunk*)dalloc(ctx, sizeof(Chunk) * std::max(1, nchunks));
-    k_bchunks<<<(ni + 127) / 128, 128, 0, s>>>(d_offs, ni, d_ntrip, 1, d_nchunk, d_choff, d_slotoff, d_chunks);
+    k_bchunks<<<(ni + 127) / 128, 128, 0, s>>>(d_offs, ni, d_ntrip, chunk_limit, 1, d_nchunk, d_choff, d_slotoff,
+                                               d_chunks);
     MWB_CUDA(cudaGetLastError());
     count(ctx);
     double* d_partials = (double*)dalloc(ctx, sizeof(double) * BS * std::max(1, nslots));

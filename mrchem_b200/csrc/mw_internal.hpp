@@ -44,6 +44,9 @@ struct Ctx {
     long long apply_ctas = 0;  // CTAs (chunks) of those launches
     double apply_ms = 0.0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // contraction work per CTA: at most this many (output, input, term) triples, per engine (FP64, FP32,
+    // split-TF32); set by the caller or an autotuner (load balance against partial-block traffic)
+    int chunk_triples[3] = {48, 48, 48};
     // handles that point here (worlds, networks); a destroyed context is freed with the last of them
     int refs = 0;
     bool closed = false;

@@ -48,6 +48,8 @@ SYMBOLS = [
     ("mw_ctx_destroy", ctypes.c_int, [_vp]),
     ("mw_ctx_synchronize", ctypes.c_int, [_vp]),
     ("mw_ctx_reserve", ctypes.c_int, [_vp, ctypes.c_ulonglong]),
+    ("mw_ctx_set_chunk_triples", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    ("mw_ctx_get_chunk_triples", ctypes.c_int, [_vp, ctypes.c_int, _ip]),
     ("mw_ctx_profile", ctypes.c_int, [_vp, ctypes.c_int]),
     ("mw_ctx_profile_read", ctypes.c_int, [_vp, _lp, _lp, _dp]),
     ("mw_ctx_profile_ctas", ctypes.c_int, [_vp, _lp]),
@@ -161,6 +163,15 @@ class Context:
     def reserve(self, nbytes):
         """Grow the device memory pool to at least nbytes up front (see mw_ctx_reserve)."""
         _check(_lib.mw_ctx_reserve(self._h, int(nbytes)))
+
+    def set_chunk_triples(self, flags, triples):
+        """Contraction work per CTA for applies under `flags` (see mw_ctx_set_chunk_triples)."""
+        _check(_lib.mw_ctx_set_chunk_triples(self._h, int(flags), int(triples)))
+
+    def chunk_triples(self, flags):
+        v = ctypes.c_int()
+        _check(_lib.mw_ctx_get_chunk_triples(self._h, int(flags), ctypes.byref(v)))
+        return v.value
 
     def profile(self, enable=True):
         """Reset and (de)activate the kernel counters."""
