@@ -582,25 +582,31 @@ def run_exchange(args):
     pairs = [(i, j) for i in range(norb) for j in range(i, norb)]
     P = G.PoissonOperator(m, args.prec)
 
-    def step(flags):
-        prods = [G.FunctionTree(m) for _ in pairs]
+    # trees allocated once and reused every step, as a caller iterating the exchange would: products are
+    # emptied before each multiply (a non-empty output would be its starting grid), potentials restart
+    # from their roots in the apply
+    prods = [G.FunctionTree(m) for _ in pairs]
+    half = (len(pairs) + 1) // 2
+
+    def step(flags, outs):
+        for p in prods:
+            G.clear(p)
         G.multiply_batched(args.prec, prods, None, [phis[i] for i, _ in pairs], [phis[j] for _, j in pairs])
-        outs = [G.FunctionTree(m) for _ in pairs]
-        half = (len(pairs) + 1) // 2
         for a in range(0, len(pairs), half):
             G.apply_batched(args.prec, outs[a:a + half], [P] * len(outs[a:a + half]), prods[a:a + half], flags)
         return prods, outs
 
     res = {}
     for name, flags in (("fp64", G.APPLY_FP64), ("mixed", G.APPLY_FP32), ("tf32x3", G.APPLY_TF32X3)):
+        leg_outs = [G.FunctionTree(m) for _ in pairs]
         for _ in range(args.warmup):
-            step(flags)
+            step(flags, leg_outs)
         torch.cuda.synchronize()
         ctx.profile(True)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         for _ in range(args.steps):
-            prods, outs = step(flags)
+            prods, outs = step(flags, leg_outs)
         ev1.record(stream)
         torch.cuda.synchronize()
         ms = ev0.elapsed_time(ev1) / args.steps
