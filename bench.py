@@ -46,8 +46,6 @@ def parse():
     p.add_argument("--cpu-sample-seconds", type=float, default=12.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--tau", type=float, default=0.99, help="proposal threshold of the learned apply")
-    p.add_argument("--e2e-workers", type=int, default=3,
-                   help="host threads (one context and stream each) sharing the batch in the e2e measurement")
     p.add_argument("--reserve-gib", type=int, default=64,
                    help="device memory pool reserved up front (GiB): the working set of the step")
     p.add_argument("--workload", default="helmholtz", choices=["helmholtz", "exchange", "density_sweep"],
@@ -337,12 +335,7 @@ def run_gpu(args):
 
     # end to end through the public API from host buffers: every step uploads the input trees from
     # pinned host memory, applies, and downloads the output trees into pinned host memory (buffers
-    # allocated once, as a caller that streams batches would).  The batch is served by several workers,
-    # each a host thread with its own context (stream), operators and copy of the network, taking
-    # a share of the orbitals (--e2e-workers, default 3): one worker's transfers overlap another's
-    # compute (the library releases the interpreter lock in every call).
-    import threading
-
+    # allocated once, as a caller that streams batches would)
     def pinned(shape, dtype):
         return torch.empty(shape, dtype=dtype, pin_memory=True).numpy()
 
@@ -362,89 +355,133 @@ def run_gpu(args):
         out_bufs.append({"depth": pinned((cap,), torch.int32), "parent": pinned((cap,), torch.int32),
                          "child0": pinned((cap,), torch.int32), "trans": pinned((3 * cap,), torch.int64),
                          "coef": pinned((cap * bs_k,), torch.float64)})
-    n_e2e = max(1, min(args.steps, 3))
+    n_e2e = min(16, max(8, args.steps))  # a stream of batches: pipeline fill and drain amortised over 8+ steps
     h2d = sum(sum(v.nbytes for v in h.values()) for h in host)
     node_bytes = 4 + 24 + 4 + 4 + 8 * bs_k
-    net_params = net.params()
-    nw = max(1, min(args.e2e_workers, args.orbitals))
-    halves = [list(range(args.orbitals * q // nw, args.orbitals * (q + 1) // nw)) for q in range(nw)]
+    nb = args.orbitals
 
-    class Worker:
-        def __init__(self, idx):
-            self.idx = idx
-            self.stream = torch.cuda.Stream()
-            self.ctx = G.Context(local, stream=self.stream.cuda_stream)
-            self.m = G.MultiResolutionAnalysis(W.WORLD["min_scale"], W.WORLD["corner"], W.WORLD["boxes"], args.order,
-                                               15, ctx=self.ctx)
-            self.ctx.set_chunk_triples(G.APPLY_FP32, ctx.chunk_triples(G.APPLY_FP32))
-            self.net = G.ProposalNet(ctx=self.ctx, hidden_layers=3, width=128, seed=5)
-            self.net.set_params(net_params)
-            self.ops = [G.HelmholtzOperator(self.m, mus[i], args.prec) for i in idx]
-            self.e_in = [G.FunctionTree(self.m) for _ in idx]
-            self.e_out = [G.FunctionTree(self.m) for _ in idx]
-            self.d2h = 0
-            self.err = None
+    # Pipeline of three host threads (the library releases the interpreter lock in every call):
+    #   upload:   pinned host -> staging input trees of a side context (stream), double-buffered;
+    #   compute:  staging inputs -> the compute context's trees (device copy, mw_tree_assign), the
+    #             learned apply of the whole batch, outputs -> staging output trees (device copy);
+    #   download: staging outputs -> pinned host, on the side contexts of the output buffers.
+    # Step i's uploads and step i-1's downloads overlap step i's compute.
+    import queue
+    import threading
 
-        def upload(self):
-            for j, i in enumerate(self.idx):
-                h = host[i]
-                self.e_in[j].load(h["depth"], h["trans"], h["parent"], h["child0"], h["coef"])
+    def side_world():
+        # high priority: the transfers' small kernels (hash index, norms) are scheduled ahead of the
+        # pending CTAs of the compute stream's long contraction launches
+        st = torch.cuda.Stream(priority=-1)
+        c = G.Context(local, stream=st.cuda_stream)
+        w = G.MultiResolutionAnalysis(W.WORLD["min_scale"], W.WORLD["corner"], W.WORLD["boxes"], args.order, 15,
+                                      ctx=c)
+        return st, c, w
 
-        def step(self, uploaded=None):
-            self.d2h = 0
-            self.upload()
-            if uploaded is not None:
-                uploaded.set()
-            G.apply_learned(args.prec, self.e_out, self.ops, self.e_in, self.net, tau=args.tau, flags=G.APPLY_FP32)
-            for j, i in enumerate(self.idx):
-                self.d2h += self.e_out[j].export_into(out_bufs[i]) * node_bytes
+    # one side context per staging buffer: a buffer's stream is idle whenever its trees are handed
+    # over (mw_tree_assign waits for the source's stream and its own), so the threads never wait on
+    # each other's transfers in flight
+    ups = [side_world() for _ in range(2)]
+    dns = [side_world() for _ in range(2)]
+    stage_in = [[G.FunctionTree(ups[q][2]) for _ in range(nb)] for q in range(2)]
+    stage_out = [[G.FunctionTree(dns[q][2]) for _ in range(nb)] for q in range(2)]
+    c_in = [G.FunctionTree(m) for _ in range(nb)]
+    c_out = [G.FunctionTree(m) for _ in range(nb)]
 
-        def run(self, steps, gate, after=None, signal=None):
-            try:
-                gate.wait()
-                if after is not None:  # staggered: start uploading while the other worker computes
-                    after.wait()
-                for q in range(steps):
-                    self.step(signal if q == 0 else None)
-            except Exception as exc:  # reported by the main thread
-                if signal is not None:
-                    signal.set()
-                self.err = exc
+    def upload(q):
+        for i in range(nb):
+            h = host[i]
+            stage_in[q][i].load(h["depth"], h["trans"], h["parent"], h["child0"], h["coef"])
 
-    workers = [Worker(idx) for idx in halves]
-    for wk in workers:  # untimed: operator tables of every depth, pool growth
-        wk.step()
+    def compute(q):
+        for i in range(nb):
+            c_in[i].assign(stage_in[q][i])
+
+    def apply_and_stage(q):
+        G.apply_learned(args.prec, c_out, ops, c_in, net, tau=args.tau, flags=G.APPLY_FP32)
+        for i in range(nb):
+            stage_out[q][i].assign(c_out[i])
+
+    def download(q):
+        d = 0
+        for i in range(nb):
+            d += stage_out[q][i].export_into(out_bufs[i]) * node_bytes
+        return d
+
+    # untimed pass through every stage (staging trees grow to size)
+    for q in (0, 1):
+        upload(q)
+        compute(q)
+        apply_and_stage(q)
+        download(q)
     torch.cuda.synchronize()
-    gate = threading.Barrier(len(workers) + 1)
-    # worker q starts after worker q-1's first upload: the workers' transfers and computes interleave
-    uploaded = [threading.Event() for _ in workers]
-    threads = [threading.Thread(target=wk.run, args=(n_e2e, gate, uploaded[q - 1] if q > 0 else None, uploaded[q]))
-               for q, wk in enumerate(workers)]
-    for th in threads:
-        th.start()
+
+    free_in = [threading.Semaphore(1) for _ in range(2)]
+    free_out = [threading.Semaphore(1) for _ in range(2)]
+    ready_in, ready_out = queue.Queue(), queue.Queue()
+    errs, d2h_steps = [], []
+
+    def guard(fn):
+        def run():
+            try:
+                fn()
+            except Exception as exc:  # reported by the main thread; unblock the others
+                errs.append(exc)
+                ready_in.put(None)
+                ready_out.put(None)
+        return run
+
+    def uploader():
+        for step_i in range(n_e2e):
+            q = step_i % 2
+            free_in[q].acquire()
+            upload(q)
+            ready_in.put(step_i)
+
+    def computer():
+        for _ in range(n_e2e):
+            step_i = ready_in.get()
+            if step_i is None:
+                return
+            q = step_i % 2
+            compute(q)
+            free_in[q].release()
+            free_out[q].acquire()
+            apply_and_stage(q)
+            ready_out.put(step_i)
+
+    def downloader():
+        for _ in range(n_e2e):
+            step_i = ready_out.get()
+            if step_i is None:
+                return
+            q = step_i % 2
+            d2h_steps.append(download(q))
+            free_out[q].release()
+
+    threads = [threading.Thread(target=guard(f)) for f in (uploader, computer, downloader)]
     barrier()
     torch.cuda.synchronize()
     gc.collect()
     gc.disable()
-    gate.wait()
     t0 = time.perf_counter()
+    for th in threads:
+        th.start()
     for th in threads:
         th.join()
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     gc.enable()
-    for wk in workers:
-        if wk.err is not None:
-            raise wk.err
-    d2h = sum(wk.d2h for wk in workers)
+    if errs:
+        raise errs[0]
+    d2h = d2h_steps[-1]
     # the e2e outputs equal the headline outputs (same inputs, same network)
     e2e_same = True
-    for wk in workers:
-        for j, i in enumerate(wk.idx):
-            ex = outsL[i].export()
-            nn = wk.e_out[j].nnodes()
-            e2e_same &= nn == outsL[i].nnodes() and np.array_equal(out_bufs[i]["depth"][:nn], ex["depth"]) and \
-                np.array_equal(out_bufs[i]["coef"][:nn * bs_k], ex["coef"].ravel())
+    for i in range(nb):
+        ex = outsL[i].export()
+        nn = c_out[i].nnodes()
+        e2e_same &= nn == outsL[i].nnodes() and np.array_equal(out_bufs[i]["depth"][:nn], ex["depth"]) and \
+            np.array_equal(out_bufs[i]["coef"][:nn * bs_k], ex["coef"].ravel())
     e2e_s = max_over_ranks(e2e_s, device=f"cuda:{local}")
     e2e_val = args.orbitals * n_e2e * world / e2e_s
 
@@ -478,10 +515,10 @@ def run_gpu(args):
                        "l2": f"inputs larger than L2 ({in_bytes / 1e9:.2f} GB of input blocks per step)"},
             "e2e": {"value": e2e_val, "unit": "applies/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "host_memory": "pinned, allocated once",
-                    "path": "per step: mw_tree_upload x32, mw_apply_learned, mw_tree_download x32; the batch split "
-                            "over workers (host threads, one context and stream each), each starting after the "
-                            "previous one's upload so that the transfers of one overlap the compute of another",
-                    "workers": nw,
+                    "path": "per step: mw_tree_upload x32 (upload thread, own context), mw_tree_assign x32 (device "
+                            "copy into the compute context), mw_apply_learned, mw_tree_assign x32 (device copy out), "
+                            "mw_tree_download x32 (download thread, own context); double-buffered staging trees, "
+                            "so a step's transfers overlap the previous and next steps' compute",
                     "steps": n_e2e,
                     "outputs_equal_headline": bool(e2e_same)},
             "plain_fp64": {"value": args.orbitals * args.steps * world / (ms64 / 1e3), "unit": "applies/s",

@@ -89,6 +89,12 @@ int mw_tree_upload(mw_tree tree, int n, const int* depth, const long long* trans
                    const int* child0, const double* coef);
 /* copy the device tree to host buffers sized with mw_tree_nnodes (any pointer may be NULL) */
 int mw_tree_download(mw_tree tree, int* depth, long long* trans, int* parent, int* child0, double* coef);
+/* dst = a deep copy of src (structure, coefficients, norms), device to device.  The two trees may
+ * belong to different contexts (streams) of the same device, on worlds with the same parameters: a
+ * thread that streams trees to or from the host on its own context hands them to the context that
+ * computes without a host round trip.  Blocking: returns when dst is complete and src may change.
+ * No reference counterpart (MRCPP's FunctionTree copy stays in host memory). */
+int mw_tree_assign(mw_tree dst, mw_tree src);
 /* device pointers of the node arrays (coef: n*(2k)^3 doubles, key: n uint64, norm2: n doubles) */
 int mw_tree_device_arrays(mw_tree tree, void** coef, void** key, void** norm2);
 /* Flat byte image of a tree: a 64-byte header (magic "MWB2TREE", format version, k, basis type, root

@@ -1306,6 +1306,41 @@ int mw_tree_upload(mw_tree t, int n, const int* depth, const long long* trans, c
     })
 }
 
+int mw_tree_assign(mw_tree dst, mw_tree src) {
+    MW_TRY({
+        MW_ARG(dst && src, "null tree");
+        MW_ARG(dst != src, "a tree cannot be assigned to itself");
+        const Mra& a = *dst->mra;
+        const Mra& b = *src->mra;
+        bool same = a.ctx->device == b.ctx->device && a.k == b.k && a.basis.type == b.basis.type && a.n0 == b.n0 &&
+                    a.max_depth == b.max_depth;
+        for (int d = 0; d < 3; ++d) same = same && a.corner[d] == b.corner[d] && a.boxes[d] == b.boxes[d];
+        MW_ARG(same, "trees on worlds with different parameters or devices");
+        MWB_CUDA(cudaSetDevice(a.ctx->device));
+        MWB_CUDA(cudaStreamSynchronize(b.ctx->stream));  // src complete before it is read on dst's stream
+        cudaStream_t s = a.ctx->stream;
+        dst->n = 0;
+        tree_reserve(*dst, src->n);
+        const size_t n = (size_t)src->n, BS = a.bsize();
+        if (n > 0) {
+            MWB_CUDA(cudaMemcpyAsync(dst->key, src->key, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, s));
+            MWB_CUDA(cudaMemcpyAsync(dst->parent, src->parent, sizeof(int) * n, cudaMemcpyDeviceToDevice, s));
+            MWB_CUDA(cudaMemcpyAsync(dst->child0, src->child0, sizeof(int) * n, cudaMemcpyDeviceToDevice, s));
+            MWB_CUDA(cudaMemcpyAsync(dst->coef, src->coef, sizeof(double) * BS * n, cudaMemcpyDeviceToDevice, s));
+            MWB_CUDA(cudaMemcpyAsync(dst->norm2, src->norm2, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+            MWB_CUDA(cudaMemcpyAsync(dst->wnorm2, src->wnorm2, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        }
+        dst->n = src->n;
+        dst->level_begin = src->level_begin;
+        dst->g0 = src->g0;
+        dst->prec = src->prec;
+        for (int q = 0; q < 8; ++q) dst->stats[q] = src->stats[q];
+        launch_hash_reset(*dst, s);
+        launch_hash_insert(*dst, 0, dst->n, s);
+        MWB_CUDA(cudaStreamSynchronize(s));  // src may change as soon as this returns
+    })
+}
+
 int mw_tree_download(mw_tree t, int* depth, long long* trans, int* parent, int* child0, double* coef) {
     MW_TRY({
         MW_ARG(t, "null tree");

@@ -48,6 +48,7 @@ SYMBOLS = [
     ("mw_ctx_destroy", ctypes.c_int, [_vp]),
     ("mw_ctx_synchronize", ctypes.c_int, [_vp]),
     ("mw_ctx_reserve", ctypes.c_int, [_vp, ctypes.c_ulonglong]),
+    ("mw_tree_assign", ctypes.c_int, [_vp, _vp]),
     ("mw_ctx_set_chunk_triples", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
     ("mw_ctx_get_chunk_triples", ctypes.c_int, [_vp, ctypes.c_int, _ip]),
     ("mw_ctx_profile", ctypes.c_int, [_vp, ctypes.c_int]),
@@ -288,6 +289,11 @@ class FunctionTree:
     def load_tree(self, path):
         """FunctionTree::loadTree (reference src/qmfunctions/Orbital.cpp:170)"""
         _check(_lib.mw_tree_load(self._h, os.fsencode(path)))
+
+    def assign(self, src):
+        """self = a deep copy of `src`, device to device; `src` may live in another context (stream) of the
+        same device, on a world with the same parameters (see mw_tree_assign).  Blocking."""
+        _check(_lib.mw_tree_assign(self._h, src._h))
 
     def export_into(self, bufs):
         """Download into caller-owned arrays (e.g. pinned host memory reused across calls): `bufs` has
