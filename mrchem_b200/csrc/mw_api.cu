@@ -447,6 +447,28 @@ static const OpDepth& op_depth(Op& op, int depth, int dir = 0) {
         for (int q = 0; q < 2 * bs[mi].L + 1; ++q) mbeta[base[mi] + q] = op.terms[mi].beta;
     }
     }
+    // line ranks: the contraction groups an output node's triples by (term, dz, dy) (sort key bits:
+    // term << 20 | dz rank << 10 | dy rank), so that the triples of one line share their y and z steps
+    {
+        std::vector<int> zs, ys;
+        for (const DeltaRec& d : od->deltas) {
+            zs.push_back(d.d[2]);
+            ys.push_back(d.d[1]);
+        }
+        for (auto* v : {&zs, &ys}) {
+            std::sort(v->begin(), v->end());
+            v->erase(std::unique(v->begin(), v->end()), v->end());
+        }
+        if (zs.size() > 1024 || ys.size() > 1024)
+            throw Error(MW_ERR_CAPACITY, "operator band wider than 1024 offsets per direction");
+        for (DeltaRec& d : od->deltas) {
+            const int rz = (int)(std::lower_bound(zs.begin(), zs.end(), d.d[2]) - zs.begin());
+            const int ry = (int)(std::lower_bound(ys.begin(), ys.end(), d.d[1]) - ys.begin());
+            d.lrank = (rz << 10) | ry;
+        }
+        for (const TermRec& t : od->terms)
+            if (t.m < 0 || t.m >= 4096) throw Error(MW_ERR_CAPACITY, "more than 4096 operator terms");
+    }
     Ctx* ctx = m.ctx;
     cudaStream_t s = ctx->stream;
     od->d_mats = (double*)dalloc(ctx, sizeof(double) * std::max<size_t>(1, od->mats.size()));

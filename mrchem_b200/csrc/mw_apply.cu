@@ -56,6 +56,10 @@ struct BTree {
     int depth;   // depth of this entry's output nodes
     int depth_limit;
     long long ext[3];
+    // block images of the pass (line-ordered contraction): input node i of this entry's depth has
+    // image slot img_base + i - img_lb, for i in [img_lb, img_le)
+    long long img_base;
+    int img_lb, img_le;
 };
 
 struct Item {
@@ -290,6 +294,100 @@ __global__ void k_multi_slots(const int* __restrict__ nchunk, int nitems, int* n
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= nitems) return;
     nslot[w] = nchunk[w] > 1 ? nchunk[w] : 0;
+}
+// triples of the line-ordered contraction: candidate c contributes its first ntrip[c] term entries,
+// at positions toff[c] ..; key = item << 32 | term << 20 | line rank (dz rank << 10 | dy rank),
+// value = candidate << 32 | term entry.  A stable sort by key then groups every output node's
+// triples by (term, dz, dy), in candidate order inside a line.
+__global__ void k_texpand(const int* __restrict__ cand_item, int ncand, const Item* __restrict__ items,
+                          const BTree* __restrict__ trees, const int* __restrict__ cdelta,
+                          const int* __restrict__ ntrip, const int* __restrict__ toff,
+                          const int* __restrict__ csrc, unsigned long long* key, unsigned long long* val, int* err) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncand) return;
+    const int w = cand_item[c];
+    const BTree& T = trees[items[w].tree];
+    const DeltaRec de = T.deltas[cdelta[c]];
+    const int n = ntrip[c], p0 = toff[c];
+    const int src = csrc[c];
+    if (n > 0 && src >= 0 && (src < T.img_lb || src >= T.img_le)) {  // not a node of this depth's level range
+        atomicOr(err, 1);
+        return;
+    }
+    for (int j = 0; j < n; ++j) {
+        const int te = de.t0 + j;
+        key[p0 + j] = ((unsigned long long)w << 32) | ((unsigned long long)T.terms[te].m << 20) | (unsigned)de.lrank;
+        val[p0 + j] = ((unsigned long long)c << 32) | (unsigned)te;
+    }
+}
+// greedy cut of each node's sorted triples into chunks of about `limit` triples, at plane
+// boundaries (a plane = the triples of one (term, dz); at least one chunk per node)
+__global__ void k_tchunks(const int* __restrict__ offs, const int* __restrict__ toff, int nitems,
+                          const unsigned long long* __restrict__ key, int limit, int fill, int* nchunk,
+                          const int* __restrict__ choff, const int* __restrict__ slotoff, Chunk* chunks) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= nitems) return;
+    const int t0 = toff[offs[w]], t1 = toff[offs[w + 1]];
+    int nch = 0, acc = 0, start = t0;
+    const int multi = fill ? (choff[w + 1] - choff[w] > 1) : 0;
+    int t = t0;
+    while (t < t1) {
+        const uint32_t plane = (uint32_t)(key[t] & 0xffffffffull) >> 10;
+        int e = t + 1;
+        while (e < t1 && ((uint32_t)(key[e] & 0xffffffffull) >> 10) == plane) ++e;
+        if (acc > 0 && acc + (e - t) > limit) {
+            if (fill) chunks[choff[w] + nch] = Chunk{w, start, t, multi ? slotoff[w] + nch : -1};
+            ++nch;
+            acc = 0;
+            start = t;
+        }
+        acc += e - t;
+        t = e;
+    }
+    if (fill) chunks[choff[w] + nch] = Chunk{w, start, t1, multi ? slotoff[w] + nch : -1};
+    ++nch;
+    if (!fill) nchunk[w] = nch;
+}
+// Block images for the line-ordered contraction: image row a (a < 2k) holds X[a][b + P c] of the
+// node block (P = 2k rounded up to 4; zero where b or c >= 2k), so that a CTA stages a block with
+// 16-byte copies.  One CTA per block: read coalesced into shared memory, write the rows coalesced.
+// Real nodes: entry e (a tree of the pass) contributes input nodes [lb[e], lb[e] + cnt[e]) at slots
+// base[e] ..; generated nodes (k^3 scaling blocks) take slots gbase ...
+struct ImgSrc {
+    const double* coef;
+    long long base;
+    int lb, cnt;
+};
+template <int K, typename R>
+__global__ void __launch_bounds__(256) k_ximage(const ImgSrc* __restrict__ srcs, int nsrc, const double* __restrict__ gblk,
+                                                long long nreal, R* __restrict__ img) {
+    constexpr int K2 = 2 * K, KP = (K2 + 3) / 4 * 4, NN = KP * KP, BS = K2 * K2 * K2, KKK = K * K * K;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    R* blk = reinterpret_cast<R*>(smraw);
+    const long long slot = blockIdx.x;
+    if (slot < nreal) {
+        int lo = 0, hi = nsrc - 1;  // last entry with base <= slot
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (srcs[mid].base <= slot) lo = mid;
+            else hi = mid - 1;
+        }
+        const ImgSrc sr = srcs[lo];
+        const double* b = sr.coef + (size_t)(sr.lb + (slot - sr.base)) * BS;
+        for (int e = threadIdx.x; e < BS; e += blockDim.x) blk[e] = (R)b[e];
+    } else {
+        const double* g = gblk + (size_t)(slot - nreal) * KKK;
+        for (int e = threadIdx.x; e < BS; e += blockDim.x) {
+            const int a = e % K2, bb = (e / K2) % K2, c = e / (K2 * K2);
+            blk[e] = (a < K && bb < K && c < K) ? (R)g[a + K * (bb + K * c)] : R(0);
+        }
+    }
+    __syncthreads();
+    R* out = img + (size_t)slot * K2 * NN;
+    for (int e = threadIdx.x; e < K2 * NN; e += blockDim.x) {
+        const int a = e / NN, j = e - a * NN, b = j % KP, c = j / KP;
+        out[e] = (b < K2 && c < K2) ? blk[a + K2 * (b + K2 * c)] : R(0);
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -626,7 +724,7 @@ __host__ __device__ constexpr int gcfg_nc(int k, int nthr) {
 // so that the epilogue stores of a warp fall into distinct banks (counted wavefronts per step,
 // consecutive column tiles per warp; the FP64 x step with an odd tile width uses strided tiles).
 __host__ __device__ constexpr int gcfg_pad1(int k, bool f32) {
-    return f32 ? ((k == 5 || k == 6 || k == 9 || k == 10) ? 8 : (k == 11 || k == 12) ? 4 : 0) : 0;
+    return f32 ? ((k == 5 || k == 6 || k == 9 || k == 10 || k == 11 || k == 12) ? 4 : 0) : 0;
 }
 __host__ __device__ constexpr int gcfg_pad2(int k) {
     return (k == 5 || k == 6 || k == 9 || k == 10) ? 0 : (k == 11 || k == 12) ? 8 : 2;
@@ -640,7 +738,7 @@ struct GCfg {
     static constexpr int NN = KP * KP;
     static constexpr int MT = KP / 4;
     static constexpr int NT = (F32 && MT * (KP / 2) <= 50) ? KP / 2 : KP / 4;
-    static constexpr int LDX = NN + 2;
+    static constexpr int LDX = NN + (F32 ? 4 : 2);  // 16-byte rows: staged by cp.async from the block images
     static constexpr int LD1 = NN + gcfg_pad1(K, F32);
     static constexpr int LD2 = NN + gcfg_pad2(K);
     static constexpr bool XSTRIDED = !F32 && (NT % 2 == 1);
@@ -656,8 +754,10 @@ struct GCfg {
     static constexpr int TCOLS_NEED = ((NWARP + 3) / 4) * 2 * ND;
     static constexpr int TCOLS = TCOLS_NEED <= 32 ? 32 : TCOLS_NEED <= 64 ? 64 : TCOLS_NEED <= 128 ? 128
                                  : TCOLS_NEED <= 256 ? 256 : 512;
+    static constexpr int XBUF = KP * (LDX > LD1 ? LDX : LD1);  // one staging buffer: X, or T1 at a line's end
+    static constexpr int IMG = K2 * NN;                          // block image: rows a < 2k of X, unpadded
     static constexpr size_t SMEM =
-        sizeof(R) * ((size_t)KP * (LDX + LD1 + LD2) + 3 * (size_t)KP * KP + 3 * (size_t)KKK) + 64;
+        sizeof(R) * (2 * (size_t)XBUF + (size_t)KP * LD2 + 4 * (size_t)KP * KP + 3 * (size_t)KKK) + 64;
     static constexpr int MINB = (F32 && 2 * (SMEM + 16 + 1024) <= 233472) ? 2 : 1;
     static constexpr bool FITS = SMEM + 16 + 1024 <= 232448 && 2 * NCT <= NTHR && TCOLS_NEED <= 512 &&
                                  (size_t)KP * LDX * sizeof(R) >= 64 * sizeof(double) && (!F32 || TCOLS * MINB <= 512);
@@ -751,6 +851,29 @@ __device__ __forceinline__ void gemm_tile(const R* __restrict__ At, int lda, con
     }
 }
 
+// FP32 tile with packed accumulators kept across calls: pc[i][j] (+)= sum_k At[k lda + o0 + i] times the
+// column pair B[k ldb + n0 + 2j], B[k ldb + n0 + 2j + 1] (the same FMAs as gemm_tile's FP32 path)
+template <int MT, int NP>
+__device__ __forceinline__ void gemm_tile_packed(const float* __restrict__ At, int lda, const float* __restrict__ B,
+                                                 int ldb, int o0, int n0, int kdim, unsigned long long (&pc)[MT][NP]) {
+    const float* ap = At + o0;
+    const float* bp = B + n0;
+#pragma unroll 2
+    for (int k = 0; k < kdim; ++k) {
+        unsigned long long a2[MT], b2[NP];
+#pragma unroll
+        for (int i = 0; i < MT; ++i) a2[i] = pack_f32x2(ap[i], ap[i]);
+#pragma unroll
+        for (int j = 0; j < NP; ++j) b2[j] = *reinterpret_cast<const unsigned long long*>(bp + 2 * j);
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NP; ++j) pc[i][j] = fma_f32x2(a2[i], b2[j], pc[i][j]);
+        ap += lda;
+        bp += ldb;
+    }
+}
+
 // the same with per-column offsets (correction GEMMs; columns not contiguous)
 template <int MT, int NT, typename R>
 __device__ __forceinline__ void gemm_tile_off(const R* __restrict__ At, int lda, const R* __restrict__ B, int ldb,
@@ -772,23 +895,37 @@ __device__ __forceinline__ void gemm_tile_off(const R* __restrict__ At, int lda,
     }
 }
 
+// Line-ordered GEMM-tiled contraction.  A chunk is a range of one output node's surviving triples,
+// sorted by (term, dz, dy): a *line* is a run of triples with the same (term, dz, dy) and a *plane* a
+// run with the same (term, dz).  Because a term's operator is separable,
+//   sum_l  Mz(dz) My(dy) Mx(dx) in_l  =  sum_dz Mz(dz) [ sum_dy My(dy) [ sum_dx Mx(dx) in_l ] ],
+// so every triple costs one x mode product (summed over its line in registers), every line one y mode
+// product (summed over its plane in T2) and every plane one z mode product (summed into the output
+// block), instead of three mode products per triple.  The s->s correction below the root follows the
+// same grouping on its k^3 blocks.
+// Input blocks are staged from their images (the X layout in `R`, built per pass) into two buffers
+// by cp.async: the next triple's block and operator load while the current triple computes.  At a
+// line's end its x sums (T1) replace the line's last block in its buffer.
+// tkey (sorted): item << 32 | term << 20 | dz rank << 10 | dy rank; tval: candidate << 32 | term entry.
 template <int K, typename R>
 __global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
     k_gapply(const Chunk* __restrict__ chunks, const Item* __restrict__ items, const BTree* __restrict__ trees,
-             const int* __restrict__ cdelta, const int* __restrict__ csrc, const double* __restrict__ gblk,
-             const double* __restrict__ gnorm2, double* partials, unsigned long long* ntrip_out) {
+             const unsigned long long* __restrict__ tkey, const unsigned long long* __restrict__ tval,
+             const int* __restrict__ csrc, const R* __restrict__ ximg, long long gbase, double* partials,
+             unsigned long long* ntrip_out) {
     using C = GCfg<K, R>;
     constexpr int K2 = C::K2, KP = C::KP, MT = C::MT, NT = C::NT, NC = C::NC, ND = C::ND;
-    constexpr int LDX = C::LDX, LD1 = C::LD1, LD2 = C::LD2;
+    constexpr int LDX = C::LDX, LD1 = C::LD1, LD2 = C::LD2, NN = C::NN, IMG = C::IMG;
     constexpr int KK = C::KK, KKK = C::KKK;
     constexpr int BS = K2 * K2 * K2;
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ uint32_t tmem_slot;
-    R* X = reinterpret_cast<R*>(smraw);  // [KP][LDX]
-    R* T1 = X + KP * LDX;                // [KP][LD1]
-    R* T2 = T1 + KP * LD1;               // [KP][LD2]
-    R* Mx = T2 + KP * LD2;               // [KP][KP], At[k][o] = M[o][k]
-    R* My = Mx + KP * KP;
+    R* XA = reinterpret_cast<R*>(smraw);  // staging buffers: X [KP][LDX], or T1 [KP][LD1]
+    R* XB = XA + C::XBUF;
+    R* T2 = XB + C::XBUF;                 // [KP][LD2]
+    R* Mx0 = T2 + KP * LD2;               // [KP][KP], At[k][o] = M[o][k]; x operators of the two buffers
+    R* Mx1 = Mx0 + KP * KP;
+    R* My = Mx1 + KP * KP;
     R* Mz = My + KP * KP;
     R* U1 = Mz + KP * KP;  // [K][K][K]
     R* U2 = U1 + KKK;
@@ -799,7 +936,6 @@ __global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
     const R* mats = reinterpret_cast<const R*>(C::F32 ? (const void*)TR.matsT32 : (const void*)TR.matsT);
     const R* matsb = reinterpret_cast<const R*>(C::F32 ? (const void*)TR.matsbT32 : (const void*)TR.matsbT);
     const bool root = TR.root != 0;
-    const double theta = TR.theta;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // tiles: 4 row tiles x 8 column tiles per warp; consecutive column tiles (y and z steps, and the
     // x step unless strided), or column tiles strided by the warp count (x step)
@@ -842,15 +978,36 @@ __global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
     bool pend2 = false;     // c2 holds a correction block not yet written to Uc
     bool uc_valid = false;  // Uc holds a correction block not yet subtracted
     R c2[MT][NC];
+    // x sums of the current line (this thread's x tile): FP32 column pairs packed (f32x2), or plain
+    constexpr bool PK = C::F32 && NT % 2 == 0;
+    unsigned long long xp[PK ? MT : 1][PK ? NT / 2 : 1];
+    R xacc[PK ? 1 : MT][PK ? 1 : NT];
 
-    // asynchronous copy of a transposed operator (At[k][o] = M[o][k], P x P) into shared memory; the
-    // copies a thread issued are complete at its next cp_async_wait_all(), which precedes every
-    // barrier that publishes an operator
+    // asynchronous copy of a transposed operator (At[k][o] = M[o][k], P x P) into shared memory, as
+    // one commit group
     auto load_mat = [&](R* dst, const R* tab, int mi) {
         constexpr int NV = KP * KP * (int)sizeof(R) / 16;
         const char* src = reinterpret_cast<const char*>(tab + (size_t)mi * KP * KP);
         for (int e = tid; e < NV; e += blockDim.x) cp_async16(reinterpret_cast<char*>(dst) + 16 * e, src + 16 * e);
         cp_async_commit();
+    };
+    auto image_of = [&](int t) -> const R* {
+        const int src = csrc[(int)(tval[t] >> 32)];
+        const long long slot = src < 0 ? gbase + (-src - 1) : TR.img_base + (src - TR.img_lb);
+        return ximg + (size_t)slot * IMG;
+    };
+    // triple t's block image into buffer q (rows a < 2k; the rows of X beyond are never read) and its
+    // x operator, one commit group
+    auto stage = [&](int t, int q) {
+        const R* img = image_of(t);
+        R* dst = q ? XB : XA;
+        constexpr int RV = NN * (int)sizeof(R) / 16;  // 16-byte vectors per row
+        constexpr int EV = 16 / (int)sizeof(R);
+        for (int e = tid; e < K2 * RV; e += blockDim.x) {
+            const int a = e / RV, v = e - a * RV;
+            cp_async16(dst + a * LDX + v * EV, img + (size_t)a * NN + v * EV);
+        }
+        load_mat(q ? Mx1 : Mx0, mats, TR.terms[(int)(tval[t] & 0xffffffffull)].mx);
     };
     // correction block of element (c', a', b') of this thread's z tile, 0 outside s->s
     auto uc_at = [&](int i, int j) -> double {
@@ -865,86 +1022,123 @@ __global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
             for (int j = 0; j < NC; ++j)
                 if (co0 + i < K) Uc[(co0 + i) * KK + cn0 + j] = c2[i][j];
     };
-    if (KP > K2) {  // padding rows/columns of X stay zero for the whole kernel
-        for (int e = tid; e < KP * LDX; e += blockDim.x) X[e] = R(0);
-    }
 
-    for (int ci = ch.c0; ci < ch.c1; ++ci) {
-        const int src = csrc[ci];
-        const bool gen = src < 0;
-        const double nu = gen ? sqrt(gnorm2[-src - 1]) : sqrt(TR.in.norm2[src]);
-        const DeltaRec de = TR.deltas[cdelta[ci]];
-        if (!(nu > 0.0) || de.maxb * nu < theta) continue;
-        if (TR.terms[de.t0].bound * nu < theta) continue;
-        if (tid == 0 && ci + 1 < ch.c1) {  // the next candidate's block: into L2 while this one runs
-            const int s1 = csrc[ci + 1];
-            if (s1 < 0) prefetch_l2_bulk(gblk + (size_t)(-s1 - 1) * KKK, (unsigned)(KKK * sizeof(double)));
-            else prefetch_l2_bulk(TR.in.coef + (size_t)s1 * BS, (unsigned)(BS * sizeof(double)));
+    auto line_of = [&](int t) -> uint32_t { return (uint32_t)(tkey[t] & 0xffffffffull); };
+    bool line_gen = true;    // every triple of the current line has a generated (scaling-only) input
+    bool plane_gen = true;   // ... of the current plane
+    bool first_line = true;  // the current line is the first of its plane
+    if (ch.c0 < ch.c1) stage(ch.c0, 0);
+    int q = 0;  // buffer of the current triple
+    for (int t = ch.c0; t < ch.c1; ++t, q ^= 1) {
+        const unsigned long long tv = tval[t];
+        const bool gen = csrc[(int)(tv >> 32)] < 0;
+        const TermRec tr = TR.terms[(int)(tv & 0xffffffffull)];
+        const uint32_t lk = line_of(t);
+        const bool lstart = t == ch.c0 || line_of(t - 1) != lk;
+        const bool pstart = t == ch.c0 || (line_of(t - 1) >> 10) != (lk >> 10);
+        const bool lend = t + 1 == ch.c1 || line_of(t + 1) != lk;
+        const bool pend = t + 1 == ch.c1 || (line_of(t + 1) >> 10) != (lk >> 10);
+        const bool more = t + 1 < ch.c1;
+        if (pstart) {
+            plane_gen = true;
+            first_line = true;
         }
+        if (lstart) line_gen = true;
+        line_gen = line_gen && gen;
+        plane_gen = plane_gen && gen;
         cp_async_wait_all();
-        __syncthreads();  // every reader of X and of the operators of the previous candidate is done
-        if (gen) {
-            const double* blk = gblk + (size_t)(-src - 1) * KKK;
-            for (int e = tid; e < BS; e += blockDim.x) {
-                const int a = e % K2, b = (e / K2) % K2, c = e / (K2 * K2);
-                X[a * LDX + b + KP * c] = (a < K && b < K && c < K) ? (R)blk[a + K * (b + K * c)] : R(0);
-            }
-        } else {
-            const double* blk = TR.in.coef + (size_t)src * BS;
-            for (int e = tid; e < BS; e += blockDim.x) {
-                const int a = e % K2, b = (e / K2) % K2, c = e / (K2 * K2);
-                X[a * LDX + b + KP * c] = (R)blk[e];
+        __syncthreads();  // triple t's block and x operator are in; every reader of the other buffer, of
+                          // My, Mz, T2, U1, U2 and Uc from earlier steps is done
+        if (lend) load_mat(My, mats, tr.my);
+        if (pend) load_mat(Mz, matsb, tr.mz);
+        if (more) stage(t + 1, q ^ 1);
+        if (tid == 0 && t + 2 < ch.c1) prefetch_l2_bulk(image_of(t + 2), (unsigned)(IMG * sizeof(R)));
+        R* Xq = q ? XB : XA;
+        const R* Mxq = q ? Mx1 : Mx0;
+        // ---- x: xacc[a'][b + P c] (+)= sum_a Mx[a'][a] X[a][b + P c]   (a line sums its triples)
+        if (own_x) {
+            const bool live = !gen || (xb0 < K && xc0 < K);  // other tiles of a generated input are zero
+            if constexpr (PK) {
+                if (lstart) {
+#pragma unroll
+                    for (int i = 0; i < MT; ++i)
+#pragma unroll
+                        for (int j = 0; j < NT / 2; ++j) xp[i][j] = 0ull;
+                }
+                if (live)
+                    gemm_tile_packed<MT, NT / 2>(reinterpret_cast<const float*>(Mxq), KP,
+                                                 reinterpret_cast<const float*>(Xq), LDX, o0, n0x, gen ? K : K2, xp);
+            } else {
+                if (lstart) {
+#pragma unroll
+                    for (int i = 0; i < MT; ++i)
+#pragma unroll
+                        for (int j = 0; j < NT; ++j) xacc[i][j] = R(0);
+                }
+                if (live) gemm_tile<MT, NT, true>(Mxq, KP, Xq, LDX, o0, n0x, gen ? K : K2, xacc);
             }
         }
-        {
-            const TermRec t0 = TR.terms[de.t0];
-            load_mat(Mx, mats, t0.mx);
-            load_mat(My, mats, t0.my);
+        if (cown) {  // U1[b][a' + k c] (+)= sum_{a<k} Tx[a'][a] X[a][b + P c]   (summed over the line)
+            int off[NC];
+#pragma unroll
+            for (int j = 0; j < NC; ++j) off[j] = (cn0 + j) % K + KP * ((cn0 + j) / K);
+            R c[MT][NC];
+            gemm_tile_off<MT, NC>(Mxq, KP, Xq, LDX, co0, off, K, c);
+#pragma unroll
+            for (int i = 0; i < MT; ++i)
+#pragma unroll
+                for (int j = 0; j < NC; ++j) {
+                    const int n = cn0 + j;
+                    if (co0 + i < K) {
+                        R& d = U1[(n % K) * KK + co0 + i + K * (n / K)];
+                        d = lstart ? c[i][j] : d + c[i][j];
+                    }
+                }
         }
-        cp_async_wait_all();
-        __syncthreads();
-        const int kd = gen ? K : KP;  // contracted length of every step
-        for (int ti = de.t0; ti < de.t1; ++ti) {
-            const TermRec tr = TR.terms[ti];
-            if (tr.bound * nu < theta) break;
-            const bool has_next = ti + 1 < de.t1 && !(TR.terms[ti + 1].bound * nu < theta);
-            const TermRec tn = has_next ? TR.terms[ti + 1] : tr;
-            // ---- x: T1[b][a' + P c] = sum_a Mx[a'][a] X[a][b + P c]
-            if (own_x && (!gen || (xb0 < K && xc0 < K))) {
-                R c[MT][NT];
-                gemm_tile<MT, NT, false>(Mx, KP, X, LDX, o0, n0x, kd, c);
+        ++ntrip;
+        if (!lend) continue;
+        __syncthreads();  // every reader of Xq is done: the line's x sums replace its last block
+        R* T1 = Xq;       // [KP][LD1]
+        if (own_x) {
+            if constexpr (PK) {
+#pragma unroll
+                for (int j = 0; j < NT / 2; ++j)
+#pragma unroll
+                    for (int i = 0; i < MT; ++i) {
+                        float lo, hi;
+                        unpack_f32x2(xp[i][j], lo, hi);
+                        T1[(xb0 + 2 * j) * LD1 + o0 + i + KP * xc0] = lo;
+                        T1[(xb0 + 2 * j + 1) * LD1 + o0 + i + KP * xc0] = hi;
+                    }
+            } else {
 #pragma unroll
                 for (int j = 0; j < NT; ++j)
 #pragma unroll
-                    for (int i = 0; i < MT; ++i) T1[(xb0 + j) * LD1 + o0 + i + KP * xc0] = c[i][j];
+                    for (int i = 0; i < MT; ++i) T1[(xb0 + j) * LD1 + o0 + i + KP * xc0] = xacc[i][j];
             }
-            if (cown) {  // U1[b][a' + k c] = sum_{a<k} Tx[a'][a] X[a][b + P c]
-                int off[NC];
-#pragma unroll
-                for (int j = 0; j < NC; ++j) off[j] = (cn0 + j) % K + KP * ((cn0 + j) / K);
-                R c[MT][NC];
-                gemm_tile_off<MT, NC>(Mx, KP, X, LDX, co0, off, K, c);
-#pragma unroll
-                for (int i = 0; i < MT; ++i)
-#pragma unroll
-                    for (int j = 0; j < NC; ++j) {
-                        const int n = cn0 + j;
-                        if (co0 + i < K) U1[(n % K) * KK + co0 + i + K * (n / K)] = c[i][j];
-                    }
-            }
-            cp_async_wait_all();
-            __syncthreads();
-            // ---- y: T2[c][a' + P b'] = sum_b My[b'][b] T1[b][a' + P c]
-            if (pend2) {  // the previous term's correction block, subtracted in this term's z phase
-                write_c2();
-                pend2 = false;
-                uc_valid = true;
-            }
-            if (has_next) load_mat(Mx, mats, tn.mx);
-            load_mat(Mz, matsb, tr.mz);
-            if (own && (!gen || tc0 < K)) {
+        }
+        // My (and Mz) were committed before the next triple's staging group
+        if (more) cp_async_wait_group<1>();
+        else cp_async_wait_all();
+        __syncthreads();  // T1, U1, My and Mz are in
+        // ---- y: T2[c][a' + P b'] (+)= sum_b My[b'][b] T1[b][a' + P c]   (a plane sums its lines)
+        if (pend2) {  // the previous plane's correction block, subtracted in this plane's z phase
+            write_c2();
+            pend2 = false;
+            uc_valid = true;
+        }
+        if (own) {
+            const bool zero = line_gen && !(tc0 < K);  // this tile is zero for generated inputs
+            if (!zero || first_line) {
                 R c[MT][NT];
-                gemm_tile<MT, NT, false>(My, KP, T1, LD1, o0, n0, kd, c);
+                if (zero) {
+#pragma unroll
+                    for (int i = 0; i < MT; ++i)
+#pragma unroll
+                        for (int j = 0; j < NT; ++j) c[i][j] = R(0);
+                } else {
+                    gemm_tile<MT, NT, false>(My, KP, T1, LD1, o0, n0, line_gen ? K : K2, c);
+                }
 #pragma unroll
                 for (int i = 0; i < MT; ++i) {
                     R* row = T2 + tc0 * LD2 + tb0 + KP * (o0 + i);
@@ -953,75 +1147,84 @@ __global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
 #pragma unroll
                         for (int j = 0; j < NT; j += 2) {
                             V2 v;
-                            v.x = c[i][j];
-                            v.y = c[i][j + 1];
+                            if (first_line) {
+                                v.x = c[i][j];
+                                v.y = c[i][j + 1];
+                            } else {
+                                v = *reinterpret_cast<const V2*>(row + j);
+                                v.x += c[i][j];
+                                v.y += c[i][j + 1];
+                            }
                             *reinterpret_cast<V2*>(row + j) = v;
                         }
                     } else {
 #pragma unroll
-                        for (int j = 0; j < NT; ++j) row[j] = c[i][j];
+                        for (int j = 0; j < NT; ++j) row[j] = first_line ? c[i][j] : row[j] + c[i][j];
                     }
                 }
             }
-            if (cown) {  // U2[c][a' + k b'] = sum_{b<k} Ty[b'][b] U1[b][a' + k c]
-                int off[NC];
+        }
+        if (cown) {  // U2[c][a' + k b'] (+)= sum_{b<k} Ty[b'][b] U1[b][a' + k c]
+            int off[NC];
 #pragma unroll
-                for (int j = 0; j < NC; ++j) off[j] = cn0 + j;
-                R c[MT][NC];
-                gemm_tile_off<MT, NC>(My, KP, U1, KK, co0, off, K, c);
+            for (int j = 0; j < NC; ++j) off[j] = cn0 + j;
+            R c[MT][NC];
+            gemm_tile_off<MT, NC>(My, KP, U1, KK, co0, off, K, c);
+#pragma unroll
+            for (int i = 0; i < MT; ++i)
+#pragma unroll
+                for (int j = 0; j < NC; ++j) {
+                    const int n = cn0 + j;
+                    if (co0 + i < K) {
+                        R& d = U2[(n / K) * KK + (n % K) + K * (co0 + i)];
+                        d = first_line ? c[i][j] : d + c[i][j];
+                    }
+                }
+        }
+        first_line = false;
+        if (!pend) continue;
+        __syncthreads();  // T2, U2 and Uc of the plane are complete
+        // ---- z: acc[c'][a' + P b'] += sum_c (beta Mz)[c'][c] T2[c][a' + P b']  (- previous correction)
+        const int kdz = plane_gen ? K : K2;
+        if constexpr (C::F32) {
+            float c[MT][NT];
+            if (own) {
+                gemm_tile<MT, NT, false>(Mz, KP, T2, LD2, o0, n0, kdz, c);
+            } else {
 #pragma unroll
                 for (int i = 0; i < MT; ++i)
 #pragma unroll
-                    for (int j = 0; j < NC; ++j) {
-                        const int n = cn0 + j;
-                        if (co0 + i < K) U2[(n / K) * KK + (n % K) + K * (co0 + i)] = c[i][j];
-                    }
+                    for (int j = 0; j < NT; ++j) c[i][j] = 0.0f;
             }
-            cp_async_wait_all();
-            __syncthreads();
-            // ---- z: acc[c'][a' + P b'] += sum_c (beta Mz)[c'][c] T2[c][a' + P b']  (- previous correction)
-            if (has_next) load_mat(My, mats, tn.my);
-            if constexpr (C::F32) {
-                float c[MT][NT];
-                if (own) {
-                    gemm_tile<MT, NT, false>(Mz, KP, T2, LD2, o0, n0, kd, c);
-                } else {
+            const bool fold = uc_valid && own;
+            tmem_visit<ND, true>(tacc, [&](int d0, int n, auto& r) {
+#pragma unroll
+                for (int q2 = 0; q2 < n; ++q2) {
+                    const int d = d0 + q2, i = d / NT, j = d % NT;
+                    double v = words_to_double(r[2 * q2], r[2 * q2 + 1]) + (double)c[i][j];
+                    if (fold) v -= uc_at(i, j);
+                    double_to_words(v, r[2 * q2], r[2 * q2 + 1]);
+                }
+            });
+        } else {
+            if (own) {
+                gemm_tile<MT, NT, true>(Mz, KP, T2, LD2, o0, n0, kdz, acc);
+                if (uc_valid) {
 #pragma unroll
                     for (int i = 0; i < MT; ++i)
 #pragma unroll
-                        for (int j = 0; j < NT; ++j) c[i][j] = 0.0f;
-                }
-                const bool fold = uc_valid && own;
-                tmem_visit<ND, true>(tacc, [&](int d0, int n, auto& r) {
-#pragma unroll
-                    for (int q = 0; q < n; ++q) {
-                        const int d = d0 + q, i = d / NT, j = d % NT;
-                        double v = words_to_double(r[2 * q], r[2 * q + 1]) + (double)c[i][j];
-                        if (fold) v -= uc_at(i, j);
-                        double_to_words(v, r[2 * q], r[2 * q + 1]);
-                    }
-                });
-            } else {
-                if (own) {
-                    gemm_tile<MT, NT, true>(Mz, KP, T2, LD2, o0, n0, kd, acc);
-                    if (uc_valid) {
-#pragma unroll
-                        for (int i = 0; i < MT; ++i)
-#pragma unroll
-                            for (int j = 0; j < NT; ++j) acc[i][j] -= uc_at(i, j);
-                    }
+                        for (int j = 0; j < NT; ++j) acc[i][j] -= uc_at(i, j);
                 }
             }
-            uc_valid = false;
-            if (cown) {  // c2[c'][a' + k b'] = sum_{c<k} (beta Tz)[c'][c] U2[c][a' + k b']
-                int off[NC];
-#pragma unroll
-                for (int j = 0; j < NC; ++j) off[j] = cn0 + j;
-                gemm_tile_off<MT, NC>(Mz, KP, U2, KK, co0, off, K, c2);
-            }
-            pend2 = !root;
-            ++ntrip;
         }
+        uc_valid = false;
+        if (cown) {  // c2[c'][a' + k b'] = sum_{c<k} (beta Tz)[c'][c] U2[c][a' + k b']
+            int off[NC];
+#pragma unroll
+            for (int j = 0; j < NC; ++j) off[j] = cn0 + j;
+            gemm_tile_off<MT, NC>(Mz, KP, U2, KK, co0, off, K, c2);
+        }
+        pend2 = !root;
     }
     cp_async_wait_all();
     __syncthreads();  // z-phase readers of Uc are done
@@ -1059,7 +1262,7 @@ __global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
                 for (int j = 0; j < NT; ++j) emit(i, j, acc[i][j]);
         }
     }
-    double* red = reinterpret_cast<double*>(X);  // X is no longer read
+    double* red = reinterpret_cast<double*>(XA);  // the staging buffers are no longer read
     __syncthreads();
     block_sum2(n2, w2, red);
     if (tid == 0) {
@@ -1201,6 +1404,7 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     std::vector<Item> items;
     std::vector<int> item_off(nt + 1, 0);
     std::vector<BTree> bt(nt);
+    long long nreal = 0;  // block images of the input nodes at the entries' depths
     for (int t = 0; t < nt; ++t) {
         BatchTree& b = bp.trees[t];
         item_off[t] = (int)items.size();
@@ -1233,6 +1437,13 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         d.depth = b.depth;
         d.depth_limit = m.depth_limit;
         for (int q = 0; q < 3; ++q) d.ext[q] = (long long)m.boxes[q] << b.depth;
+        d.img_lb = d.img_le = 0;
+        if (in.levels() > b.depth) {
+            d.img_lb = in.level_begin[b.depth];
+            d.img_le = in.level_begin[b.depth + 1];
+        }
+        d.img_base = nreal;
+        nreal += d.img_le - d.img_lb;
     }
     item_off[nt] = (int)items.size();
     const int ni = (int)items.size();
@@ -1312,8 +1523,23 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     }
 
     // 3-4. triples per candidate, chunks
+    const bool pencil = contraction_pencil();
+    // the split-TF32 engine's error floor (about 2e-7 relative, data in two TF32 pieces) stays below the
+    // requested precision only from prec = 1e-6 up: finer requests take the FP32 engine
+    bool tc_prec_ok = true;
+    for (const BatchTree& b : bp.trees) tc_prec_ok &= !(b.prec > 0.0 && b.prec < kTensorCoreMinPrec);
+    // the GEMM-tiled engine runs the line-ordered contraction (chunks of sorted triples); the
+    // tensor-core and pencil engines take chunks of whole candidates
+    bool lined = false, lined32 = false;
+#define L_ENG(KK)                                                                                    \
+    lined = !pencil && !(bp.precision == 2 && TCfg<KK>::FITS && tc_prec_ok) &&                       \
+            ((bp.precision >= 1 && GCfg<KK, float>::FITS) || (bp.precision != 1 && GCfg<KK, double>::FITS)); \
+    lined32 = lined && bp.precision >= 1 && GCfg<KK, float>::FITS;
+    MWB_DISPATCH_K(K, L_ENG)
+#undef L_ENG
     int* d_cand_item = (int*)dalloc(ctx, sizeof(int) * ncap);
-    int* d_ntrip = (int*)dalloc(ctx, sizeof(int) * ncap);
+    int* d_ntrip = (int*)dalloc(ctx, sizeof(int) * (ncap + 1));
+    MWB_CUDA(cudaMemsetAsync(d_ntrip, 0, sizeof(int) * (ncap + 1), s));
     if (ncand > 0) {
         k_cand_item<<<ni, 128, 0, s>>>(d_offs, ni, d_cand_item);
         k_bterms<<<(ncand + 255) / 256, 256, 0, s>>>(d_cand_item, ncand, d_items, d_trees, d_cdelta, d_csrc, d_gnorm2,
@@ -1328,14 +1554,88 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     MWB_CUDA(cudaMemsetAsync(d_nchunk, 0, sizeof(int) * (ni + 1), s));
     MWB_CUDA(cudaMemsetAsync(d_nslot, 0, sizeof(int) * (ni + 1), s));
     const int chunk_limit = ctx->chunk_triples[std::min(std::max(bp.precision, 0), 2)];
-    k_bchunks<<<(ni + 127) / 128, 128, 0, s>>>(d_offs, ni, d_ntrip, chunk_limit, 0, d_nchunk, nullptr, nullptr, nullptr);
-    k_multi_slots<<<(ni + 127) / 128, 128, 0, s>>>(d_nchunk, ni, d_nslot);
-    count(ctx, 2);
-    const int nchunks = scan_total(ctx, d_nchunk, d_choff, ni);
-    const int nslots = scan_total(ctx, d_nslot, d_slotoff, ni);
-    Chunk* d_chunks = (Chunk*)dalloc(ctx, sizeof(Chunk) * std::max(1, nchunks));
-    k_bchunks<<<(ni + 127) / 128, 128, 0, s>>>(d_offs, ni, d_ntrip, chunk_limit, 1, d_nchunk, d_choff, d_slotoff,
-                                               d_chunks);
+    int* d_toff = nullptr;
+    int* d_terr = nullptr;
+    unsigned long long *d_tkey = nullptr, *d_tval = nullptr;
+    void* d_ximg = nullptr;
+    int nchunks = 0, nslots = 0;
+    Chunk* d_chunks = nullptr;
+    if (lined) {
+        d_terr = (int*)dalloc(ctx, sizeof(int));
+        MWB_CUDA(cudaMemsetAsync(d_terr, 0, sizeof(int), s));
+        d_toff = (int*)dalloc(ctx, sizeof(int) * (ncap + 1));
+        const int ntri = scan_total(ctx, d_ntrip, d_toff, ncand);
+        const size_t tcap = (size_t)std::max(1, ntri);
+        unsigned long long* d_tkey_in = (unsigned long long*)dalloc(ctx, sizeof(unsigned long long) * tcap);
+        unsigned long long* d_tval_in = (unsigned long long*)dalloc(ctx, sizeof(unsigned long long) * tcap);
+        d_tkey = (unsigned long long*)dalloc(ctx, sizeof(unsigned long long) * tcap);
+        d_tval = (unsigned long long*)dalloc(ctx, sizeof(unsigned long long) * tcap);
+        if (ntri > 0) {
+            k_texpand<<<(ncand + 255) / 256, 256, 0, s>>>(d_cand_item, ncand, d_items, d_trees, d_cdelta, d_ntrip,
+                                                          d_toff, d_csrc, d_tkey_in, d_tval_in, d_terr);
+            MWB_CUDA(cudaGetLastError());
+            int hb = 1;
+            while (hb < 31 && (1ll << hb) < (long long)ni) ++hb;
+            size_t tmp = 0;
+            MWB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, d_tkey_in, d_tkey, d_tval_in, d_tval, ntri, 0, 32 + hb, s));
+            void* d_tmp = dalloc(ctx, tmp);
+            MWB_CUDA(cub::DeviceRadixSort::SortPairs(d_tmp, tmp, d_tkey_in, d_tkey, d_tval_in, d_tval, ntri, 0, 32 + hb, s));
+            dfree(ctx, d_tmp);
+            count(ctx, 2);
+        }
+        dfree(ctx, d_tkey_in);
+        dfree(ctx, d_tval_in);
+        k_tchunks<<<(ni + 127) / 128, 128, 0, s>>>(d_offs, d_toff, ni, d_tkey, chunk_limit, 0, d_nchunk, nullptr,
+                                                   nullptr, nullptr);
+        k_multi_slots<<<(ni + 127) / 128, 128, 0, s>>>(d_nchunk, ni, d_nslot);
+        count(ctx, 2);
+        nchunks = scan_total(ctx, d_nchunk, d_choff, ni);
+        nslots = scan_total(ctx, d_nslot, d_slotoff, ni);
+        d_chunks = (Chunk*)dalloc(ctx, sizeof(Chunk) * std::max(1, nchunks));
+        k_tchunks<<<(ni + 127) / 128, 128, 0, s>>>(d_offs, d_toff, ni, d_tkey, chunk_limit, 1, d_nchunk, d_choff,
+                                                   d_slotoff, d_chunks);
+        int terr = 0;
+        MWB_CUDA(cudaMemcpyAsync(&terr, d_terr, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MWB_CUDA(cudaStreamSynchronize(s));
+        if (terr != 0) throw Error(-3, "input tree nodes are not in level order");
+        // block images of this pass's input nodes (the entries' depth levels) and generated nodes
+        const long long nimg = nreal + nu;
+        if (nimg > 0) {
+            std::vector<ImgSrc> srcs(nt);
+            for (int t = 0; t < nt; ++t)
+                srcs[t] = ImgSrc{bp.trees[t].inp->coef, bt[t].img_base, bt[t].img_lb, bt[t].img_le - bt[t].img_lb};
+            ImgSrc* d_srcs = upload(ctx, srcs);
+#define L_IMG(KK)                                                                                               \
+    {                                                                                                           \
+        if (lined32) {                                                                                          \
+            d_ximg = dalloc(ctx, sizeof(float) * (size_t)nimg * GCfg<KK, float>::IMG);                          \
+            const int smem = (int)(sizeof(float) * 8 * KK * KK * KK);                                          \
+            MWB_CUDA(cudaFuncSetAttribute(k_ximage<KK, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); \
+            k_ximage<KK, float><<<(unsigned)nimg, 256, smem, s>>>(d_srcs, nt, d_gblk, nreal, (float*)d_ximg);    \
+        } else {                                                                                                \
+            d_ximg = dalloc(ctx, sizeof(double) * (size_t)nimg * GCfg<KK, double>::IMG);                        \
+            const int smem = (int)(sizeof(double) * 8 * KK * KK * KK);                                         \
+            MWB_CUDA(cudaFuncSetAttribute(k_ximage<KK, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); \
+            k_ximage<KK, double><<<(unsigned)nimg, 256, smem, s>>>(d_srcs, nt, d_gblk, nreal, (double*)d_ximg);  \
+        }                                                                                                       \
+    }
+            MWB_DISPATCH_K(K, L_IMG)
+#undef L_IMG
+            MWB_CUDA(cudaGetLastError());
+            count(ctx);
+            dfree(ctx, d_srcs);
+        }
+    } else {
+        k_bchunks<<<(ni + 127) / 128, 128, 0, s>>>(d_offs, ni, d_ntrip, chunk_limit, 0, d_nchunk, nullptr, nullptr,
+                                                   nullptr);
+        k_multi_slots<<<(ni + 127) / 128, 128, 0, s>>>(d_nchunk, ni, d_nslot);
+        count(ctx, 2);
+        nchunks = scan_total(ctx, d_nchunk, d_choff, ni);
+        nslots = scan_total(ctx, d_nslot, d_slotoff, ni);
+        d_chunks = (Chunk*)dalloc(ctx, sizeof(Chunk) * std::max(1, nchunks));
+        k_bchunks<<<(ni + 127) / 128, 128, 0, s>>>(d_offs, ni, d_ntrip, chunk_limit, 1, d_nchunk, d_choff, d_slotoff,
+                                                   d_chunks);
+    }
     MWB_CUDA(cudaGetLastError());
     count(ctx);
     double* d_partials = (double*)dalloc(ctx, sizeof(double) * BS * std::max(1, nslots));
@@ -1345,11 +1645,6 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     int* d_kerr = reinterpret_cast<int*>(d_ntrip_tot + 1);  // set by the tensor-core kernel on a wait timeout
     MWB_CUDA(cudaMemsetAsync(d_ntrip_tot, 0, 2 * sizeof(unsigned long long), s));
     if (ctx->prof) MWB_CUDA(cudaEventRecord(ctx->ev0, s));
-    const bool pencil = contraction_pencil();
-    // the split-TF32 engine's error floor (about 2e-7 relative, data in two TF32 pieces) stays below the
-    // requested precision only from prec = 1e-6 up: finer requests take the FP32 engine
-    bool tc_prec_ok = true;
-    for (const BatchTree& b : bp.trees) tc_prec_ok &= !(b.prec > 0.0 && b.prec < kTensorCoreMinPrec);
 #define L_AP(KK)                                                                                             \
     {                                                                                                        \
         if (bp.precision == 2 && TCfg<KK>::FITS && !pencil && tc_prec_ok) {                                  \
@@ -1360,15 +1655,15 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         } else if (bp.precision >= 1 && GCfg<KK, float>::FITS && !pencil) {                                  \
             size_t smem = GCfg<KK, float>::SMEM;                                                             \
             MWB_CUDA(cudaFuncSetAttribute(k_gapply<KK, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-            k_gapply<KK, float><<<nchunks, GCfg<KK, float>::NTHR, smem, s>>>(d_chunks, d_items, d_trees, d_cdelta, \
-                                                                              d_csrc, d_gblk, d_gnorm2, d_partials, \
-                                                                              d_ntrip_tot);                        \
+            k_gapply<KK, float><<<nchunks, GCfg<KK, float>::NTHR, smem, s>>>(d_chunks, d_items, d_trees, d_tkey, \
+                                                                              d_tval, d_csrc, (const float*)d_ximg, \
+                                                                              nreal, d_partials, d_ntrip_tot);     \
         } else if (bp.precision != 1 && GCfg<KK, double>::FITS && !pencil) {                                  \
             size_t smem = GCfg<KK, double>::SMEM;                                                            \
             MWB_CUDA(cudaFuncSetAttribute(k_gapply<KK, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-            k_gapply<KK, double><<<nchunks, GCfg<KK, double>::NTHR, smem, s>>>(d_chunks, d_items, d_trees, d_cdelta, \
-                                                                                d_csrc, d_gblk, d_gnorm2, d_partials, \
-                                                                                d_ntrip_tot);                       \
+            k_gapply<KK, double><<<nchunks, GCfg<KK, double>::NTHR, smem, s>>>(d_chunks, d_items, d_trees, d_tkey, \
+                                                                                d_tval, d_csrc, (const double*)d_ximg, \
+                                                                                nreal, d_partials, d_ntrip_tot);    \
         } else if (bp.precision >= 1) {                                                                      \
             size_t smem = ACfg<KK, float>::SMEM;                                                             \
             MWB_CUDA(cudaFuncSetAttribute(k_bapply<KK, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
@@ -1462,7 +1757,7 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     for (void* p : std::initializer_list<void*>{d_items, d_trees, d_item_off, d_count, d_offs, d_ngreq, d_cdelta, d_csrc,
                                                 d_greq_key, d_greq_leaf, d_ukey, d_uleaf, d_gblk, d_gnorm2, d_cand_item,
                                                 d_ntrip, d_nchunk, d_choff, d_nslot, d_slotoff, d_chunks, d_partials,
-                                                d_ntrip_tot, d_sflags, d_spos})
+                                                d_ntrip_tot, d_sflags, d_spos, d_toff, d_tkey, d_tval, d_terr, d_ximg})
         dfree(ctx, p);
     bp.nchunks = nchunks;
     bp.nslots = nslots;

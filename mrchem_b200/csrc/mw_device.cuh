@@ -83,6 +83,11 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+// wait until at most N of this thread's most recently committed groups are pending
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 // prefetch the 16-byte-aligned part of [gmem, gmem + bytes) into L2 through the bulk-copy engine
 // (the instruction wants a 16-byte aligned address and a size that is a multiple of 16)
 __device__ __forceinline__ void prefetch_l2_bulk(const void* gmem, unsigned bytes) {

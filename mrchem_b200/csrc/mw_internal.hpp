@@ -77,7 +77,7 @@ struct Mra {
 struct DeltaRec {
     int d[3];
     int t0, t1;
-    int pad;
+    int lrank;  // dz rank << 10 | dy rank among the depth's offsets (line order of the contraction)
     double maxb;
 };
 struct TermRec {
