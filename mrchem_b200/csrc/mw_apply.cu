@@ -7,8 +7,11 @@
 //      up in the input tree's hash index (or its leaf ancestor -> generated node) and screens it;
 //   2. generated (scaling-only) input nodes are de-duplicated per tree and built once;
 //   3. per candidate, the number of terms that pass the screening (the triples it contributes);
-//   4. each output node's candidate list is cut into chunks of at most chunk_triples triples (a
-//      per-engine context setting, 48 unless tuned);
+//   4. GEMM-tiled engine: the triples are expanded and sorted per output node by (term, dz, dy), and
+//      each node's sorted triples are cut at plane boundaries into chunks of about chunk_triples
+//      triples (a per-engine context setting, 48 unless tuned); the input blocks of the pass get
+//      images in the kernel's staging layout.  Tensor-core and pencil engines: each node's candidate
+//      list is cut into chunks of at most chunk_triples triples;
 //   5. the contraction kernel runs one CTA per chunk; multi-chunk nodes write partial blocks that
 //      a reduction kernel adds in chunk order (deterministic), single-chunk nodes write directly;
 //   6. norms and split flags; children are appended to each tree.
@@ -321,32 +324,46 @@ __global__ void k_texpand(const int* __restrict__ cand_item, int ncand, const It
     }
 }
 // greedy cut of each node's sorted triples into chunks of about `limit` triples, at plane
-// boundaries (a plane = the triples of one (term, dz); at least one chunk per node)
+// boundaries (a plane = the triples of one (term, dz); at least one chunk per node).  One warp per
+// node: the plane starts of 32 triples at a time come from one ballot, and the cut walks the planes
+// in order (a plane's size is known when the next one starts)
 __global__ void k_tchunks(const int* __restrict__ offs, const int* __restrict__ toff, int nitems,
                           const unsigned long long* __restrict__ key, int limit, int fill, int* nchunk,
                           const int* __restrict__ choff, const int* __restrict__ slotoff, Chunk* chunks) {
-    const int w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= nitems) return;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= nitems) return;  // uniform over the warp
     const int t0 = toff[offs[w]], t1 = toff[offs[w + 1]];
-    int nch = 0, acc = 0, start = t0;
+    int nch = 0, acc = 0, start = t0, ps = -1;  // ps: start of the plane being measured
     const int multi = fill ? (choff[w + 1] - choff[w] > 1) : 0;
-    int t = t0;
-    while (t < t1) {
-        const uint32_t plane = (uint32_t)(key[t] & 0xffffffffull) >> 10;
-        int e = t + 1;
-        while (e < t1 && ((uint32_t)(key[e] & 0xffffffffull) >> 10) == plane) ++e;
-        if (acc > 0 && acc + (e - t) > limit) {
-            if (fill) chunks[choff[w] + nch] = Chunk{w, start, t, multi ? slotoff[w] + nch : -1};
+    auto plane_done = [&](int end) {  // plane [ps, end) is complete: cut before it if it overflows
+        const int sz = end - ps;
+        if (acc > 0 && acc + sz > limit) {
+            if (fill && lane == 0) chunks[choff[w] + nch] = Chunk{w, start, ps, multi ? slotoff[w] + nch : -1};
             ++nch;
             acc = 0;
-            start = t;
+            start = ps;
         }
-        acc += e - t;
-        t = e;
+        acc += sz;
+    };
+    for (int b = t0; b < t1; b += 32) {
+        const int t = b + lane;
+        bool st = false;
+        if (t < t1)
+            st = t == t0 ||
+                 ((uint32_t)(key[t] & 0xffffffffull) >> 10) != ((uint32_t)(key[t - 1] & 0xffffffffull) >> 10);
+        unsigned m = __ballot_sync(0xffffffffu, st);
+        while (m) {
+            const int p = b + __ffs(m) - 1;
+            m &= m - 1;
+            if (ps >= 0) plane_done(p);
+            ps = p;
+        }
     }
-    if (fill) chunks[choff[w] + nch] = Chunk{w, start, t1, multi ? slotoff[w] + nch : -1};
+    if (ps >= 0) plane_done(t1);
+    if (fill && lane == 0) chunks[choff[w] + nch] = Chunk{w, start, t1, multi ? slotoff[w] + nch : -1};
     ++nch;
-    if (!fill) nchunk[w] = nch;
+    if (!fill && lane == 0) nchunk[w] = nch;
 }
 // Block images for the line-ordered contraction: image row a (a < 2k) holds X[a][b + P c] of the
 // node block (P = 2k rounded up to 4; zero where b or c >= 2k), so that a CTA stages a block with
@@ -721,8 +738,10 @@ __host__ __device__ constexpr int gcfg_nc(int k, int nthr) {
     return d;
 }
 // Row-stride padding of the T1 (x-step output) and T2 (y-step output) buffers, chosen per basis size
-// so that the epilogue stores of a warp fall into distinct banks (counted wavefronts per step,
-// consecutive column tiles per warp; the FP64 x step with an odd tile width uses strided tiles).
+// so that the epilogue stores of a warp fall into few banks (counted wavefronts per step, consecutive
+// column tiles per warp; the FP64 x step with an odd tile width uses strided tiles).  In FP32 the T1
+// stride matches the 16-byte staging rows (T1 replaces a staged block at a line's end), which leaves
+// two-way conflicts on the once-per-line T1 stores at k = 9, 10.
 __host__ __device__ constexpr int gcfg_pad1(int k, bool f32) {
     return f32 ? ((k == 5 || k == 6 || k == 9 || k == 10 || k == 11 || k == 12) ? 4 : 0) : 0;
 }
@@ -1585,14 +1604,14 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         }
         dfree(ctx, d_tkey_in);
         dfree(ctx, d_tval_in);
-        k_tchunks<<<(ni + 127) / 128, 128, 0, s>>>(d_offs, d_toff, ni, d_tkey, chunk_limit, 0, d_nchunk, nullptr,
+        k_tchunks<<<(ni * 32 + 127) / 128, 128, 0, s>>>(d_offs, d_toff, ni, d_tkey, chunk_limit, 0, d_nchunk, nullptr,
                                                    nullptr, nullptr);
         k_multi_slots<<<(ni + 127) / 128, 128, 0, s>>>(d_nchunk, ni, d_nslot);
         count(ctx, 2);
         nchunks = scan_total(ctx, d_nchunk, d_choff, ni);
         nslots = scan_total(ctx, d_nslot, d_slotoff, ni);
         d_chunks = (Chunk*)dalloc(ctx, sizeof(Chunk) * std::max(1, nchunks));
-        k_tchunks<<<(ni + 127) / 128, 128, 0, s>>>(d_offs, d_toff, ni, d_tkey, chunk_limit, 1, d_nchunk, d_choff,
+        k_tchunks<<<(ni * 32 + 127) / 128, 128, 0, s>>>(d_offs, d_toff, ni, d_tkey, chunk_limit, 1, d_nchunk, d_choff,
                                                    d_slotoff, d_chunks);
         int terr = 0;
         MWB_CUDA(cudaMemcpyAsync(&terr, d_terr, sizeof(int), cudaMemcpyDeviceToHost, s));
