@@ -965,7 +965,7 @@ void generate_node(const Tree& inp, int leaf, int depth, const int64_t t[3], dou
     std::memcpy(s, cur.data(), sizeof(double) * k * k * k);
 }
 
-void apply(double prec, Tree& out, Operator& op, const Tree& inp, ApplyStats* stats) {
+void apply(double prec, Tree& out, Operator& op, const Tree& inp, ApplyStats* stats, bool line_order = false) {
     const MRA& mra = *inp.mra;
     const int k = mra.k();
     const int K2 = 2 * k;
@@ -1062,6 +1062,86 @@ void apply(double prec, Tree& out, Operator& op, const Tree& inp, ApplyStats* st
             std::vector<double> acc(BS, 0.0), t1(BS), t2(BS), t3(BS);
             std::vector<double> s_in(SS), u1(SS), u2(SS), u3(SS);
             std::vector<std::array<int, 3>> seen_yz, seen_z;
+            if (line_order) {
+                // The same triples summed in line order (the order of the GPU's line-ordered
+                // contraction): sorted by (term, dz, dy), a line's x products are summed before its y
+                // product and a plane's y products before its z product.  Linear algebra makes this
+                // the same sum in another order.
+                struct Tri { int m, dz, dy, c; };
+                std::vector<Tri> tri;
+                for (int ci = 0; ci < (int)cands[q].size(); ++ci) {
+                    const Cand& c = cands[q][ci];
+                    const DeltaEntry& de = dl[c.delta];
+                    const double nu = c.src < 0 ? gnorm[-c.src - 1] : inorm[c.src];
+                    if (!(nu > 0.0) || de.maxb * nu < theta) continue;
+                    for (const auto& tb : de.terms) {
+                        if (tb.first * nu < theta) break;
+                        tri.push_back({tb.second, de.d[2], de.d[1], ci});
+                    }
+                }
+                std::stable_sort(tri.begin(), tri.end(), [](const Tri& a, const Tri& b) {
+                    return a.m != b.m ? a.m < b.m : a.dz != b.dz ? a.dz < b.dz : a.dy < b.dy;
+                });
+                std::vector<double> full(BS), line(BS), plane(BS), tmp(BS), sline(SS), splane(SS), stmp(SS);
+                size_t t = 0;
+                while (t < tri.size()) {
+                    const int m = tri[t].m, dz = tri[t].dz;
+                    const Band& b = bs[m];
+                    const double beta = op.terms[m].beta;
+                    std::fill(plane.begin(), plane.end(), 0.0);
+                    std::fill(splane.begin(), splane.end(), 0.0);
+                    while (t < tri.size() && tri[t].m == m && tri[t].dz == dz) {
+                        const int dy = tri[t].dy;
+                        std::fill(line.begin(), line.end(), 0.0);
+                        std::fill(sline.begin(), sline.end(), 0.0);
+                        while (t < tri.size() && tri[t].m == m && tri[t].dz == dz && tri[t].dy == dy) {
+                            const Cand& c = cands[q][tri[t].c];
+                            const DeltaEntry& de = dl[c.delta];
+                            const bool gen = c.src < 0;
+                            if (gen) {  // the scaling-only block, zero elsewhere
+                                const double* g = &gblk[(size_t)(-c.src - 1) * SS];
+                                std::fill(full.begin(), full.end(), 0.0);
+                                for (int z = 0; z < k; ++z)
+                                    for (int y = 0; y < k; ++y)
+                                        for (int x = 0; x < k; ++x) full[x + K2 * (y + K2 * z)] = g[x + k * (y + k * z)];
+                            } else {
+                                std::copy(inp.nodes[c.src].c.begin(), inp.nodes[c.src].c.end(), full.begin());
+                            }
+                            const double* Mx = &b.ns[(size_t)(de.d[0] + b.L) * K2 * K2];
+                            mode_product(Mx, K2, K2, K2, 0, full.data(), K2, K2, K2, tmp.data());
+                            for (size_t i = 0; i < BS; ++i) line[i] += tmp[i];
+                            if (!root) {
+                                for (int z = 0; z < k; ++z)
+                                    for (int y = 0; y < k; ++y)
+                                        for (int x = 0; x < k; ++x) s_in[x + k * (y + k * z)] = full[x + K2 * (y + K2 * z)];
+                                mode_product(Mx, K2, k, k, 0, s_in.data(), k, k, k, stmp.data());
+                                for (size_t i = 0; i < SS; ++i) sline[i] += stmp[i];
+                            }
+                            ++trip[q];
+                            if (gen) ++tripg[q];
+                            seen_yz.push_back({m, dy, dz});
+                            seen_z.push_back({m, 0, dz});
+                            ++t;
+                        }
+                        const double* My = &b.ns[(size_t)(dy + b.L) * K2 * K2];
+                        mode_product(My, K2, K2, K2, 1, line.data(), K2, K2, K2, tmp.data());
+                        for (size_t i = 0; i < BS; ++i) plane[i] += tmp[i];
+                        if (!root) {
+                            mode_product(My, K2, k, k, 1, sline.data(), k, k, k, stmp.data());
+                            for (size_t i = 0; i < SS; ++i) splane[i] += stmp[i];
+                        }
+                    }
+                    const double* Mz = &b.ns[(size_t)(dz + b.L) * K2 * K2];
+                    mode_product(Mz, K2, K2, K2, 2, plane.data(), K2, K2, K2, tmp.data());
+                    for (size_t i = 0; i < BS; ++i) acc[i] += beta * tmp[i];
+                    if (!root) {  // remove the scaling->scaling block (it belongs to the coarser scale)
+                        mode_product(Mz, K2, k, k, 2, splane.data(), k, k, k, u3.data());
+                        for (int z = 0; z < k; ++z)
+                            for (int y = 0; y < k; ++y)
+                                for (int x = 0; x < k; ++x) acc[x + K2 * (y + K2 * z)] -= beta * u3[x + k * (y + k * z)];
+                    }
+                }
+            } else
             for (const Cand& c : cands[q]) {
                 const DeltaEntry& de = dl[c.delta];
                 const bool gen = c.src < 0;
@@ -1651,9 +1731,14 @@ void oracle_scaling_matrix(void* o, double alpha, int n, int l, double* T) {
     ((Operator*)o)->scaling_matrix(alpha, n, l, T);
 }
 
+int oracle_apply_ordered(double prec, void* out, void* op, void* inp, long long* stats, int line_order);
 int oracle_apply(double prec, void* out, void* op, void* inp, long long* stats) {
+    return oracle_apply_ordered(prec, out, op, inp, stats, 0);
+}
+// line_order != 0: the per-node sums in the line order of the GPU contraction (same triples)
+int oracle_apply_ordered(double prec, void* out, void* op, void* inp, long long* stats, int line_order) {
     ApplyStats st;
-    apply(prec, *(Tree*)out, *(Operator*)op, *(Tree*)inp, &st);
+    apply(prec, *(Tree*)out, *(Operator*)op, *(Tree*)inp, &st, line_order != 0);
     if (stats) {
         stats[0] = st.triples;
         stats[1] = st.triples_gen;

@@ -62,6 +62,7 @@ def lib():
         L.oracle_operator_ns.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp]
         L.oracle_scaling_matrix.argtypes = [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp]
         L.oracle_apply.argtypes = [ctypes.c_double, _vp, _vp, _vp, _lp]
+        L.oracle_apply_ordered.argtypes = [ctypes.c_double, _vp, _vp, _vp, _lp, ctypes.c_int]
         L.oracle_multiply.argtypes = [ctypes.c_double, _vp, ctypes.c_double, _vp, _vp, ctypes.c_int]
         L.oracle_build_grid.argtypes = [_vp, _vp]
         L.oracle_derivative.argtypes = [_vp, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_int]
@@ -229,6 +230,15 @@ def apply(prec, out: FunctionTree, op: ConvolutionOperator, inp: FunctionTree):
     """Adaptive NS-form apply; returns (triples, triples_with_generated_input, passes)."""
     st = np.zeros(8, np.int64)
     lib().oracle_apply(float(prec), out._h, op._h, inp._h, st.ctypes.data_as(_lp))
+    return int(st[0]), int(st[1]), int(st[2])
+
+
+def apply_line_ordered(prec, out: FunctionTree, op: ConvolutionOperator, inp: FunctionTree):
+    """The same apply with every output node's sums taken in the line order of the GPU contraction
+    (triples sorted by (term, dz, dy); a line's x products, then a plane's y products, summed before
+    the next mode product); returns (triples, triples_with_generated_input, passes)."""
+    st = np.zeros(8, np.int64)
+    lib().oracle_apply_ordered(float(prec), out._h, op._h, inp._h, st.ctypes.data_as(_lp), 1)
     return int(st[0]), int(st[1]), int(st[2])
 
 

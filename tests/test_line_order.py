@@ -7,8 +7,8 @@ The contraction kernel (mrchem_b200/csrc/mw_apply.cu, k_gapply) sorts an output 
 
 so that a line (equal term, dz, dy) shares one y mode product and a plane (equal term, dz) one z
 mode product.  These tests restate that grouping in numpy with the oracle's own NS-form operator
-matrices and compare it with the per-triple sum of the oracle's method, and check the oracle's
-line statistics of a real apply.
+matrices and compare it with the per-triple sum of the oracle's method, check the oracle's line
+statistics of a real apply, and compare whole oracle applies summed in either order.
 """
 import numpy as np
 import pytest
@@ -104,3 +104,28 @@ def test_oracle_line_statistics(oracle_mod):
     assert 0 < planes < lines < triples
     per_triple = (triples + lines + planes) / triples
     assert 1.0 < per_triple < 3.0
+
+
+@pytest.mark.parametrize("mu", [0.0, 3.0])
+def test_oracle_line_order_apply_matches_per_triple_order(oracle_mod, mu):
+    """A whole adaptive apply with every output node summed in line order gives the same tree and,
+    up to FP64 rounding, the same coefficients as the per-triple order, over the same triples
+    (including triples whose input is a generated scaling-only block)."""
+    O = oracle_mod
+    prec = 1e-4
+    m = O.MultiResolutionAnalysis(*WORLD, 5, 10)
+    f = O.FunctionTree(m)
+    O.project(prec, f, O.gauss_params([1.0, -0.3, 0.5], [4.0, 60.0, 15.0],
+                                      [(0.1, -0.2, 0.3), (-0.4, 0.2, 0.0), (0.6, 0.5, -0.3)]))
+    op = O.PoissonOperator(m, prec) if mu == 0.0 else O.HelmholtzOperator(m, mu, prec)
+    a, b = O.FunctionTree(m), O.FunctionTree(m)
+    sa = O.apply(prec, a, op, f)
+    sb = O.apply_line_ordered(prec, b, op, f)
+    assert sa == sb  # triples, triples with generated inputs, passes
+    if mu > 0.0:
+        assert sa[1] > 0  # this case covers generated inputs
+    ea, eb = a.export(), b.export()
+    for key in ("depth", "trans", "parent", "child0"):
+        assert np.array_equal(ea[key], eb[key]), key
+    scale = np.abs(ea["coef"]).max()
+    assert np.abs(ea["coef"] - eb["coef"]).max() <= 1e-13 * scale
