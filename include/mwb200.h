@@ -36,8 +36,12 @@ enum { MW_FUNC_GAUSSIANS = 1, MW_FUNC_HYDROGEN_PRODUCTS = 2 };
  * accumulated in FP64 (mixed precision), or split-TF32 products on the tensor cores (data in two TF32
  * pieces, operators in three; FP32 sums inside a term, compensated summation over terms; relative
  * error 2e-7 .. 1e-6, so it serves orders k <= 10 at prec >= 1e-6 (where its error is at most about
- * prec), and other requests take the FP32 path); norms, screening and refinement are FP64 in all three */
-enum { MW_APPLY_FP64 = 0, MW_APPLY_FP32 = 1, MW_APPLY_TF32X3 = 2 };
+ * prec), and other requests take the FP32 path), or BF16x3: the x mode product of every
+ * (output, input, term) triple on the tensor cores with data and operator rows as three BF16 slices of a
+ * per-row fixed-point form (exact FP32 sums inside a triple; FP32-level error), the y and z mode
+ * products as FP32 products on the CUDA cores and every term's contribution accumulated in FP64 (orders
+ * k = 7 .. 10; other orders take the FP32 path); norms, screening and refinement are FP64 in all four */
+enum { MW_APPLY_FP64 = 0, MW_APPLY_FP32 = 1, MW_APPLY_TF32X3 = 2, MW_APPLY_BF16X3 = 3 };
 
 const char* mw_last_error(void);
 int mw_version(int* major, int* minor);

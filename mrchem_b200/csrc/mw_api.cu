@@ -11,6 +11,7 @@
 
 #include "../../include/mwb200.h"
 #include "mw_kernels.cuh"
+#include "mw_slice.hpp"
 #include "mw_learned.cuh"
 
 namespace mwb {
@@ -207,6 +208,9 @@ Op::~Op() {
         dfree(c, kv.second->d_matsbT32);
         dfree(c, kv.second->d_matsI);
         dfree(c, kv.second->d_matsbI);
+        dfree(c, kv.second->d_matsS32);
+        dfree(c, kv.second->d_matsbS32);
+        dfree(c, kv.second->d_matsX);
         dfree(c, kv.second->d_deltas);
         dfree(c, kv.second->d_terms);
     }
@@ -521,6 +525,50 @@ static const OpDepth& op_depth(Op& op, int depth, int dir = 0) {
     if (!mI.empty()) {
         MWB_CUDA(cudaMemcpyAsync(od->d_matsI, mI.data(), sizeof(float) * mI.size(), cudaMemcpyHostToDevice, s));
         MWB_CUDA(cudaMemcpyAsync(od->d_matsbI, mbI.data(), sizeof(float) * mbI.size(), cudaMemcpyHostToDevice, s));
+    }
+    // tensor-core x step (k_happly, 2k <= 20): split-layout FP32 operators of the y/z tiles and the BF16
+    // slice images of every matrix as an x operator
+    if (K2 >= 13 && K2 <= 20) {
+        const int MT = KP / 4;
+        std::vector<float> mS(nmat * KP * KP, 0.0f), mbS(nmat * KP * KP, 0.0f);
+        for (size_t mi = 0; mi < nmat; ++mi)
+            for (int o = 0; o < K2; ++o)
+                for (int k = 0; k < K2; ++k) {
+                    const size_t w = mi * KP * KP + (size_t)k * KP + split_pos(o, MT, 4);
+                    mS[w] = (float)od->mats[mi * K2 * K2 + (size_t)o * K2 + k];
+                    mbS[w] = (float)mb[mi * K2 * K2 + (size_t)o * K2 + k];
+                }
+        const XGeo xg(K2);
+        std::vector<uint16_t> mX(nmat * (size_t)xg.OPB / 2, 0);
+        std::vector<float> sl0(K2), sl1(K2), sl2(K2);
+        for (size_t mi = 0; mi < nmat; ++mi)
+            for (int o = 0; o < K2; ++o) {
+                slice3_row(&od->mats[mi * K2 * K2 + (size_t)o * K2], K2, 1, sl0.data(), sl1.data(), sl2.data());
+                const float* sl[3] = {sl0.data(), sl1.data(), sl2.data()};
+                for (int q = 0; q < 3; ++q) {
+                    const int row = (2 + q) * xg.W + o;
+                    for (int k = 0; k < K2; ++k)
+                        mX[mi * (size_t)xg.OPB / 2 + ((size_t)(k / 8) * xg.NB + row) * 8 + k % 8] = bf16_bits_exact(sl[q][k]);
+                }
+                if (o < xg.W2) {  // the s->s block row M[o][0 .. k)
+                    slice3_row(&od->mats[mi * K2 * K2 + (size_t)o * K2], xg.W2, 1, sl0.data(), sl1.data(), sl2.data());
+                    for (int q = 0; q < 3; ++q) {
+                        const int row = (2 + q) * xg.W2 + o;
+                        for (int k = 0; k < xg.W2; ++k)
+                            mX[(mi * (size_t)xg.OPB + xg.OPB_MAIN) / 2 + ((size_t)(k / 8) * xg.NB2 + row) * 8 + k % 8] =
+                                bf16_bits_exact(sl[q][k]);
+                    }
+                }
+            }
+        od->d_matsS32 = (float*)dalloc(ctx, sizeof(float) * std::max<size_t>(1, mS.size()));
+        od->d_matsbS32 = (float*)dalloc(ctx, sizeof(float) * std::max<size_t>(1, mS.size()));
+        od->d_matsX = (unsigned char*)dalloc(ctx, std::max<size_t>(16, mX.size() * 2));
+        if (!mS.empty()) {
+            MWB_CUDA(cudaMemcpyAsync(od->d_matsS32, mS.data(), sizeof(float) * mS.size(), cudaMemcpyHostToDevice, s));
+            MWB_CUDA(cudaMemcpyAsync(od->d_matsbS32, mbS.data(), sizeof(float) * mS.size(), cudaMemcpyHostToDevice, s));
+            MWB_CUDA(cudaMemcpyAsync(od->d_matsX, mX.data(), mX.size() * 2, cudaMemcpyHostToDevice, s));
+        }
+        MWB_CUDA(cudaStreamSynchronize(s));  // host vectors leave scope
     }
     if (!mT.empty()) {
         MWB_CUDA(cudaMemcpyAsync(od->d_matsT, mT.data(), sizeof(double) * mT.size(), cudaMemcpyHostToDevice, s));
@@ -1048,7 +1096,8 @@ int mw_ctx_create(int device, void* stream, mw_ctx* out) {
 int mw_ctx_set_chunk_triples(mw_ctx ctx, int flags, int triples) {
     MW_TRY({
         MW_ARG(ctx, "null context");
-        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3, "unknown apply flags");
+        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3 || flags == MW_APPLY_BF16X3,
+               "unknown apply flags");
         MW_ARG(triples >= 1 && triples <= 4096, "triples per CTA must be in [1, 4096]");
         ctx->chunk_triples[flags] = triples;
     })
@@ -1057,7 +1106,8 @@ int mw_ctx_set_chunk_triples(mw_ctx ctx, int flags, int triples) {
 int mw_ctx_get_chunk_triples(mw_ctx ctx, int flags, int* triples) {
     MW_TRY({
         MW_ARG(ctx && triples, "null pointer");
-        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3, "unknown apply flags");
+        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3 || flags == MW_APPLY_BF16X3,
+               "unknown apply flags");
         *triples = ctx->chunk_triples[flags];
     })
 }
@@ -1483,7 +1533,8 @@ int mw_op_create_abgv(mw_mra m, double a, double b, mw_op* out) {
 int mw_apply_derivative(mw_tree out, mw_op op, mw_tree inp, int dir, int flags) {
     MW_TRY({
         MW_ARG(out && op && inp, "null pointer");
-        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3, "unknown apply flags");
+        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3 || flags == MW_APPLY_BF16X3,
+               "unknown apply flags");
         MWB_CUDA(cudaSetDevice(inp->mra->ctx->device));
         apply_derivative(out, op, inp, dir, flags);
     })
@@ -1518,7 +1569,8 @@ int mw_op_terms(mw_op op, double* alpha, double* beta) {
 int mw_apply(double prec, mw_tree out, mw_op op, mw_tree inp, int flags) {
     MW_TRY({
         MW_ARG(out && op && inp, "null pointer");
-        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3, "unknown apply flags");
+        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3 || flags == MW_APPLY_BF16X3,
+               "unknown apply flags");
         MWB_CUDA(cudaSetDevice(inp->mra->ctx->device));
         Tree* o = out;
         Op* p = op;
@@ -1530,7 +1582,8 @@ int mw_apply(double prec, mw_tree out, mw_op op, mw_tree inp, int flags) {
 int mw_apply_batched(int n, double prec, mw_tree* out, mw_op* ops, mw_tree* inp, int flags) {
     MW_TRY({
         MW_ARG(n > 0 && out && ops && inp, "null pointer or empty batch");
-        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3, "unknown apply flags");
+        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3 || flags == MW_APPLY_BF16X3,
+               "unknown apply flags");
         MW_ARG(inp[0], "null input tree");
         MWB_CUDA(cudaSetDevice(inp[0]->mra->ctx->device));
         std::vector<Tree*> o(n), i(n);
@@ -1680,7 +1733,8 @@ int mw_apply_learned(int n, double prec, mw_tree* out, mw_op* ops, mw_tree* inp,
                      long long* stats) {
     MW_TRY({
         MW_ARG(n > 0 && out && ops && inp && mlp, "null pointer or empty batch");
-        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3, "unknown apply flags");
+        MW_ARG(flags == MW_APPLY_FP64 || flags == MW_APPLY_FP32 || flags == MW_APPLY_TF32X3 || flags == MW_APPLY_BF16X3,
+               "unknown apply flags");
         MW_ARG(tau > 0.0f && tau < 1.0f, "tau must be in (0, 1)");
         MW_ARG(inp[0], "null input tree");
         MW_ARG(mlp->ctx == inp[0]->mra->ctx, "the network and the trees belong to different contexts");

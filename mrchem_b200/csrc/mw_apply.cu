@@ -52,6 +52,9 @@ struct BTree {
     const float* matsbT32;
     const float* matsI;  // split-TF32 operator images (tensor-core contraction)
     const float* matsbI;
+    const float* matsS32;  // tensor-core x step engine: split-layout y/z operators and x-operator slices
+    const float* matsbS32;
+    const unsigned char* matsX;
     int nprefix;
     int root;
     double theta;
@@ -1295,6 +1298,7 @@ __global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
 
 }  // namespace mwb
 #include "mw_tapply.cuh"
+#include "mw_happly.cuh"
 namespace mwb {
 
 // add the partial blocks of a multi-chunk node in chunk order; write block and norms
@@ -1413,6 +1417,35 @@ static int scan_total(Ctx* ctx, const int* d_in, int* d_out, int n) {
         default: throw Error(-1, "unsupported order (k must be 4..12)"); \
     }
 
+// launches of the tensor-core x step engine (instantiated only for the orders it serves)
+template <int K>
+static void* launch_simage(Ctx* ctx, long long nimg, const ImgSrc* d_srcs, int nt, const double* d_gblk,
+                           long long nreal, cudaStream_t s) {
+    if constexpr (HCfg<K>::FITS) {
+        void* img = dalloc(ctx, (size_t)nimg * HCfg<K>::IMGB);
+        const int smem = (int)(sizeof(double) * 8 * K * K * K);
+        MWB_CUDA(cudaFuncSetAttribute(k_simage<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        k_simage<K><<<(unsigned)nimg, 256, smem, s>>>(d_srcs, nt, d_gblk, nreal, (unsigned char*)img);
+        return img;
+    } else {
+        throw Error(-1, "BF16x3 engine: unsupported order");
+    }
+}
+template <int K>
+static void launch_happly(int nchunks, const Chunk* d_chunks, const Item* d_items, const BTree* d_trees,
+                          const unsigned long long* d_tkey, const unsigned long long* d_tval, const int* d_csrc,
+                          const unsigned char* d_img, long long nreal, double* d_partials,
+                          unsigned long long* d_ntrip, int* d_kerr, cudaStream_t s) {
+    if constexpr (HCfg<K>::FITS) {
+        const size_t smem = HCfg<K>::SMEM;
+        MWB_CUDA(cudaFuncSetAttribute(k_happly<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_happly<K><<<nchunks, HCfg<K>::NTHR, smem, s>>>(d_chunks, d_items, d_trees, d_tkey, d_tval, d_csrc, d_img,
+                                                          nreal, d_partials, d_ntrip, d_kerr);
+    } else {
+        throw Error(-1, "BF16x3 engine: unsupported order");
+    }
+}
+
 void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     const int nt = (int)bp.trees.size();
     Ctx* ctx = bp.trees[0].out->mra->ctx;
@@ -1449,6 +1482,9 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         d.matsbT32 = b.tab->d_matsbT32;
         d.matsI = b.tab->d_matsI;
         d.matsbI = b.tab->d_matsbI;
+        d.matsS32 = b.tab->d_matsS32;
+        d.matsbS32 = b.tab->d_matsbS32;
+        d.matsX = b.tab->d_matsX;
         d.nprefix = b.nprefix;
         d.root = b.depth == 0;
         d.theta = b.theta;
@@ -1549,11 +1585,12 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     for (const BatchTree& b : bp.trees) tc_prec_ok &= !(b.prec > 0.0 && b.prec < kTensorCoreMinPrec);
     // the GEMM-tiled engine runs the line-ordered contraction (chunks of sorted triples); the
     // tensor-core and pencil engines take chunks of whole candidates
-    bool lined = false, lined32 = false;
+    bool lined = false, lined32 = false, hyb = false;
 #define L_ENG(KK)                                                                                    \
-    lined = !pencil && !(bp.precision == 2 && TCfg<KK>::FITS && tc_prec_ok) &&                       \
-            ((bp.precision >= 1 && GCfg<KK, float>::FITS) || (bp.precision != 1 && GCfg<KK, double>::FITS)); \
-    lined32 = lined && bp.precision >= 1 && GCfg<KK, float>::FITS;
+    hyb = !pencil && bp.precision == 3 && HCfg<KK>::FITS;                                            \
+    lined = hyb || (!pencil && !(bp.precision == 2 && TCfg<KK>::FITS && tc_prec_ok) &&               \
+            ((bp.precision >= 1 && GCfg<KK, float>::FITS) || (bp.precision != 1 && GCfg<KK, double>::FITS))); \
+    lined32 = lined && !hyb && bp.precision >= 1 && GCfg<KK, float>::FITS;
     MWB_DISPATCH_K(K, L_ENG)
 #undef L_ENG
     int* d_cand_item = (int*)dalloc(ctx, sizeof(int) * ncap);
@@ -1572,7 +1609,7 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     int* d_slotoff = (int*)dalloc(ctx, sizeof(int) * (ni + 1));
     MWB_CUDA(cudaMemsetAsync(d_nchunk, 0, sizeof(int) * (ni + 1), s));
     MWB_CUDA(cudaMemsetAsync(d_nslot, 0, sizeof(int) * (ni + 1), s));
-    const int chunk_limit = ctx->chunk_triples[std::min(std::max(bp.precision, 0), 2)];
+    const int chunk_limit = ctx->chunk_triples[std::min(std::max(bp.precision, 0), 3)];
     int* d_toff = nullptr;
     int* d_terr = nullptr;
     unsigned long long *d_tkey = nullptr, *d_tval = nullptr;
@@ -1626,7 +1663,9 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
             ImgSrc* d_srcs = upload(ctx, srcs);
 #define L_IMG(KK)                                                                                               \
     {                                                                                                           \
-        if (lined32) {                                                                                          \
+        if (hyb) {                                                                                              \
+            d_ximg = launch_simage<KK>(ctx, nimg, d_srcs, nt, d_gblk, nreal, s);                                \
+        } else if (lined32) {                                                                                   \
             d_ximg = dalloc(ctx, sizeof(float) * (size_t)nimg * GCfg<KK, float>::IMG);                          \
             const int smem = (int)(sizeof(float) * 8 * KK * KK * KK);                                          \
             MWB_CUDA(cudaFuncSetAttribute(k_ximage<KK, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)); \
@@ -1666,7 +1705,10 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     if (ctx->prof) MWB_CUDA(cudaEventRecord(ctx->ev0, s));
 #define L_AP(KK)                                                                                             \
     {                                                                                                        \
-        if (bp.precision == 2 && TCfg<KK>::FITS && !pencil && tc_prec_ok) {                                  \
+        if (hyb) {                                                                                           \
+            launch_happly<KK>(nchunks, d_chunks, d_items, d_trees, d_tkey, d_tval, d_csrc,                   \
+                              (const unsigned char*)d_ximg, nreal, d_partials, d_ntrip_tot, d_kerr, s);       \
+        } else if (bp.precision == 2 && TCfg<KK>::FITS && !pencil && tc_prec_ok) {                           \
             size_t smem = TCfg<KK>::SMEM;                                                                    \
             MWB_CUDA(cudaFuncSetAttribute(k_tapply<KK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
             k_tapply<KK><<<nchunks, TCfg<KK>::NTHR, smem, s>>>(d_chunks, d_items, d_trees, d_cdelta, d_csrc,     \
@@ -1725,7 +1767,7 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     MWB_CUDA(cudaMemcpyAsync(ntot, d_ntrip_tot, sizeof(ntot), cudaMemcpyDeviceToHost, s));
     MWB_CUDA(cudaStreamSynchronize(s));
     if ((ntot[1] & 0xffffffffull) != 0)
-        throw Error(-2, "tensor-core contraction: an MMA completion wait exceeded its time limit");
+        throw Error(-2, "tensor-core contraction: an MMA or copy completion wait exceeded its time limit");
     if (ctx->prof) {
         float ms = 0.0f;
         MWB_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));

@@ -1,0 +1,645 @@
+// mw_happly.cuh -- line-ordered contraction of the NS-form apply with its x step on the fifth-generation
+// tensor cores (tcgen05.mma kind::f16, BF16 operands) and its y and z steps on the CUDA cores (FP32
+// products); every term's contribution is accumulated in FP64.  Included by mw_apply.cu after the Chunk /
+// Item / BTree records and k_gapply's helpers; same contract as k_gapply: one CTA per chunk of one output
+// node's triples sorted by (term, dz, dy), the sum written to the output block (or a partial slot)
+// with its norms.
+//
+// Operator application (reference src/treebuilders/ConvolutionCalculator.cpp: applyOperator ->
+// tensorXProd), grouped by line = (term, dz, dy) and plane = (term, dz):
+//     out += sum_dz beta Mz(dz) [ sum_dy My(dy) [ sum_dx Mx(dx) in_(dx,dy,dz) ] ]
+//
+// x step (tensor cores).  One GEMM per triple, D[(y, z)][x'] += sum_x X[(y, z)][x] Mx[x'][x], with
+// M = the R = (2k)^2 data rows (y, z) in tiles of 128 TMEM lanes, K = x (16 per instruction) and
+// N = three column blocks of 2k: the data block and the operator are each written as three BF16 slices
+// of a per-row fixed-point form (mw_slice.hpp), and the operator slices are stacked along N so that
+//     data slice 0 x [m0 | m1 | m2],   data slice 1 x [0 | m0 | m1],   data slice 2 x [0 | 0 | m0]
+// put the products of equal weight 2^-16 / 2^-24 / 2^-32 into column blocks 0 / 1 / 2.  Within one
+// block row every block holds exact multiples of one quantum below 2^24 quanta, so the tensor core's
+// FP32 accumulation is exact inside a triple; the triples of a line accumulate in TMEM (the MMA
+// accumulate flag), and the line's epilogue adds the three blocks (round to nearest) into the y step's
+// operand.  Products dropped by the scheme (slice pairs of weight <= 2^-40 of the row scales) and the
+// slicing remainder (2^-25 of the row maximum) are below FP32 rounding of the same products.
+// Staging: each triple's data image (built once per pass by k_simage) and operator image travel by one
+// 1-D bulk copy each (cp.async.bulk, completion on an mbarrier) into one of two buffers; the copy for
+// the next triple overlaps the current triple's MMAs.  At a line's end the MMAs of the next line's first
+// triple are issued before the CUDA cores start this line's y and z steps, so both units work at once.
+//
+// y and z steps (CUDA cores), as in k_gapply: register-tiled GEMMs on shared operands, one thread per
+// MT x NT output tile (MT = NT = 2k/4 rounded up), FP32 products; the y step sums a plane's lines in
+// shared memory, the z step adds each plane (beta-scaled operator) into FP64 accumulators in TMEM.
+// Operand rows use the split column layout of mw_slice.hpp, so a thread's tile row is one 16-byte load
+// and one 4-byte load.
+//
+// Below the root the s->s block (T x T x T on the scaling part) is left out, as in k_gapply: the k^3
+// correction GEMMs run on the CUDA cores, their input rebuilt from the data slices.
+//
+// Every mbarrier wait has a time limit: a wait that runs out sets the kernel's error word, and the CTA
+// leaves after waiting (again with a limit) for the copies and MMAs it started.
+#pragma once
+#include "mw_slice.hpp"
+#include "mw_umma.cuh"
+
+namespace mwb {
+
+template <int K>
+struct HCfg {
+    static constexpr int K2 = 2 * K;
+    static constexpr int KP = (K2 + 3) / 4 * 4;  // 16 or 20
+    static constexpr int NN = KP * KP;
+    static constexpr int MT = KP / 4, NT = KP / 4;  // CUDA-core tiles of the y and z steps
+    static constexpr int NTILE = NN / NT;           // column tiles: 4 KP
+    static constexpr int NWARP = NTILE / 8;         // CUDA-core warps; one more warp stages and issues MMAs
+    static constexpr int NTHR_S = 32 * NWARP;
+    static constexpr int NTHR = NTHR_S + 32;
+    static constexpr int ND = MT * NT;
+    static constexpr int LDT = NN + 4;  // row stride of T1 and T2 (split column layout)
+    static constexpr int MATP = KP * KP;
+    // x step
+    static constexpr int R = K2 * K2;
+    static constexpr int TILES = (R + 127) / 128;
+    static constexpr int NCH = (K2 + 7) / 8;
+    static constexpr int KSTEPS = (NCH + 1) / 2;
+    static constexpr bool PADCH = 2 * KSTEPS > NCH;  // the last K step reads one chunk past the slice
+    static constexpr int W = K2;
+    static constexpr int NCOL = (3 * W + 15) / 16 * 16;
+    static constexpr int TSTR = (NCOL + 31) / 32 * 32;  // TMEM columns per lane tile
+    static constexpr int NB = 2 * W + NCOL;
+    static constexpr int SLICE = NCH * R * 16;
+    static constexpr int IMGB = 3 * SLICE;
+    // s->s block of the x step (x', x < k; data rows y, z < k)
+    static constexpr int W2 = K;
+    static constexpr int NCOL2 = (3 * W2 + 15) / 16 * 16;
+    static constexpr int TSTR2 = (NCOL2 + 31) / 32 * 32;
+    static constexpr int NB2 = 2 * W2 + NCOL2;
+    static constexpr int OPB_MAIN = 2 * KSTEPS * NB * 16;
+    static constexpr int OPB = OPB_MAIN + 2 * NB2 * 16;
+    static constexpr int BUF = (IMGB + OPB + 127) / 128 * 128;
+    static constexpr int ZC = TILES * 128 * 16;  // zero chunk: the padding chunk of the last slice
+    // generated (scaling-only) inputs, and the s->s block: rows y, z < k, x < k only
+    static constexpr int TILES_GEN = (K + K2 * (K - 1) + 127) / 128;
+    static constexpr int KSTEPS_GEN = (K + 15) / 16;
+    // TMEM: x sums [0, COLC), s->s x sums [COLC, ACC0), FP64 accumulators after (warps of one lane quarter
+    // side by side)
+    static constexpr int COLC = TILES * TSTR;
+    static constexpr int ACC0 = COLC + TILES_GEN * TSTR2;
+    static constexpr int NWQ = (NWARP + 3) / 4;
+    static constexpr int TCOLS_NEED = ACC0 + NWQ * 2 * ND;
+    static constexpr int TCOLS = TCOLS_NEED <= 128 ? 128 : TCOLS_NEED <= 256 ? 256 : 512;
+    // s->s correction of the y and z steps
+    static constexpr int KK = K * K, KKK = K * K * K;
+    static constexpr int NC = gcfg_nc(K, NTHR_S);
+    static constexpr int NCT = KK / NC;
+    static constexpr int MAXT = 128;  // triples per chunk whose records are kept in shared memory
+    static constexpr size_t SMEM = 2 * (size_t)BUF + ZC +
+                                   sizeof(float) * (2 * (size_t)KP * LDT + 2 * MATP + 3 * KKK) + MAXT * 24 + 128;
+    static constexpr bool FITS = (KP == 16 || KP == 20) && KSTEPS <= 2 && KSTEPS_GEN == 1 && NCOL <= 256 &&
+                                 TCOLS_NEED <= 512 && SMEM + 1024 <= 232448 && 2 * NCT <= NTHR_S &&
+                                 R < (1 << 14) && NB < (1 << 14) && K <= 16;
+};
+
+// Block images of the tensor-core x step, one CTA per block: the FP64 block (or the generated k^3
+// scaling block) is read coalesced, every data row (y, z) is sliced (mw_slice.hpp) and written as
+// 16-byte chunks of 8 x values.  Slot numbering as k_ximage.
+template <int K>
+__global__ void __launch_bounds__(256) k_simage(const ImgSrc* __restrict__ srcs, int nsrc, const double* __restrict__ gblk,
+                                                long long nreal, unsigned char* __restrict__ img) {
+    using C = HCfg<K>;
+    constexpr int K2 = C::K2, R = C::R, NCH = C::NCH, BS = K2 * K2 * K2, KKK = K * K * K;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    double* blk = reinterpret_cast<double*>(smraw);
+    const long long slot = blockIdx.x;
+    if (slot < nreal) {
+        int lo = 0, hi = nsrc - 1;  // last entry with base <= slot
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (srcs[mid].base <= slot) lo = mid;
+            else hi = mid - 1;
+        }
+        const ImgSrc sr = srcs[lo];
+        const double* b = sr.coef + (size_t)(sr.lb + (slot - sr.base)) * BS;
+        for (int e = threadIdx.x; e < BS; e += blockDim.x) blk[e] = b[e];
+    } else {
+        const double* g = gblk + (size_t)(slot - nreal) * KKK;
+        for (int e = threadIdx.x; e < BS; e += blockDim.x) {
+            const int a = e % K2, bb = (e / K2) % K2, c = e / (K2 * K2);
+            blk[e] = (a < K && bb < K && c < K) ? g[a + K * (bb + K * c)] : 0.0;
+        }
+    }
+    __syncthreads();
+    unsigned char* out = img + (size_t)slot * C::IMGB;
+    for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        float s[3][8 * NCH];
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+#pragma unroll
+            for (int x = 0; x < 8 * NCH; ++x) s[q][x] = 0.0f;
+        slice3_row(blk + (size_t)K2 * r, K2, 1, s[0], s[1], s[2]);
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+#pragma unroll
+            for (int c = 0; c < NCH; ++c) {
+                uint32_t w[4];
+#pragma unroll
+                for (int h = 0; h < 4; ++h)
+                    w[h] = (uint32_t)bf16_bits_exact(s[q][8 * c + 2 * h]) |
+                           ((uint32_t)bf16_bits_exact(s[q][8 * c + 2 * h + 1]) << 16);
+                *reinterpret_cast<uint4*>(out + (size_t)q * C::SLICE + ((size_t)c * R + r) * 16) =
+                    make_uint4(w[0], w[1], w[2], w[3]);
+            }
+    }
+}
+
+__device__ __forceinline__ float bf16_to_f32(uint16_t h) { return __uint_as_float((uint32_t)h << 16); }
+
+// c[i][j] (+)= sum_{k < kdim} A[k][o0 + i] B[k][n0 + j] with A rows in the split layout of MT-tiles
+// (4 row tiles) and B rows in the split layout of NT-tiles (NTILE tiles); a thread tile is (rt, ct)
+template <int MT, int NT, int NTILE, bool ACC>
+__device__ __forceinline__ void gemm_tile_split(const float* __restrict__ A, int lda, const float* __restrict__ B,
+                                                int ldb, int rt, int ct, int kdim, float (&c)[MT][NT]) {
+    static_assert(MT == 4 || MT == 5, "tile");
+    static_assert(NT == 4 || NT == 5, "tile");
+    if (!ACC) {
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NT; ++j) c[i][j] = 0.0f;
+    }
+    const float* ap = A + 4 * rt;
+    const float* bp = B + 4 * ct;
+#pragma unroll 2
+    for (int k = 0; k < kdim; ++k) {
+        float a[MT], b[NT];
+        const float4 av = *reinterpret_cast<const float4*>(ap);
+        a[0] = av.x;
+        a[1] = av.y;
+        a[2] = av.z;
+        a[3] = av.w;
+        if constexpr (MT == 5) a[4] = ap[16 - 3 * rt];  // A + 16 + rt
+        const float4 bv = *reinterpret_cast<const float4*>(bp);
+        b[0] = bv.x;
+        b[1] = bv.y;
+        b[2] = bv.z;
+        b[3] = bv.w;
+        if constexpr (NT == 5) b[4] = bp[4 * NTILE - 3 * ct];  // B + 4 NTILE + ct
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < NT; ++j) c[i][j] = fmaf(a[i], b[j], c[i][j]);
+        ap += lda;
+        bp += ldb;
+    }
+}
+
+// record of one triple of a chunk, kept in shared memory for the first MAXT triples
+struct HTri {
+    uint32_t lkey;  // term << 20 | dz rank << 10 | dy rank (line = equal key, plane = equal key >> 10)
+    int slot;       // block image slot of the input node
+    int mx, my, mz;
+    int gen;        // generated (scaling-only) input
+};
+
+__device__ __forceinline__ void named_bar(int id, int nthr) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthr) : "memory");
+}
+// barrier of `nthr` threads on `id` that returns whether any of them passed a nonzero `pred`
+__device__ __forceinline__ int named_bar_or(int id, int nthr, int pred) {
+    int r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\tsetp.ne.s32 p, %1, 0;\n\tbar.red.or.pred q, %2, %3, p;\n\tselp.s32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"(pred), "r"(id), "r"(nthr)
+        : "memory");
+    return r;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr_u32(bar)) : "memory");
+}
+
+// Warp roles: warps 0 .. NWARP-1 run the epilogues and the y and z steps (CUDA cores); warp NWARP
+// (one thread) stages every triple and issues its MMAs.  mbarriers between them:
+//   staged[b]   the bulk copies of buffer b landed              (producer -> producer)
+//   mma_done[b] the MMAs reading buffer b completed              (tcgen05.commit -> producer)
+//   line_done   the MMAs of the current line completed           (tcgen05.commit -> CUDA-core warps)
+//   sums_free   the line's x sums were read out of TMEM          (one CUDA-core thread -> producer)
+// Each has at most one completed phase that its waiter has not yet consumed, so parities never skip.
+template <int K>
+__global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
+    k_happly(const Chunk* __restrict__ chunks, const Item* __restrict__ items, const BTree* __restrict__ trees,
+             const unsigned long long* __restrict__ tkey, const unsigned long long* __restrict__ tval,
+             const int* __restrict__ csrc, const unsigned char* __restrict__ simg, long long gbase, double* partials,
+             unsigned long long* ntrip_out, int* err_out) {
+    using C = HCfg<K>;
+    constexpr int K2 = C::K2, KP = C::KP, MT = C::MT, NT = C::NT, NTILE = C::NTILE, ND = C::ND, NC = C::NC;
+    constexpr int LDT = C::LDT, MATP = C::MATP, KK = C::KK, KKK = C::KKK, R = C::R, W = C::W, W2 = C::W2;
+    constexpr int NS = C::NTHR_S;
+    constexpr int BS = K2 * K2 * K2;
+    constexpr uint64_t kWaitNs = 2000000000ull;  // per mbarrier wait
+    extern __shared__ __align__(16) unsigned char smraw[];  // 16-byte aligned: all the no-swizzle operands and bulk copies need
+    __shared__ uint32_t tmem_slot;
+    __shared__ __align__(8) uint64_t bars[6];  // staged[2], mma_done[2], line_done, sums_free
+    __shared__ int s_bad;
+    unsigned char* bufs[2] = {smraw, smraw + C::BUF};
+    unsigned char* zc = smraw + 2 * (size_t)C::BUF;
+    float* T1 = reinterpret_cast<float*>(zc + C::ZC);  // [KP][LDT], split columns
+    float* T2 = T1 + KP * LDT;
+    float* My = T2 + KP * LDT;  // [KP][split o]: My[b'][b] at (b, o = b')
+    float* Mz = My + MATP;
+    float* U1 = Mz + MATP;  // [K][K][K]
+    float* U2 = U1 + KKK;
+    float* Uc = U2 + KKK;
+    HTri* meta = reinterpret_cast<HTri*>(Uc + KKK);
+    const Chunk ch = chunks[blockIdx.x];
+    const Item it = items[ch.item];
+    const BTree& TR = trees[it.tree];
+    const bool root = TR.root != 0;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, quarter = warp & 3;
+    const int ntri = ch.c1 - ch.c0;
+
+    auto load_rec = [&](int t) -> HTri {
+        const unsigned long long tv = tval[t];
+        const int src = csrc[(int)(tv >> 32)];
+        const TermRec tr = TR.terms[(int)(tv & 0xffffffffull)];
+        HTri h;
+        h.lkey = (uint32_t)(tkey[t] & 0xffffffffull);
+        h.slot = (int)(src < 0 ? gbase + (-src - 1) : TR.img_base + (src - TR.img_lb));
+        h.mx = tr.mx;
+        h.my = tr.my;
+        h.mz = tr.mz;
+        h.gen = src < 0;
+        return h;
+    };
+    for (int e = tid; e < min(ntri, C::MAXT); e += C::NTHR) meta[e] = load_rec(ch.c0 + e);
+    auto rec = [&](int t) -> HTri { return t - ch.c0 < C::MAXT ? meta[t - ch.c0] : load_rec(t); };
+
+    if (warp == 0) {
+        tmem_alloc(&tmem_slot, C::TCOLS);
+        tmem_relinquish();
+    }
+    if (tid == 0) {
+        for (int i = 0; i < 6; ++i) mbar_init(&bars[i], 1);
+        mbar_fence_init();
+        s_bad = 0;
+    }
+    for (int e = tid; e < C::ZC / 16; e += C::NTHR) *reinterpret_cast<uint4*>(zc + 16 * e) = make_uint4(0u, 0u, 0u, 0u);
+    fence_proxy_async_smem();
+    tmem_fence_before_sync();
+    __syncthreads();
+    tmem_fence_after_sync();
+    const uint32_t tbase = tmem_slot;
+    int bad = 0;
+
+    if (warp == C::NWARP) {
+        // ================= producer: staging and MMAs (one thread) =================
+        if (lane == 0) {
+            uint32_t fph = 0, mph = 0, dph = 0;
+            bool spend[2] = {false, false}, mpend[2] = {false, false};
+            auto stage = [&](const HTri& h, int b) {
+                mbar_arrive_expect_tx(&bars[b], (uint32_t)(C::IMGB + C::OPB));
+                bulk_g2s(bufs[b], simg + (size_t)h.slot * C::IMGB, C::IMGB, &bars[b]);
+                bulk_g2s(bufs[b] + C::IMGB, TR.matsX + (size_t)h.mx * C::OPB, C::OPB, &bars[b]);
+                spend[b] = true;
+            };
+            // x-step MMAs of the triple in buffer b into the line's TMEM sums; a generated input is zero
+            // outside its first TILES_GEN tiles and first K step, but the first triple of a line clears
+            // every tile; below the root also the s->s block's sums (x', x < k; first TILES_GEN tiles)
+            auto issue = [&](int b, bool first, bool gen) {
+                const uint32_t base = smem_addr_u32(bufs[b]);
+                const uint32_t zca = smem_addr_u32(zc);
+                constexpr uint32_t idesc = umma_idesc_bf16(128, C::NCOL);
+                constexpr uint32_t idesc2 = umma_idesc_bf16(128, C::NCOL2);
+#pragma unroll 1
+                for (int tl = 0; tl < C::TILES; ++tl) {
+                    const bool live = !gen || tl < C::TILES_GEN;
+                    const int nks = gen ? C::KSTEPS_GEN : C::KSTEPS;
+#pragma unroll 1
+                    for (int kq = 0; kq < nks; ++kq)
+#pragma unroll
+                        for (int s = 0; s < 3; ++s) {
+                            if (!live && !(first && kq == 0 && s == 0)) continue;
+                            const uint32_t a = base + s * C::SLICE + 2 * kq * R * 16 + tl * 2048;
+                            // the last slice's padding chunk is the zero chunk (the other slices' is the
+                            // next slice's first chunk, which the zero operator rows cancel)
+                            const uint32_t lbo = (C::PADCH && kq == C::KSTEPS - 1 && s == 2) ? zca + tl * 2048 - a : R * 16;
+                            const uint64_t ad = umma_sdesc(a, lbo, 128);
+                            const uint64_t bd = umma_sdesc(base + C::IMGB + 2 * kq * C::NB * 16 + (2 - s) * W * 16,
+                                                           C::NB * 16, 128);
+                            umma_bf16(tbase + (uint32_t)(tl * C::TSTR), ad, bd, idesc,
+                                      (first && kq == 0 && s == 0) ? 0u : 1u);
+                        }
+                }
+                if (!root) {
+#pragma unroll 1
+                    for (int tl = 0; tl < C::TILES_GEN; ++tl)
+#pragma unroll
+                        for (int s = 0; s < 3; ++s) {
+                            const uint64_t ad = umma_sdesc(base + s * C::SLICE + tl * 2048, R * 16, 128);
+                            const uint64_t bd = umma_sdesc(base + C::IMGB + C::OPB_MAIN + (2 - s) * W2 * 16,
+                                                           C::NB2 * 16, 128);
+                            umma_bf16(tbase + (uint32_t)(C::COLC + tl * C::TSTR2), ad, bd, idesc2,
+                                      (first && s == 0) ? 0u : 1u);
+                        }
+                }
+            };
+            if (ntri > 0) stage(rec(ch.c0), 0);
+            if (ntri > 1) stage(rec(ch.c0 + 1), 1);
+            for (int t = ch.c0; t < ch.c1; ++t) {
+                const int b = (t - ch.c0) & 1;
+                const HTri h = rec(t);
+                const bool lstart = t == ch.c0 || rec(t - 1).lkey != h.lkey;
+                const bool lend = t + 1 == ch.c1 || rec(t + 1).lkey != h.lkey;
+                if (!mbar_wait(&bars[b], (fph >> b) & 1u, kWaitNs)) bad = 1;
+                fph ^= 1u << b;
+                spend[b] = false;
+                if (!bad && lstart && t != ch.c0) {  // the previous line's sums are read out
+                    if (!mbar_wait(&bars[5], dph, kWaitNs)) bad = 1;
+                    dph ^= 1u;
+                }
+                if (bad || *reinterpret_cast<volatile int*>(&s_bad)) {
+                    bad = 1;
+                    break;
+                }
+                tmem_fence_after_sync();
+                issue(b, lstart, h.gen != 0);
+                umma_commit(&bars[2 + b]);
+                mpend[b] = true;
+                if (lend) umma_commit(&bars[4]);
+                if (t + 2 < ch.c1) {  // refill buffer b once its MMAs are done
+                    if (!mbar_wait(&bars[2 + b], (mph >> b) & 1u, kWaitNs)) {
+                        bad = 1;
+                        break;
+                    }
+                    mph ^= 1u << b;
+                    mpend[b] = false;
+                    stage(rec(t + 2), b);
+                    if (t + 3 < ch.c1) prefetch_l2_bulk(simg + (size_t)rec(t + 3).slot * C::IMGB, C::IMGB);
+                }
+            }
+            for (int b = 0; b < 2; ++b) {  // leave only after this thread's copies and MMAs have landed
+                if (spend[b] && !mbar_wait(&bars[b], (fph >> b) & 1u, kWaitNs)) bad = 1;
+                if (mpend[b] && !mbar_wait(&bars[2 + b], (mph >> b) & 1u, kWaitNs)) bad = 1;
+            }
+            if (bad) atomicExch(&s_bad, 1);
+        }
+        __syncwarp();
+    } else {
+        // ================= CUDA-core warps: epilogues, y and z steps =================
+        const int rt = lane & 3, ct = warp * 8 + (lane >> 2);
+        const int o0 = rt * MT, n0 = ct * NT;
+        const int tb0 = n0 % KP, tc0 = n0 / KP;  // y tile: first a', c;  z tile: first a', b'
+        const int crt = tid & 1, cct = tid >> 1;
+        const bool cown = !root && cct < C::NCT;
+        const int co0 = crt * MT, cn0 = cown ? cct * NC : 0;
+        auto opos = [](int o) { return split_pos(o, MT, 4); };  // operator column of output index o
+        const uint32_t tlane = tbase + ((uint32_t)(32 * quarter) << 16);
+        const uint32_t tacc = tlane + (uint32_t)(C::ACC0 + (warp >> 2) * 2 * ND);
+        tmem_visit<ND, true>(tacc, [&](int, int n, auto& r) {
+#pragma unroll
+            for (int q = 0; q < 2 * n; ++q) r[q] = 0u;
+        });
+        auto load_mat = [&](float* dst, const float* tab, int mi) {
+            constexpr int NV = MATP * 4 / 16;
+            const char* src = reinterpret_cast<const char*>(tab + (size_t)mi * MATP);
+            for (int e = tid; e < NV; e += NS) cp_async16(reinterpret_cast<char*>(dst) + 16 * e, src + 16 * e);
+            cp_async_commit();
+        };
+        auto uc_at = [&](int i, int j) -> double {
+            const int cz = o0 + i, n = n0 + j, ax = n % KP, by = n / KP;
+            return (cz < K && ax < K && by < K) ? (double)Uc[cz * KK + ax + K * by] : 0.0;
+        };
+        float c2[MT][NC];
+        auto write_c2 = [&]() {
+            if (!cown) return;
+#pragma unroll
+            for (int i = 0; i < MT; ++i)
+#pragma unroll
+                for (int j = 0; j < NC; ++j)
+                    if (co0 + i < K) Uc[(co0 + i) * KK + cn0 + j] = c2[i][j];
+        };
+        const int nq = (C::NWARP - quarter + 3) / 4;  // warps of this lane quarter
+        uint32_t lph = 0;
+        bool pend2 = false, uc_valid = false, plane_gen = true, first_line = true;
+        int t = ch.c0;
+        while (t < ch.c1) {
+            const HTri h0 = rec(t);
+            int l1 = t + 1;
+            bool lgen = h0.gen != 0;
+            while (l1 < ch.c1) {
+                const HTri h = rec(l1);
+                if (h.lkey != h0.lkey) break;
+                lgen = lgen && h.gen != 0;
+                ++l1;
+            }
+            const bool pstart = t == ch.c0 || (rec(t - 1).lkey >> 10) != (h0.lkey >> 10);
+            const bool pend = l1 == ch.c1 || (rec(l1).lkey >> 10) != (h0.lkey >> 10);
+            if (pstart) {
+                plane_gen = true;
+                first_line = true;
+            }
+            plane_gen = plane_gen && lgen;
+            named_bar(1, NS);  // readers of T1, My, U1 (last line) and of Mz, T2, U2 (last plane) are done
+            load_mat(My, TR.matsS32, h0.my);
+            if (pend) load_mat(Mz, TR.matsbS32, h0.mz);
+            if (!mbar_wait(&bars[4], lph, kWaitNs)) bad = 1;
+            bad = __any_sync(0xffffffffu, bad);  // warp-uniform: the TMEM loads below are warp-collective
+            lph ^= 1u;
+            tmem_fence_after_sync();
+            // ---- epilogue: the line's x sums (three column blocks) -> T1 [y][x' + P z], s->s sums -> U1
+            if (!bad) {
+#pragma unroll 1
+                for (int tl = warp >> 2; tl < C::TILES; tl += nq) {
+                    uint32_t v[3 * W];
+                    tmem_span_ld<0, 3 * W>(tlane + (uint32_t)(tl * C::TSTR), v);
+                    tmem_span_wait<0, 3 * W>(v);
+                    const int r = 128 * tl + 32 * quarter + lane;
+                    if (r < R) {
+                        const int y = r % K2, z = r / K2;
+                        float o[KP];
+#pragma unroll
+                        for (int x = 0; x < KP; ++x)
+                            o[x] = x < W ? __uint_as_float(v[x]) + (__uint_as_float(v[W + x]) + __uint_as_float(v[2 * W + x]))
+                                         : 0.0f;
+                        float* row = T1 + y * LDT;
+                        constexpr int TPR = KP / NT;  // column tiles per z
+#pragma unroll
+                        for (int u = 0; u < TPR; ++u)
+                            *reinterpret_cast<float4*>(row + 4 * (TPR * z + u)) =
+                                make_float4(o[NT * u], o[NT * u + 1], o[NT * u + 2], o[NT * u + 3]);
+                        if constexpr (NT == 5)
+                            *reinterpret_cast<float4*>(row + 4 * NTILE + TPR * z) = make_float4(o[4], o[9], o[14], o[19]);
+                    }
+                }
+                if (!root) {
+#pragma unroll 1
+                    for (int tl = warp >> 2; tl < C::TILES_GEN; tl += nq) {
+                        uint32_t v[3 * W2];
+                        tmem_span_ld<0, 3 * W2>(tlane + (uint32_t)(C::COLC + tl * C::TSTR2), v);
+                        tmem_span_wait<0, 3 * W2>(v);
+                        const int r = 128 * tl + 32 * quarter + lane;
+                        const int y = r % K2, z = r / K2;
+                        if (y < K && z < K) {
+#pragma unroll
+                            for (int x = 0; x < W2; ++x)
+                                U1[y * KK + x + K * z] =
+                                    __uint_as_float(v[x]) + (__uint_as_float(v[W2 + x]) + __uint_as_float(v[2 * W2 + x]));
+                        }
+                    }
+                }
+            }
+            tmem_fence_before_sync();
+            cp_async_wait_all();
+            bad = named_bar_or(1, NS, bad || *reinterpret_cast<volatile int*>(&s_bad));  // T1, U1, My, Mz are in
+            if (tid == 0) mbar_arrive(&bars[5]);  // the producer may start the next line's MMAs
+            if (bad) break;
+            // ---- y: T2[c][a' + P b'] (+)= sum_b My[b'][b] T1[b][a' + P c]   (a plane sums its lines)
+            if (pend2) {  // the previous plane's correction block, subtracted in this plane's z phase
+                write_c2();
+                pend2 = false;
+                uc_valid = true;
+            }
+            {
+                const bool zero = lgen && !(tc0 < K);
+                if (!zero || first_line) {
+                    float c[MT][NT];
+                    if (zero) {
+#pragma unroll
+                        for (int i = 0; i < MT; ++i)
+#pragma unroll
+                            for (int j = 0; j < NT; ++j) c[i][j] = 0.0f;
+                    } else {
+                        gemm_tile_split<MT, NT, NTILE, false>(My, KP, T1, LDT, rt, ct, lgen ? K : K2, c);
+                    }
+#pragma unroll
+                    for (int i = 0; i < MT; ++i) {
+                        const int m = tb0 + KP * (o0 + i);  // column a' + P b' of the tile's first value
+                        float* row = T2 + tc0 * LDT;
+                        float4* p4 = reinterpret_cast<float4*>(row + 4 * (m / NT));
+                        float4 v = first_line ? make_float4(0.f, 0.f, 0.f, 0.f) : *p4;
+                        v.x += c[i][0];
+                        v.y += c[i][1];
+                        v.z += c[i][2];
+                        v.w += c[i][3];
+                        *p4 = v;
+                        if constexpr (NT == 5) {
+                            float& s = row[4 * NTILE + m / NT];
+                            s = first_line ? c[i][4] : s + c[i][4];
+                        }
+                    }
+                }
+            }
+            if (cown) {  // U2[c][a' + k b'] (+)= sum_{b<k} Ty[b'][b] U1[b][a' + k c]
+                float cc[MT][NC];
+#pragma unroll
+                for (int i = 0; i < MT; ++i)
+#pragma unroll
+                    for (int j = 0; j < NC; ++j) cc[i][j] = 0.0f;
+                for (int b = 0; b < K; ++b) {
+#pragma unroll
+                    for (int i = 0; i < MT; ++i) {
+                        const float m = My[b * KP + opos(co0 + i)];
+#pragma unroll
+                        for (int j = 0; j < NC; ++j) cc[i][j] = fmaf(m, U1[b * KK + cn0 + j], cc[i][j]);
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < MT; ++i)
+#pragma unroll
+                    for (int j = 0; j < NC; ++j) {
+                        const int n = cn0 + j;
+                        if (co0 + i < K) {
+                            float& d = U2[(n / K) * KK + (n % K) + K * (co0 + i)];
+                            d = first_line ? cc[i][j] : d + cc[i][j];
+                        }
+                    }
+            }
+            first_line = false;
+            t = l1;
+            if (!pend) continue;
+            named_bar(1, NS);  // T2, U2 and Uc of the plane are complete
+            // ---- z: acc[c'][a' + P b'] += sum_c (beta Mz)[c'][c] T2[c][a' + P b']  (- previous correction)
+            {
+                float c[MT][NT];
+                gemm_tile_split<MT, NT, NTILE, false>(Mz, KP, T2, LDT, rt, ct, plane_gen ? K : K2, c);
+                const bool fold = uc_valid;
+                tmem_visit<ND, true>(tacc, [&](int d0, int n, auto& r) {
+#pragma unroll
+                    for (int q2 = 0; q2 < n; ++q2) {
+                        const int d = d0 + q2, i = d / NT, j = d % NT;
+                        double v = words_to_double(r[2 * q2], r[2 * q2 + 1]) + (double)c[i][j];
+                        if (fold) v -= uc_at(i, j);
+                        double_to_words(v, r[2 * q2], r[2 * q2 + 1]);
+                    }
+                });
+            }
+            uc_valid = false;
+            if (cown) {  // c2[c'][a' + k b'] = sum_{c<k} (beta Tz)[c'][c] U2[c][a' + k b']
+#pragma unroll
+                for (int i = 0; i < MT; ++i)
+#pragma unroll
+                    for (int j = 0; j < NC; ++j) c2[i][j] = 0.0f;
+                for (int cz = 0; cz < K; ++cz) {
+#pragma unroll
+                    for (int i = 0; i < MT; ++i) {
+                        const float m = Mz[cz * KP + opos(co0 + i)];
+#pragma unroll
+                        for (int j = 0; j < NC; ++j) c2[i][j] = fmaf(m, U2[cz * KK + cn0 + j], c2[i][j]);
+                    }
+                }
+            }
+            pend2 = !root;
+        }
+        cp_async_wait_all();
+        named_bar(1, NS);
+        if (!bad && pend2) write_c2();
+        uc_valid = pend2;
+        named_bar(1, NS);
+        if (!bad) {
+            double* dst = ch.slot < 0 ? TR.ocoef + (size_t)it.node * BS : partials + (size_t)ch.slot * BS;
+            double n2 = 0.0, w2 = 0.0;
+            tmem_visit<ND, false>(tacc, [&](int d0, int n, auto& r) {
+#pragma unroll
+                for (int q2 = 0; q2 < n; ++q2) {
+                    const int d = d0 + q2, i = d / NT, j = d % NT;
+                    double v = words_to_double(r[2 * q2], r[2 * q2 + 1]);
+                    const int cz = o0 + i, nn = n0 + j, ax = nn % KP, by = nn / KP;
+                    if (uc_valid) v -= uc_at(i, j);
+                    if (cz < K2 && ax < K2 && by < K2) {
+                        dst[ax + K2 * (by + K2 * cz)] = v;
+                        n2 += v * v;
+                        if (!(ax < K && by < K && cz < K)) w2 += v * v;
+                    }
+                }
+            });
+            // per-warp partial norms into the zero chunk (no longer read)
+            for (int o = 16; o; o >>= 1) {
+                n2 += __shfl_down_sync(0xffffffffu, n2, o);
+                w2 += __shfl_down_sync(0xffffffffu, w2, o);
+            }
+            if (lane == 0) {
+                reinterpret_cast<double*>(zc)[warp] = n2;
+                reinterpret_cast<double*>(zc)[32 + warp] = w2;
+            }
+        }
+    }
+    tmem_fence_before_sync();
+    bad = __syncthreads_or(bad || s_bad);
+    tmem_fence_after_sync();
+    if (warp == 0) tmem_dealloc(tbase, C::TCOLS);
+    if (bad) {
+        if (tid == 0) atomicExch(err_out, 1);
+        return;
+    }
+    if (tid == 0) {
+        double n2 = 0.0, w2 = 0.0;
+        for (int w = 0; w < C::NWARP; ++w) {
+            n2 += reinterpret_cast<const double*>(zc)[w];
+            w2 += reinterpret_cast<const double*>(zc)[32 + w];
+        }
+        if (ch.slot < 0) {
+            TR.onorm2[it.node] = n2;
+            TR.ownorm2[it.node] = w2;
+        }
+        atomicAdd(ntrip_out, (unsigned long long)ntri);
+    }
+}
+}  // namespace mwb

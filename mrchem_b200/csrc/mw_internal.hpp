@@ -45,8 +45,8 @@ struct Ctx {
     double apply_ms = 0.0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // contraction work per CTA: at most this many (output, input, term) triples, per engine (FP64, FP32,
-    // split-TF32); set by the caller or an autotuner (load balance against partial-block traffic)
-    int chunk_triples[3] = {48, 48, 48};
+    // split-TF32, BF16x3 tensor-core x step); set by the caller or an autotuner (load balance against partial-block traffic)
+    int chunk_triples[4] = {48, 48, 48, 48};
     // handles that point here (worlds, networks); a destroyed context is freed with the last of them
     int refs = 0;
     bool closed = false;
@@ -106,6 +106,13 @@ struct OpDepth {
     // 4 (n + 3 KP8 (k / 4)) + k % 4; plain and beta-scaled
     float* d_matsI = nullptr;
     float* d_matsbI = nullptr;
+    // tensor-core x step with CUDA-core y and z steps (k_happly, 2k <= 20 only): the FP32 transposed
+    // operators in the split column layout of its y/z tiles (entry [k][split_pos(o, P/4, 4)] = M[o][k]),
+    // plain and beta-scaled, and per matrix one image of its three BF16 slices (mw_slice.hpp, XGeo::OPB
+    // bytes)
+    float* d_matsS32 = nullptr;
+    float* d_matsbS32 = nullptr;
+    unsigned char* d_matsX = nullptr;
     DeltaRec* d_deltas = nullptr;
     TermRec* d_terms = nullptr;
 };
