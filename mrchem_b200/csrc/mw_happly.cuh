@@ -152,52 +152,52 @@ __global__ void __launch_bounds__(256) k_simage(const ImgSrc* __restrict__ srcs,
 
 __device__ __forceinline__ float bf16_to_f32(uint16_t h) { return __uint_as_float((uint32_t)h << 16); }
 
-// c[i][j] (+)= sum_{k < kdim} A[k][o0 + i] B[k][n0 + j] with A rows in the split layout of MT-tiles
-// (4 row tiles) and B rows in the split layout of NT-tiles (NTILE tiles); a thread tile is (rt, ct)
-template <int MT, int NT, int NTILE, bool ACC>
-__device__ __forceinline__ void gemm_tile_split(const float* __restrict__ A, int lda, const float* __restrict__ B,
-                                                int ldb, int rt, int ct, int kdim, float (&c)[MT][NT]) {
+// c[i][j] = sum_{k < KD} A[k][o0 + i] B[k][n0 + j] with A rows (stride LDA) in the split layout of
+// MT-tiles (4 row tiles) and B rows (stride LDB) in the split layout of NT-tiles (NTILE tiles); a thread
+// tile is (rt, ct).  Fully unrolled, so the loads of step k + 1 issue ahead of the FMAs of step k.
+template <int MT, int NT, int NTILE, int LDA, int LDB, int KD>
+__device__ __forceinline__ void gemm_tile_split(const float* __restrict__ A, const float* __restrict__ B, int rt, int ct,
+                                                float (&c)[MT][NT]) {
     static_assert(MT == 4 || MT == 5, "tile");
     static_assert(NT == 4 || NT == 5, "tile");
-    if (!ACC) {
 #pragma unroll
-        for (int i = 0; i < MT; ++i)
+    for (int i = 0; i < MT; ++i)
 #pragma unroll
-            for (int j = 0; j < NT; ++j) c[i][j] = 0.0f;
-    }
+        for (int j = 0; j < NT; ++j) c[i][j] = 0.0f;
     const float* ap = A + 4 * rt;
+    const float* a5 = A + 16 + rt;
     const float* bp = B + 4 * ct;
-#pragma unroll 2
-    for (int k = 0; k < kdim; ++k) {
+    const float* b5 = B + 4 * NTILE + ct;
+#pragma unroll
+    for (int k = 0; k < KD; ++k) {
         float a[MT], b[NT];
-        const float4 av = *reinterpret_cast<const float4*>(ap);
+        const float4 av = *reinterpret_cast<const float4*>(ap + k * LDA);
         a[0] = av.x;
         a[1] = av.y;
         a[2] = av.z;
         a[3] = av.w;
-        if constexpr (MT == 5) a[4] = ap[16 - 3 * rt];  // A + 16 + rt
-        const float4 bv = *reinterpret_cast<const float4*>(bp);
+        if constexpr (MT == 5) a[4] = a5[k * LDA];
+        const float4 bv = *reinterpret_cast<const float4*>(bp + k * LDB);
         b[0] = bv.x;
         b[1] = bv.y;
         b[2] = bv.z;
         b[3] = bv.w;
-        if constexpr (NT == 5) b[4] = bp[4 * NTILE - 3 * ct];  // B + 4 NTILE + ct
+        if constexpr (NT == 5) b[4] = b5[k * LDB];
 #pragma unroll
         for (int i = 0; i < MT; ++i)
 #pragma unroll
             for (int j = 0; j < NT; ++j) c[i][j] = fmaf(a[i], b[j], c[i][j]);
-        ap += lda;
-        bp += ldb;
     }
 }
 
 // record of one triple of a chunk, kept in shared memory for the first MAXT triples
 struct HTri {
-    uint32_t lkey;  // term << 20 | dz rank << 10 | dy rank (line = equal key, plane = equal key >> 10)
-    int slot;       // block image slot of the input node
+    int slot;  // block image slot of the input node
     int mx, my, mz;
-    int gen;        // generated (scaling-only) input
+    int flags;  // HT_* below
+    int pad;
 };
+enum { HT_GEN = 1, HT_LSTART = 2, HT_LEND = 4, HT_PSTART = 8, HT_PEND = 16 };
 
 __device__ __forceinline__ void named_bar(int id, int nthr) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthr) : "memory");
@@ -239,7 +239,6 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
     __shared__ uint32_t tmem_slot;
     __shared__ __align__(8) uint64_t bars[6];  // staged[2], mma_done[2], line_done, sums_free
     __shared__ int s_bad;
-    unsigned char* bufs[2] = {smraw, smraw + C::BUF};
     unsigned char* zc = smraw + 2 * (size_t)C::BUF;
     float* T1 = reinterpret_cast<float*>(zc + C::ZC);  // [KP][LDT], split columns
     float* T2 = T1 + KP * LDT;
@@ -256,17 +255,23 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, quarter = warp & 3;
     const int ntri = ch.c1 - ch.c0;
 
+    // the triple's input slot, operators and place in its line and plane (a line = equal key bits
+    // 0..31: term << 20 | dz rank << 10 | dy rank; a plane = equal bits 10..31)
     auto load_rec = [&](int t) -> HTri {
         const unsigned long long tv = tval[t];
         const int src = csrc[(int)(tv >> 32)];
         const TermRec tr = TR.terms[(int)(tv & 0xffffffffull)];
+        const uint32_t lk = (uint32_t)(tkey[t] & 0xffffffffull);
+        const uint32_t lp = t > ch.c0 ? (uint32_t)(tkey[t - 1] & 0xffffffffull) : ~lk;
+        const uint32_t ln = t + 1 < ch.c1 ? (uint32_t)(tkey[t + 1] & 0xffffffffull) : ~lk;
         HTri h;
-        h.lkey = (uint32_t)(tkey[t] & 0xffffffffull);
         h.slot = (int)(src < 0 ? gbase + (-src - 1) : TR.img_base + (src - TR.img_lb));
         h.mx = tr.mx;
         h.my = tr.my;
         h.mz = tr.mz;
-        h.gen = src < 0;
+        h.flags = (src < 0 ? HT_GEN : 0) | (lp != lk ? HT_LSTART : 0) | (ln != lk ? HT_LEND : 0) |
+                  ((lp >> 10) != (lk >> 10) ? HT_PSTART : 0) | ((ln >> 10) != (lk >> 10) ? HT_PEND : 0);
+        h.pad = 0;
         return h;
     };
     for (int e = tid; e < min(ntri, C::MAXT); e += C::NTHR) meta[e] = load_rec(ch.c0 + e);
@@ -294,51 +299,55 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
         if (lane == 0) {
             uint32_t fph = 0, mph = 0, dph = 0;
             bool spend[2] = {false, false}, mpend[2] = {false, false};
+            const uint32_t sbase = smem_addr_u32(smraw), zca = smem_addr_u32(zc);
             auto stage = [&](const HTri& h, int b) {
+                unsigned char* dst = smraw + (size_t)b * C::BUF;
                 mbar_arrive_expect_tx(&bars[b], (uint32_t)(C::IMGB + C::OPB));
-                bulk_g2s(bufs[b], simg + (size_t)h.slot * C::IMGB, C::IMGB, &bars[b]);
-                bulk_g2s(bufs[b] + C::IMGB, TR.matsX + (size_t)h.mx * C::OPB, C::OPB, &bars[b]);
+                bulk_g2s(dst, simg + (size_t)h.slot * C::IMGB, C::IMGB, &bars[b]);
+                bulk_g2s(dst + C::IMGB, TR.matsX + (size_t)h.mx * C::OPB, C::OPB, &bars[b]);
                 spend[b] = true;
             };
-            // x-step MMAs of the triple in buffer b into the line's TMEM sums; a generated input is zero
-            // outside its first TILES_GEN tiles and first K step, but the first triple of a line clears
-            // every tile; below the root also the s->s block's sums (x', x < k; first TILES_GEN tiles)
+            // x-step MMAs of the triple in buffer b into the line's TMEM sums, fully unrolled on descriptors
+            // prepared once per buffer (start addresses in 16-byte units); a generated input is zero outside
+            // its first TILES_GEN tiles and first K step, but the first triple of a line clears every tile;
+            // below the root also the s->s block's sums (x', x < k; first TILES_GEN tiles)
+            constexpr uint32_t idesc = umma_idesc_bf16(128, C::NCOL);
+            constexpr uint32_t idesc2 = umma_idesc_bf16(128, C::NCOL2);
             auto issue = [&](int b, bool first, bool gen) {
-                const uint32_t base = smem_addr_u32(bufs[b]);
-                const uint32_t zca = smem_addr_u32(zc);
-                constexpr uint32_t idesc = umma_idesc_bf16(128, C::NCOL);
-                constexpr uint32_t idesc2 = umma_idesc_bf16(128, C::NCOL2);
-#pragma unroll 1
-                for (int tl = 0; tl < C::TILES; ++tl) {
+                const uint32_t base = sbase + (uint32_t)(b * C::BUF);
+                const uint64_t da = umma_sdesc(base, R * 16, 128);
+                const uint32_t apad = base + 2 * C::SLICE + 2 * (C::KSTEPS - 1) * R * 16;
+                const uint64_t dp = umma_sdesc(apad, zca - apad, 128);
+                const uint64_t db = umma_sdesc(base + C::IMGB, C::NB * 16, 128);
+                static_for<C::TILES>([&](auto TL) {
+                    constexpr int tl = decltype(TL)::value;
                     const bool live = !gen || tl < C::TILES_GEN;
-                    const int nks = gen ? C::KSTEPS_GEN : C::KSTEPS;
-#pragma unroll 1
-                    for (int kq = 0; kq < nks; ++kq)
-#pragma unroll
-                        for (int s = 0; s < 3; ++s) {
-                            if (!live && !(first && kq == 0 && s == 0)) continue;
-                            const uint32_t a = base + s * C::SLICE + 2 * kq * R * 16 + tl * 2048;
-                            // the last slice's padding chunk is the zero chunk (the other slices' is the
-                            // next slice's first chunk, which the zero operator rows cancel)
-                            const uint32_t lbo = (C::PADCH && kq == C::KSTEPS - 1 && s == 2) ? zca + tl * 2048 - a : R * 16;
-                            const uint64_t ad = umma_sdesc(a, lbo, 128);
-                            const uint64_t bd = umma_sdesc(base + C::IMGB + 2 * kq * C::NB * 16 + (2 - s) * W * 16,
-                                                           C::NB * 16, 128);
-                            umma_bf16(tbase + (uint32_t)(tl * C::TSTR), ad, bd, idesc,
-                                      (first && kq == 0 && s == 0) ? 0u : 1u);
-                        }
-                }
+                    static_for<C::KSTEPS>([&](auto KQ) {
+                        constexpr int kq = decltype(KQ)::value;
+                        static_for<3>([&](auto SQ) {
+                            constexpr int sq = decltype(SQ)::value;
+                            const bool init = first && kq == 0 && sq == 0;
+                            if (!(live && (!gen || kq < C::KSTEPS_GEN)) && !init) return;
+                            constexpr bool pad = C::PADCH && kq == C::KSTEPS - 1 && sq == 2;
+                            const uint64_t ad = pad ? dp + (uint64_t)(tl * 128)
+                                                    : da + (uint64_t)((sq * C::SLICE + 2 * kq * R * 16 + tl * 2048) >> 4);
+                            const uint64_t bd = db + (uint64_t)((2 * kq * C::NB * 16 + (2 - sq) * W * 16) >> 4);
+                            umma_bf16(tbase + (uint32_t)(tl * C::TSTR), ad, bd, idesc, init ? 0u : 1u);
+                        });
+                    });
+                });
                 if (!root) {
-#pragma unroll 1
-                    for (int tl = 0; tl < C::TILES_GEN; ++tl)
-#pragma unroll
-                        for (int s = 0; s < 3; ++s) {
-                            const uint64_t ad = umma_sdesc(base + s * C::SLICE + tl * 2048, R * 16, 128);
-                            const uint64_t bd = umma_sdesc(base + C::IMGB + C::OPB_MAIN + (2 - s) * W2 * 16,
-                                                           C::NB2 * 16, 128);
+                    const uint64_t dc = umma_sdesc(base + C::IMGB + C::OPB_MAIN, C::NB2 * 16, 128);
+                    static_for<C::TILES_GEN>([&](auto TL) {
+                        constexpr int tl = decltype(TL)::value;
+                        static_for<3>([&](auto SQ) {
+                            constexpr int sq = decltype(SQ)::value;
+                            const uint64_t ad = da + (uint64_t)((sq * C::SLICE + tl * 2048) >> 4);
+                            const uint64_t bd = dc + (uint64_t)(((2 - sq) * W2 * 16) >> 4);
                             umma_bf16(tbase + (uint32_t)(C::COLC + tl * C::TSTR2), ad, bd, idesc2,
-                                      (first && s == 0) ? 0u : 1u);
-                        }
+                                      (first && sq == 0) ? 0u : 1u);
+                        });
+                    });
                 }
             };
             if (ntri > 0) stage(rec(ch.c0), 0);
@@ -346,8 +355,7 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
             for (int t = ch.c0; t < ch.c1; ++t) {
                 const int b = (t - ch.c0) & 1;
                 const HTri h = rec(t);
-                const bool lstart = t == ch.c0 || rec(t - 1).lkey != h.lkey;
-                const bool lend = t + 1 == ch.c1 || rec(t + 1).lkey != h.lkey;
+                const bool lstart = (h.flags & HT_LSTART) != 0;
                 if (!mbar_wait(&bars[b], (fph >> b) & 1u, kWaitNs)) bad = 1;
                 fph ^= 1u << b;
                 spend[b] = false;
@@ -360,18 +368,19 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
                     break;
                 }
                 tmem_fence_after_sync();
-                issue(b, lstart, h.gen != 0);
+                issue(b, lstart, (h.flags & HT_GEN) != 0);
                 umma_commit(&bars[2 + b]);
                 mpend[b] = true;
-                if (lend) umma_commit(&bars[4]);
+                if (h.flags & HT_LEND) umma_commit(&bars[4]);
                 if (t + 2 < ch.c1) {  // refill buffer b once its MMAs are done
+                    const HTri h2 = rec(t + 2);
                     if (!mbar_wait(&bars[2 + b], (mph >> b) & 1u, kWaitNs)) {
                         bad = 1;
                         break;
                     }
                     mph ^= 1u << b;
                     mpend[b] = false;
-                    stage(rec(t + 2), b);
+                    stage(h2, b);
                     if (t + 3 < ch.c1) prefetch_l2_bulk(simg + (size_t)rec(t + 3).slot * C::IMGB, C::IMGB);
                 }
             }
@@ -393,19 +402,24 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
         auto opos = [](int o) { return split_pos(o, MT, 4); };  // operator column of output index o
         const uint32_t tlane = tbase + ((uint32_t)(32 * quarter) << 16);
         const uint32_t tacc = tlane + (uint32_t)(C::ACC0 + (warp >> 2) * 2 * ND);
-        tmem_visit<ND, true>(tacc, [&](int, int n, auto& r) {
+        {
+            uint32_t z[2 * ND];
 #pragma unroll
-            for (int q = 0; q < 2 * n; ++q) r[q] = 0u;
-        });
+            for (int q = 0; q < 2 * ND; ++q) z[q] = 0u;
+            tmem_span_st<0, 2 * ND>(tacc, z);
+            tmem_wait_st();
+        }
         auto load_mat = [&](float* dst, const float* tab, int mi) {
             constexpr int NV = MATP * 4 / 16;
             const char* src = reinterpret_cast<const char*>(tab + (size_t)mi * MATP);
             for (int e = tid; e < NV; e += NS) cp_async16(reinterpret_cast<char*>(dst) + 16 * e, src + 16 * e);
             cp_async_commit();
         };
+        // correction value of element (c' = o0 + i, a' = tb0 + j, b' = tc0) of this thread's z tile (zero
+        // outside the s->s block; a tile never wraps a row since NT divides KP)
+        const bool tile_sss = o0 < K && tb0 < K && tc0 < K;
         auto uc_at = [&](int i, int j) -> double {
-            const int cz = o0 + i, n = n0 + j, ax = n % KP, by = n / KP;
-            return (cz < K && ax < K && by < K) ? (double)Uc[cz * KK + ax + K * by] : 0.0;
+            return (o0 + i < K && tb0 + j < K) ? (double)Uc[(o0 + i) * KK + tb0 + j + K * tc0] : 0.0;
         };
         float c2[MT][NC];
         auto write_c2 = [&]() {
@@ -419,24 +433,18 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
         const int nq = (C::NWARP - quarter + 3) / 4;  // warps of this lane quarter
         uint32_t lph = 0;
         bool pend2 = false, uc_valid = false, plane_gen = true, first_line = true;
-        int t = ch.c0;
-        while (t < ch.c1) {
+        bool lgen = true;
+        for (int t = ch.c0; t < ch.c1; ++t) {
             const HTri h0 = rec(t);
-            int l1 = t + 1;
-            bool lgen = h0.gen != 0;
-            while (l1 < ch.c1) {
-                const HTri h = rec(l1);
-                if (h.lkey != h0.lkey) break;
-                lgen = lgen && h.gen != 0;
-                ++l1;
-            }
-            const bool pstart = t == ch.c0 || (rec(t - 1).lkey >> 10) != (h0.lkey >> 10);
-            const bool pend = l1 == ch.c1 || (rec(l1).lkey >> 10) != (h0.lkey >> 10);
-            if (pstart) {
+            const bool pend = (h0.flags & HT_PEND) != 0;
+            if (h0.flags & HT_PSTART) {
                 plane_gen = true;
                 first_line = true;
             }
-            plane_gen = plane_gen && lgen;
+            if (h0.flags & HT_LSTART) lgen = true;
+            lgen = lgen && (h0.flags & HT_GEN) != 0;
+            plane_gen = plane_gen && (h0.flags & HT_GEN) != 0;
+            if (!(h0.flags & HT_LEND)) continue;
             named_bar(1, NS);  // readers of T1, My, U1 (last line) and of Mz, T2, U2 (last plane) are done
             load_mat(My, TR.matsS32, h0.my);
             if (pend) load_mat(Mz, TR.matsbS32, h0.mz);
@@ -506,8 +514,10 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
                         for (int i = 0; i < MT; ++i)
 #pragma unroll
                             for (int j = 0; j < NT; ++j) c[i][j] = 0.0f;
+                    } else if (lgen) {
+                        gemm_tile_split<MT, NT, NTILE, KP, LDT, K>(My, T1, rt, ct, c);
                     } else {
-                        gemm_tile_split<MT, NT, NTILE, false>(My, KP, T1, LDT, rt, ct, lgen ? K : K2, c);
+                        gemm_tile_split<MT, NT, NTILE, KP, LDT, K2>(My, T1, rt, ct, c);
                     }
 #pragma unroll
                     for (int i = 0; i < MT; ++i) {
@@ -553,23 +563,29 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
                     }
             }
             first_line = false;
-            t = l1;
             if (!pend) continue;
             named_bar(1, NS);  // T2, U2 and Uc of the plane are complete
             // ---- z: acc[c'][a' + P b'] += sum_c (beta Mz)[c'][c] T2[c][a' + P b']  (- previous correction)
             {
                 float c[MT][NT];
-                gemm_tile_split<MT, NT, NTILE, false>(Mz, KP, T2, LDT, rt, ct, plane_gen ? K : K2, c);
-                const bool fold = uc_valid;
-                tmem_visit<ND, true>(tacc, [&](int d0, int n, auto& r) {
+                if (plane_gen) gemm_tile_split<MT, NT, NTILE, KP, LDT, K>(Mz, T2, rt, ct, c);
+                else gemm_tile_split<MT, NT, NTILE, KP, LDT, K2>(Mz, T2, rt, ct, c);
+                // FP64 accumulators: one read of all this thread's TMEM words, one write back
+                uint32_t r[2 * ND];
+                tmem_span_ld<0, 2 * ND>(tacc, r);
+                tmem_span_wait<0, 2 * ND>(r);
+                const bool fold = uc_valid && tile_sss;
 #pragma unroll
-                    for (int q2 = 0; q2 < n; ++q2) {
-                        const int d = d0 + q2, i = d / NT, j = d % NT;
-                        double v = words_to_double(r[2 * q2], r[2 * q2 + 1]) + (double)c[i][j];
+                for (int i = 0; i < MT; ++i)
+#pragma unroll
+                    for (int j = 0; j < NT; ++j) {
+                        const int d = i * NT + j;
+                        double v = words_to_double(r[2 * d], r[2 * d + 1]) + (double)c[i][j];
                         if (fold) v -= uc_at(i, j);
-                        double_to_words(v, r[2 * q2], r[2 * q2 + 1]);
+                        double_to_words(v, r[2 * d], r[2 * d + 1]);
                     }
-                });
+                tmem_span_st<0, 2 * ND>(tacc, r);
+                tmem_wait_st();
             }
             uc_valid = false;
             if (cown) {  // c2[c'][a' + k b'] = sum_{c<k} (beta Tz)[c'][c] U2[c][a' + k b']
@@ -596,20 +612,23 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
         if (!bad) {
             double* dst = ch.slot < 0 ? TR.ocoef + (size_t)it.node * BS : partials + (size_t)ch.slot * BS;
             double n2 = 0.0, w2 = 0.0;
-            tmem_visit<ND, false>(tacc, [&](int d0, int n, auto& r) {
+            uint32_t r[2 * ND];
+            tmem_span_ld<0, 2 * ND>(tacc, r);
+            tmem_span_wait<0, 2 * ND>(r);
 #pragma unroll
-                for (int q2 = 0; q2 < n; ++q2) {
-                    const int d = d0 + q2, i = d / NT, j = d % NT;
-                    double v = words_to_double(r[2 * q2], r[2 * q2 + 1]);
-                    const int cz = o0 + i, nn = n0 + j, ax = nn % KP, by = nn / KP;
-                    if (uc_valid) v -= uc_at(i, j);
+            for (int i = 0; i < MT; ++i)
+#pragma unroll
+                for (int j = 0; j < NT; ++j) {
+                    const int d = i * NT + j;
+                    double v = words_to_double(r[2 * d], r[2 * d + 1]);
+                    const int cz = o0 + i, ax = tb0 + j, by = tc0;
+                    if (uc_valid && tile_sss) v -= uc_at(i, j);
                     if (cz < K2 && ax < K2 && by < K2) {
                         dst[ax + K2 * (by + K2 * cz)] = v;
                         n2 += v * v;
                         if (!(ax < K && by < K && cz < K)) w2 += v * v;
                     }
                 }
-            });
             // per-warp partial norms into the zero chunk (no longer read)
             for (int o = 16; o; o >>= 1) {
                 n2 += __shfl_down_sync(0xffffffffu, n2, o);
