@@ -55,30 +55,26 @@ struct HCfg {
     static constexpr int ND = MT * NT;
     static constexpr int LDT = NN + 4;  // row stride of T1 and T2 (split column layout)
     static constexpr int MATP = KP * KP;
-    // x step
+    // x step (image layouts in mw_slice.hpp, XGeo)
     static constexpr int R = K2 * K2;
     static constexpr int TILES = (R + 127) / 128;
-    static constexpr int NCH = (K2 + 7) / 8;
-    static constexpr int KSTEPS = (NCH + 1) / 2;
-    static constexpr bool PADCH = 2 * KSTEPS > NCH;  // the last K step reads one chunk past the slice
+    static constexpr int NCHM = K2 > 8 ? 2 : 1;  // chunks of x = 0 .. 15 per slice
+    static constexpr int PACK = K2 > 16 ? 1 : 0;  // the packed step over x = 16 .. K2-1
     static constexpr int W = K2;
     static constexpr int NCOL = (3 * W + 15) / 16 * 16;
     static constexpr int TSTR = (NCOL + 31) / 32 * 32;  // TMEM columns per lane tile
     static constexpr int NB = 2 * W + NCOL;
-    static constexpr int SLICE = NCH * R * 16;
-    static constexpr int IMGB = 3 * SLICE;
-    // s->s block of the x step (x', x < k; data rows y, z < k)
-    static constexpr int W2 = K;
+    static constexpr int IMGB = (3 * NCHM + 2 * PACK) * R * 16;
+    static constexpr int W2 = K;  // s->s block of the x step (x', x < k; data rows y, z < k)
     static constexpr int NCOL2 = (3 * W2 + 15) / 16 * 16;
     static constexpr int TSTR2 = (NCOL2 + 31) / 32 * 32;
     static constexpr int NB2 = 2 * W2 + NCOL2;
-    static constexpr int OPB_MAIN = 2 * KSTEPS * NB * 16;
-    static constexpr int OPB = OPB_MAIN + 2 * NB2 * 16;
+    static constexpr int OPB_A = NCHM * NB * 16;
+    static constexpr int OPB_B = PACK * 2 * NCOL * 16;
+    static constexpr int OPB = OPB_A + OPB_B + 2 * NB2 * 16;
     static constexpr int BUF = (IMGB + OPB + 127) / 128 * 128;
-    static constexpr int ZC = TILES * 128 * 16;  // zero chunk: the padding chunk of the last slice
     // generated (scaling-only) inputs, and the s->s block: rows y, z < k, x < k only
     static constexpr int TILES_GEN = (K + K2 * (K - 1) + 127) / 128;
-    static constexpr int KSTEPS_GEN = (K + 15) / 16;
     // TMEM: x sums [0, COLC), s->s x sums [COLC, ACC0), FP64 accumulators after (warps of one lane quarter
     // side by side)
     static constexpr int COLC = TILES * TSTR;
@@ -91,11 +87,11 @@ struct HCfg {
     static constexpr int NC = gcfg_nc(K, NTHR_S);
     static constexpr int NCT = KK / NC;
     static constexpr int MAXT = 128;  // triples per chunk whose records are kept in shared memory
-    static constexpr size_t SMEM = 2 * (size_t)BUF + ZC +
-                                   sizeof(float) * (2 * (size_t)KP * LDT + 2 * MATP + 3 * KKK) + MAXT * 24 + 128;
-    static constexpr bool FITS = (KP == 16 || KP == 20) && KSTEPS <= 2 && KSTEPS_GEN == 1 && NCOL <= 256 &&
-                                 TCOLS_NEED <= 512 && SMEM + 1024 <= 232448 && 2 * NCT <= NTHR_S &&
-                                 R < (1 << 14) && NB < (1 << 14) && K <= 16;
+    static constexpr size_t SMEM = 2 * (size_t)BUF + sizeof(float) * (2 * (size_t)KP * LDT + 2 * MATP + 3 * KKK) +
+                                   MAXT * 24 + 128;
+    // the last tile reads (TILES 128 - R) rows past the last chunk: they land in the operator image
+    static constexpr bool FITS = (KP == 16 || KP == 20) && K <= 10 && K2 > 8 && NCOL <= 256 && TCOLS_NEED <= 512 &&
+                                 SMEM + 1024 <= 232448 && 2 * NCT <= NTHR_S && (TILES * 128 - R) * 16 <= OPB;
 };
 
 // Block images of the tensor-core x step, one CTA per block: the FP64 block (or the generated k^3
@@ -105,7 +101,7 @@ template <int K>
 __global__ void __launch_bounds__(256) k_simage(const ImgSrc* __restrict__ srcs, int nsrc, const double* __restrict__ gblk,
                                                 long long nreal, unsigned char* __restrict__ img) {
     using C = HCfg<K>;
-    constexpr int K2 = C::K2, R = C::R, NCH = C::NCH, BS = K2 * K2 * K2, KKK = K * K * K;
+    constexpr int K2 = C::K2, R = C::R, NCHM = C::NCHM, BS = K2 * K2 * K2, KKK = K * K * K;
     extern __shared__ __align__(16) unsigned char smraw[];
     double* blk = reinterpret_cast<double*>(smraw);
     const long long slot = blockIdx.x;
@@ -128,25 +124,31 @@ __global__ void __launch_bounds__(256) k_simage(const ImgSrc* __restrict__ srcs,
     }
     __syncthreads();
     unsigned char* out = img + (size_t)slot * C::IMGB;
+    auto put = [&](int chunk, int r, const float* v) {
+        uint32_t w[4];
+#pragma unroll
+        for (int h = 0; h < 4; ++h)
+            w[h] = (uint32_t)bf16_bits_exact(v[2 * h]) | ((uint32_t)bf16_bits_exact(v[2 * h + 1]) << 16);
+        *reinterpret_cast<uint4*>(out + ((size_t)chunk * R + r) * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+    };
     for (int r = threadIdx.x; r < R; r += blockDim.x) {
-        float s[3][8 * NCH];
+        float s[3][16 + 8 * NCHM];
 #pragma unroll
         for (int q = 0; q < 3; ++q)
 #pragma unroll
-            for (int x = 0; x < 8 * NCH; ++x) s[q][x] = 0.0f;
+            for (int x = 0; x < 16 + 8 * NCHM; ++x) s[q][x] = 0.0f;
         slice3_row(blk + (size_t)K2 * r, K2, 1, s[0], s[1], s[2]);
 #pragma unroll
         for (int q = 0; q < 3; ++q)
 #pragma unroll
-            for (int c = 0; c < NCH; ++c) {
-                uint32_t w[4];
+            for (int c = 0; c < NCHM; ++c) put(q * NCHM + c, r, &s[q][8 * c]);
+        if constexpr (C::PACK) {  // [s0 | s1 | s2 | 0] of x = 16 .., four K slots per slice
+            float pk[16];
 #pragma unroll
-                for (int h = 0; h < 4; ++h)
-                    w[h] = (uint32_t)bf16_bits_exact(s[q][8 * c + 2 * h]) |
-                           ((uint32_t)bf16_bits_exact(s[q][8 * c + 2 * h + 1]) << 16);
-                *reinterpret_cast<uint4*>(out + (size_t)q * C::SLICE + ((size_t)c * R + r) * 16) =
-                    make_uint4(w[0], w[1], w[2], w[3]);
-            }
+            for (int e = 0; e < 16; ++e) pk[e] = (e < 12 && 16 + (e & 3) < K2) ? s[e >> 2][16 + (e & 3)] : 0.0f;
+            put(3 * NCHM, r, pk);
+            put(3 * NCHM + 1, r, pk + 8);
+        }
     }
 }
 
@@ -239,8 +241,7 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
     __shared__ uint32_t tmem_slot;
     __shared__ __align__(8) uint64_t bars[6];  // staged[2], mma_done[2], line_done, sums_free
     __shared__ int s_bad;
-    unsigned char* zc = smraw + 2 * (size_t)C::BUF;
-    float* T1 = reinterpret_cast<float*>(zc + C::ZC);  // [KP][LDT], split columns
+    float* T1 = reinterpret_cast<float*>(smraw + 2 * (size_t)C::BUF);  // [KP][LDT], split columns
     float* T2 = T1 + KP * LDT;
     float* My = T2 + KP * LDT;  // [KP][split o]: My[b'][b] at (b, o = b')
     float* Mz = My + MATP;
@@ -286,8 +287,6 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
         mbar_fence_init();
         s_bad = 0;
     }
-    for (int e = tid; e < C::ZC / 16; e += C::NTHR) *reinterpret_cast<uint4*>(zc + 16 * e) = make_uint4(0u, 0u, 0u, 0u);
-    fence_proxy_async_smem();
     tmem_fence_before_sync();
     __syncthreads();
     tmem_fence_after_sync();
@@ -299,7 +298,7 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
         if (lane == 0) {
             uint32_t fph = 0, mph = 0, dph = 0;
             bool spend[2] = {false, false}, mpend[2] = {false, false};
-            const uint32_t sbase = smem_addr_u32(smraw), zca = smem_addr_u32(zc);
+            const uint32_t sbase = smem_addr_u32(smraw);
             auto stage = [&](const HTri& h, int b) {
                 unsigned char* dst = smraw + (size_t)b * C::BUF;
                 mbar_arrive_expect_tx(&bars[b], (uint32_t)(C::IMGB + C::OPB));
@@ -316,33 +315,33 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
             auto issue = [&](int b, bool first, bool gen) {
                 const uint32_t base = sbase + (uint32_t)(b * C::BUF);
                 const uint64_t da = umma_sdesc(base, R * 16, 128);
-                const uint32_t apad = base + 2 * C::SLICE + 2 * (C::KSTEPS - 1) * R * 16;
-                const uint64_t dp = umma_sdesc(apad, zca - apad, 128);
                 const uint64_t db = umma_sdesc(base + C::IMGB, C::NB * 16, 128);
+                const uint64_t dq = umma_sdesc(base + C::IMGB + C::OPB_A, C::NCOL * 16, 128);
                 static_for<C::TILES>([&](auto TL) {
                     constexpr int tl = decltype(TL)::value;
                     const bool live = !gen || tl < C::TILES_GEN;
-                    static_for<C::KSTEPS>([&](auto KQ) {
-                        constexpr int kq = decltype(KQ)::value;
-                        static_for<3>([&](auto SQ) {
-                            constexpr int sq = decltype(SQ)::value;
-                            const bool init = first && kq == 0 && sq == 0;
-                            if (!(live && (!gen || kq < C::KSTEPS_GEN)) && !init) return;
-                            constexpr bool pad = C::PADCH && kq == C::KSTEPS - 1 && sq == 2;
-                            const uint64_t ad = pad ? dp + (uint64_t)(tl * 128)
-                                                    : da + (uint64_t)((sq * C::SLICE + 2 * kq * R * 16 + tl * 2048) >> 4);
-                            const uint64_t bd = db + (uint64_t)((2 * kq * C::NB * 16 + (2 - sq) * W * 16) >> 4);
-                            umma_bf16(tbase + (uint32_t)(tl * C::TSTR), ad, bd, idesc, init ? 0u : 1u);
-                        });
+                    static_for<3>([&](auto SQ) {  // x = 0 .. 15 of data slice sq against [m0|m1|m2] shifted
+                        constexpr int sq = decltype(SQ)::value;
+                        const bool init = first && sq == 0;
+                        if (!live && !init) return;
+                        const uint64_t ad = da + (uint64_t)((sq * C::NCHM * R * 16 + tl * 2048) >> 4);
+                        const uint64_t bd = db + (uint64_t)(((2 - sq) * W * 16) >> 4);
+                        umma_bf16(tbase + (uint32_t)(tl * C::TSTR), ad, bd, idesc, init ? 0u : 1u);
                     });
+                    if constexpr (C::PACK) {  // x = 16 .. K2-1 of all slices in one step
+                        if (!gen) {
+                            const uint64_t ad = da + (uint64_t)((3 * C::NCHM * R * 16 + tl * 2048) >> 4);
+                            umma_bf16(tbase + (uint32_t)(tl * C::TSTR), ad, dq, idesc, 1u);
+                        }
+                    }
                 });
                 if (!root) {
-                    const uint64_t dc = umma_sdesc(base + C::IMGB + C::OPB_MAIN, C::NB2 * 16, 128);
+                    const uint64_t dc = umma_sdesc(base + C::IMGB + C::OPB_A + C::OPB_B, C::NB2 * 16, 128);
                     static_for<C::TILES_GEN>([&](auto TL) {
                         constexpr int tl = decltype(TL)::value;
                         static_for<3>([&](auto SQ) {
                             constexpr int sq = decltype(SQ)::value;
-                            const uint64_t ad = da + (uint64_t)((sq * C::SLICE + tl * 2048) >> 4);
+                            const uint64_t ad = da + (uint64_t)((sq * C::NCHM * R * 16 + tl * 2048) >> 4);
                             const uint64_t bd = dc + (uint64_t)(((2 - sq) * W2 * 16) >> 4);
                             umma_bf16(tbase + (uint32_t)(C::COLC + tl * C::TSTR2), ad, bd, idesc2,
                                       (first && sq == 0) ? 0u : 1u);
@@ -407,7 +406,6 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
 #pragma unroll
             for (int q = 0; q < 2 * ND; ++q) z[q] = 0u;
             tmem_span_st<0, 2 * ND>(tacc, z);
-            tmem_wait_st();
         }
         auto load_mat = [&](float* dst, const float* tab, int mi) {
             constexpr int NV = MATP * 4 / 16;
@@ -433,6 +431,7 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
         const int nq = (C::NWARP - quarter + 3) / 4;  // warps of this lane quarter
         uint32_t lph = 0;
         bool pend2 = false, uc_valid = false, plane_gen = true, first_line = true;
+        float yacc[MT][NT];
         bool lgen = true;
         for (int t = ch.c0; t < ch.c1; ++t) {
             const HTri h0 = rec(t);
@@ -506,34 +505,31 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
                 uc_valid = true;
             }
             {
-                const bool zero = lgen && !(tc0 < K);
-                if (!zero || first_line) {
+                // this thread's y tile, summed over the plane's lines in registers (a tile of a generated
+                // line is zero when its z index c >= k)
+                if (first_line) {
+#pragma unroll
+                    for (int i = 0; i < MT; ++i)
+#pragma unroll
+                        for (int j = 0; j < NT; ++j) yacc[i][j] = 0.0f;
+                }
+                if (!(lgen && !(tc0 < K))) {
                     float c[MT][NT];
-                    if (zero) {
+                    if (lgen) gemm_tile_split<MT, NT, NTILE, KP, LDT, K>(My, T1, rt, ct, c);
+                    else gemm_tile_split<MT, NT, NTILE, KP, LDT, K2>(My, T1, rt, ct, c);
 #pragma unroll
-                        for (int i = 0; i < MT; ++i)
+                    for (int i = 0; i < MT; ++i)
 #pragma unroll
-                            for (int j = 0; j < NT; ++j) c[i][j] = 0.0f;
-                    } else if (lgen) {
-                        gemm_tile_split<MT, NT, NTILE, KP, LDT, K>(My, T1, rt, ct, c);
-                    } else {
-                        gemm_tile_split<MT, NT, NTILE, KP, LDT, K2>(My, T1, rt, ct, c);
-                    }
+                        for (int j = 0; j < NT; ++j) yacc[i][j] += c[i][j];
+                }
+                if (pend) {  // the plane's y sums -> T2[c][a' + P b'] for the z step
+                    float* row = T2 + tc0 * LDT;
 #pragma unroll
                     for (int i = 0; i < MT; ++i) {
                         const int m = tb0 + KP * (o0 + i);  // column a' + P b' of the tile's first value
-                        float* row = T2 + tc0 * LDT;
-                        float4* p4 = reinterpret_cast<float4*>(row + 4 * (m / NT));
-                        float4 v = first_line ? make_float4(0.f, 0.f, 0.f, 0.f) : *p4;
-                        v.x += c[i][0];
-                        v.y += c[i][1];
-                        v.z += c[i][2];
-                        v.w += c[i][3];
-                        *p4 = v;
-                        if constexpr (NT == 5) {
-                            float& s = row[4 * NTILE + m / NT];
-                            s = first_line ? c[i][4] : s + c[i][4];
-                        }
+                        *reinterpret_cast<float4*>(row + 4 * (m / NT)) =
+                            make_float4(yacc[i][0], yacc[i][1], yacc[i][2], yacc[i][3]);
+                        if constexpr (NT == 5) row[4 * NTILE + m / NT] = yacc[i][4];
                     }
                 }
             }
@@ -567,12 +563,14 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
             named_bar(1, NS);  // T2, U2 and Uc of the plane are complete
             // ---- z: acc[c'][a' + P b'] += sum_c (beta Mz)[c'][c] T2[c][a' + P b']  (- previous correction)
             {
+                // FP64 accumulators in TMEM: one read of all this thread's words, issued ahead of the GEMM
+                // (the previous plane's write back completes first), one write back
+                uint32_t r[2 * ND];
+                tmem_wait_st();
+                tmem_span_ld<0, 2 * ND>(tacc, r);
                 float c[MT][NT];
                 if (plane_gen) gemm_tile_split<MT, NT, NTILE, KP, LDT, K>(Mz, T2, rt, ct, c);
                 else gemm_tile_split<MT, NT, NTILE, KP, LDT, K2>(Mz, T2, rt, ct, c);
-                // FP64 accumulators: one read of all this thread's TMEM words, one write back
-                uint32_t r[2 * ND];
-                tmem_span_ld<0, 2 * ND>(tacc, r);
                 tmem_span_wait<0, 2 * ND>(r);
                 const bool fold = uc_valid && tile_sss;
 #pragma unroll
@@ -585,7 +583,6 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
                         double_to_words(v, r[2 * d], r[2 * d + 1]);
                     }
                 tmem_span_st<0, 2 * ND>(tacc, r);
-                tmem_wait_st();
             }
             uc_valid = false;
             if (cown) {  // c2[c'][a' + k b'] = sum_{c<k} (beta Tz)[c'][c] U2[c][a' + k b']
@@ -613,6 +610,7 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
             double* dst = ch.slot < 0 ? TR.ocoef + (size_t)it.node * BS : partials + (size_t)ch.slot * BS;
             double n2 = 0.0, w2 = 0.0;
             uint32_t r[2 * ND];
+            tmem_wait_st();
             tmem_span_ld<0, 2 * ND>(tacc, r);
             tmem_span_wait<0, 2 * ND>(r);
 #pragma unroll
@@ -629,14 +627,14 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
                         if (!(ax < K && by < K && cz < K)) w2 += v * v;
                     }
                 }
-            // per-warp partial norms into the zero chunk (no longer read)
+            // per-warp partial norms into T2 (no longer read)
             for (int o = 16; o; o >>= 1) {
                 n2 += __shfl_down_sync(0xffffffffu, n2, o);
                 w2 += __shfl_down_sync(0xffffffffu, w2, o);
             }
             if (lane == 0) {
-                reinterpret_cast<double*>(zc)[warp] = n2;
-                reinterpret_cast<double*>(zc)[32 + warp] = w2;
+                reinterpret_cast<double*>(T2)[warp] = n2;
+                reinterpret_cast<double*>(T2)[32 + warp] = w2;
             }
         }
     }
@@ -651,8 +649,8 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
     if (tid == 0) {
         double n2 = 0.0, w2 = 0.0;
         for (int w = 0; w < C::NWARP; ++w) {
-            n2 += reinterpret_cast<const double*>(zc)[w];
-            w2 += reinterpret_cast<const double*>(zc)[32 + w];
+            n2 += reinterpret_cast<const double*>(T2)[w];
+            w2 += reinterpret_cast<const double*>(T2)[32 + w];
         }
         if (ch.slot < 0) {
             TR.onorm2[it.node] = n2;

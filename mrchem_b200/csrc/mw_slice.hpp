@@ -53,23 +53,27 @@ MWB_HD inline uint16_t bf16_bits_exact(float x) {
     return (uint16_t)(u >> 16);
 }
 
-// Image geometry of the tensor-core x step for 2k = K2 (see k_happly):
-//   data block image: 3 slices, each NCH chunks of R rows x 16 bytes (row r = y + K2 z holds x = 8c ..
-//   8c + 7 of chunk c, BF16, zero for x >= K2);
-//   operator image: (a) the whole NS matrix, 2 KSTEPS chunks of NB rows x 16 bytes, rows [2W, 3W) /
-//   [3W, 4W) / [4W, 5W) = slices 0 / 1 / 2 of M[x'][.], all other rows zero; then (b) its top-left
-//   k x k block (the s->s part, x', x < k), 2 chunks of NB2 rows, rows [2W2, 3W2) / [3W2, 4W2) /
-//   [4W2, 5W2) = slices of M[x'][0 .. k) (W2 = k).
+// Image geometry of the tensor-core x step for 2k = K2 <= 20 (see k_happly).  A "chunk" is R rows x 16
+// bytes (8 BF16 values per row); row r = y + K2 z of the data.
+//   data block image: slices 0, 1, 2, each NCHM chunks holding x = 0 .. 8 NCHM - 1 (zero for x >= K2);
+//   then, when K2 > 16, two packed chunks holding per row [s0 | s1 | s2 | 0] of x = 16 .. K2 - 1
+//   (LO = K2 - 16 values per slice), so that one 16-deep MMA step covers the rest of x for all slices;
+//   operator image, one per NS matrix M[x'][x]: (a) NCHM chunks of NB rows: rows [2W, 3W) / [3W, 4W) /
+//   [4W, 5W) = slices 0 / 1 / 2 of M[x'][0 .. 8 NCHM), other rows zero; (b) when K2 > 16, two chunks
+//   of NCOL rows for the packed step: row n = b W + x' of column block b (b = 0, 1, 2) holds, at K
+//   offset 4 q (q = 0, 1, 2), slice b - q of M[x'][16 ..] when 0 <= b - q, else zero; (c) the top-left
+//   k x k block (x', x < k), 2 chunks of NB2 rows, rows [2W2, 3W2) / ... = slices of M[x'][0 .. k).
 struct XGeo {
-    int K2, R, TILES, NCH, KSTEPS, W, NCOL, NB, SLICE, IMGB, W2, NCOL2, NB2, OPB_MAIN, OPB;
+    int K2, R, TILES, NCHM, PACK, LO, W, NCOL, NB, IMGB, W2, NCOL2, NB2, OPB_A, OPB_B, OPB;
     MWB_HD explicit XGeo(int k2)
-        : K2(k2), R(k2 * k2), TILES((k2 * k2 + 127) / 128), NCH((k2 + 7) / 8), KSTEPS(((k2 + 7) / 8 + 1) / 2), W(k2),
-          NCOL((3 * k2 + 15) / 16 * 16), NB(2 * k2 + (3 * k2 + 15) / 16 * 16), SLICE(((k2 + 7) / 8) * k2 * k2 * 16),
-          IMGB(3 * ((k2 + 7) / 8) * k2 * k2 * 16), W2(k2 / 2), NCOL2((3 * (k2 / 2) + 15) / 16 * 16),
-          NB2(k2 + (3 * (k2 / 2) + 15) / 16 * 16),
-          OPB_MAIN(2 * (((k2 + 7) / 8 + 1) / 2) * (2 * k2 + (3 * k2 + 15) / 16 * 16) * 16),
-          OPB(2 * (((k2 + 7) / 8 + 1) / 2) * (2 * k2 + (3 * k2 + 15) / 16 * 16) * 16 +
-              2 * (k2 + (3 * (k2 / 2) + 15) / 16 * 16) * 16) {}
+        : K2(k2), R(k2 * k2), TILES((k2 * k2 + 127) / 128), NCHM(k2 > 8 ? 2 : 1), PACK(k2 > 16 ? 1 : 0),
+          LO(k2 > 16 ? k2 - 16 : 0), W(k2), NCOL((3 * k2 + 15) / 16 * 16), NB(2 * k2 + (3 * k2 + 15) / 16 * 16),
+          IMGB((3 * (k2 > 8 ? 2 : 1) + (k2 > 16 ? 2 : 0)) * k2 * k2 * 16), W2(k2 / 2),
+          NCOL2((3 * (k2 / 2) + 15) / 16 * 16), NB2(k2 + (3 * (k2 / 2) + 15) / 16 * 16),
+          OPB_A((k2 > 8 ? 2 : 1) * (2 * k2 + (3 * k2 + 15) / 16 * 16) * 16),
+          OPB_B(k2 > 16 ? 2 * ((3 * k2 + 15) / 16 * 16) * 16 : 0),
+          OPB((k2 > 8 ? 2 : 1) * (2 * k2 + (3 * k2 + 15) / 16 * 16) * 16 +
+              (k2 > 16 ? 2 * ((3 * k2 + 15) / 16 * 16) * 16 : 0) + 2 * (k2 + (3 * (k2 / 2) + 15) / 16 * 16) * 16) {}
 };
 
 // Split column layout of the CUDA-core GEMM tiles (tile width NT in {4, 5}): column n of a row is stored
