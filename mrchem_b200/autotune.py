@@ -4,7 +4,7 @@ The contraction kernels run one CTA per chunk of (input node, term) pairs of one
 that a chunk holds at most `chunk_triples` (output, input, term) triples.  Small chunks balance the
 load across the 148 SMs, but an output node cut into several chunks writes partial blocks that a
 reduction kernel adds afterwards.  Large chunks keep the node in one CTA.  The best value depends on
-the engine (FP64, FP32, split-TF32), the order and the tree shapes, so it is measured on the
+the engine (FP64, FP32, split-TF32, BF16x3), the order and the tree shapes, so it is measured on the
 caller's own workload: `tune_chunk_triples` times a representative call under each candidate and
 leaves the fastest set on the context.  Results agree to FP64 rounding for every value (only the
 grouping of the partial sums changes).
@@ -14,7 +14,7 @@ from __future__ import annotations
 import statistics
 import time
 
-DEFAULT_CANDIDATES = (16, 24, 32, 48, 64, 96, 128)
+DEFAULT_CANDIDATES = (16, 24, 32, 48, 64, 96, 128, 192, 256)
 
 
 def _wall_ms(run, sync):

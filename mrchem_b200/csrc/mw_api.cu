@@ -540,16 +540,27 @@ static const OpDepth& op_depth(Op& op, int depth, int dir = 0) {
                 }
         const XGeo xg(K2);
         std::vector<uint16_t> mX(nmat * (size_t)xg.OPB / 2, 0);
-        std::vector<float> sl0(K2), sl1(K2), sl2(K2);
+        std::vector<float> sl0(K2), sl1(K2), sl2(K2), t0(K2), t1(K2), t2(K2);
         for (size_t mi = 0; mi < nmat; ++mi) {
             uint16_t* img = mX.data() + mi * (size_t)xg.OPB / 2;
             for (int o = 0; o < K2; ++o) {
                 slice3_row(&od->mats[mi * K2 * K2 + (size_t)o * K2], K2, 1, sl0.data(), sl1.data(), sl2.data());
                 const float* sl[3] = {sl0.data(), sl1.data(), sl2.data()};
-                for (int q = 0; q < 3; ++q) {  // (a) x < 8 NCHM
-                    const int row = (2 + q) * xg.W + o;
-                    for (int k = 0; k < std::min(K2, 8 * xg.NCHM); ++k)
-                        img[((size_t)(k / 8) * xg.NB + row) * 8 + k % 8] = bf16_bits_exact(sl[q][k]);
+                if (o < xg.W2)  // the s->s block row M[o][0 .. k)
+                    slice3_row(&od->mats[mi * K2 * K2 + (size_t)o * K2], xg.W2, 1, t0.data(), t1.data(), t2.data());
+                const float* tl[3] = {t0.data(), t1.data(), t2.data()};
+                for (int q = 0; q < 3; ++q) {  // (a) the operand of data slice q
+                    uint16_t* op = img + (size_t)q * xg.OPB_Q / 2;
+                    for (int b = q; b < 3; ++b) {
+                        const int row = b * xg.W + o;
+                        for (int k = 0; k < std::min(K2, 8 * xg.NCHM); ++k)
+                            op[((size_t)(k / 8) * xg.NBQ + row) * 8 + k % 8] = bf16_bits_exact(sl[b - q][k]);
+                        if (o < xg.W2) {
+                            const int row2 = xg.NCOL + b * xg.W2 + o;
+                            for (int k = 0; k < xg.W2; ++k)
+                                op[((size_t)(k / 8) * xg.NBQ + row2) * 8 + k % 8] = bf16_bits_exact(tl[b - q][k]);
+                        }
+                    }
                 }
                 if (xg.PACK) {  // (b) the packed step over x = 16 .. K2-1
                     uint16_t* pk = img + (size_t)xg.OPB_A / 2;
@@ -559,14 +570,6 @@ static const OpDepth& op_depth(Op& op, int depth, int dir = 0) {
                                 const int kk = 4 * q + l, row = b * xg.W + o;
                                 pk[((size_t)(kk / 8) * xg.NCOL + row) * 8 + kk % 8] = bf16_bits_exact(sl[b - q][16 + l]);
                             }
-                }
-                if (o < xg.W2) {  // (c) the s->s block row M[o][0 .. k)
-                    slice3_row(&od->mats[mi * K2 * K2 + (size_t)o * K2], xg.W2, 1, sl0.data(), sl1.data(), sl2.data());
-                    uint16_t* cb = img + (size_t)(xg.OPB_A + xg.OPB_B) / 2;
-                    for (int q = 0; q < 3; ++q) {
-                        const int row = (2 + q) * xg.W2 + o;
-                        for (int k = 0; k < xg.W2; ++k) cb[((size_t)(k / 8) * xg.NB2 + row) * 8 + k % 8] = bf16_bits_exact(sl[q][k]);
-                    }
                 }
             }
         }

@@ -62,23 +62,23 @@ struct HCfg {
     static constexpr int PACK = K2 > 16 ? 1 : 0;  // the packed step over x = 16 .. K2-1
     static constexpr int W = K2;
     static constexpr int NCOL = (3 * W + 15) / 16 * 16;
-    static constexpr int TSTR = (NCOL + 31) / 32 * 32;  // TMEM columns per lane tile
-    static constexpr int NB = 2 * W + NCOL;
     static constexpr int IMGB = (3 * NCHM + 2 * PACK) * R * 16;
     static constexpr int W2 = K;  // s->s block of the x step (x', x < k; data rows y, z < k)
     static constexpr int NCOL2 = (3 * W2 + 15) / 16 * 16;
-    static constexpr int TSTR2 = (NCOL2 + 31) / 32 * 32;
-    static constexpr int NB2 = 2 * W2 + NCOL2;
-    static constexpr int OPB_A = NCHM * NB * 16;
+    static constexpr int NBQ = NCOL + NCOL2;  // rows of one data slice's operand: whole matrix, then s->s block
+    static constexpr int OPB_Q = NCHM * NBQ * 16;
+    static constexpr int OPB_A = 3 * OPB_Q;
     static constexpr int OPB_B = PACK * 2 * NCOL * 16;
-    static constexpr int OPB = OPB_A + OPB_B + 2 * NB2 * 16;
+    static constexpr int OPB = OPB_A + OPB_B;
     static constexpr int BUF = (IMGB + OPB + 127) / 128 * 128;
     // generated (scaling-only) inputs, and the s->s block: rows y, z < k, x < k only
     static constexpr int TILES_GEN = (K + K2 * (K - 1) + 127) / 128;
-    // TMEM: x sums [0, COLC), s->s x sums [COLC, ACC0), FP64 accumulators after (warps of one lane quarter
-    // side by side)
-    static constexpr int COLC = TILES * TSTR;
-    static constexpr int ACC0 = COLC + TILES_GEN * TSTR2;
+    // TMEM: lane tile t's x sums at columns tcol(t) (NCOL of them, then below the root NCOL2 s->s sums for
+    // the first TILES_GEN tiles), FP64 accumulators from ACC0 (warps of one lane quarter side by side)
+    static constexpr int TSTR_C = (NBQ + 31) / 32 * 32;   // tiles with s->s sums
+    static constexpr int TSTR = (NCOL + 31) / 32 * 32;    // the others
+    __host__ __device__ static constexpr int tcol(int t) { return t < TILES_GEN ? t * TSTR_C : TILES_GEN * TSTR_C + (t - TILES_GEN) * TSTR; }
+    static constexpr int ACC0 = TILES_GEN * TSTR_C + (TILES - TILES_GEN) * TSTR;
     static constexpr int NWQ = (NWARP + 3) / 4;
     static constexpr int TCOLS_NEED = ACC0 + NWQ * 2 * ND;
     static constexpr int TCOLS = TCOLS_NEED <= 128 ? 128 : TCOLS_NEED <= 256 ? 256 : 512;
@@ -86,7 +86,7 @@ struct HCfg {
     static constexpr int KK = K * K, KKK = K * K * K;
     static constexpr int NC = gcfg_nc(K, NTHR_S);
     static constexpr int NCT = KK / NC;
-    static constexpr int MAXT = 128;  // triples per chunk whose records are kept in shared memory
+    static constexpr int MAXT = 256;  // triples per chunk whose records are kept in shared memory
     static constexpr size_t SMEM = 2 * (size_t)BUF + sizeof(float) * (2 * (size_t)KP * LDT + 2 * MATP + 3 * KKK) +
                                    MAXT * 24 + 128;
     // the last tile reads (TILES 128 - R) rows past the last chunk: they land in the operator image
@@ -95,15 +95,16 @@ struct HCfg {
 };
 
 // Block images of the tensor-core x step, one CTA per block: the FP64 block (or the generated k^3
-// scaling block) is read coalesced, every data row (y, z) is sliced (mw_slice.hpp) and written as
-// 16-byte chunks of 8 x values.  Slot numbering as k_ximage.
+// scaling block) is read coalesced into shared memory (row stride K2 + 1 doubles: no bank conflicts
+// between the rows of a warp), every data row (y, z) is sliced (mw_slice.hpp) and written as 16-byte
+// chunks.  Slot numbering as k_ximage.
 template <int K>
-__global__ void __launch_bounds__(256) k_simage(const ImgSrc* __restrict__ srcs, int nsrc, const double* __restrict__ gblk,
+__global__ void __launch_bounds__(512) k_simage(const ImgSrc* __restrict__ srcs, int nsrc, const double* __restrict__ gblk,
                                                 long long nreal, unsigned char* __restrict__ img) {
     using C = HCfg<K>;
-    constexpr int K2 = C::K2, R = C::R, NCHM = C::NCHM, BS = K2 * K2 * K2, KKK = K * K * K;
+    constexpr int K2 = C::K2, R = C::R, NCHM = C::NCHM, BS = K2 * K2 * K2, KKK = K * K * K, LDR = K2 + 1;
     extern __shared__ __align__(16) unsigned char smraw[];
-    double* blk = reinterpret_cast<double*>(smraw);
+    double* blk = reinterpret_cast<double*>(smraw);  // [R][LDR]
     const long long slot = blockIdx.x;
     if (slot < nreal) {
         int lo = 0, hi = nsrc - 1;  // last entry with base <= slot
@@ -114,12 +115,12 @@ __global__ void __launch_bounds__(256) k_simage(const ImgSrc* __restrict__ srcs,
         }
         const ImgSrc sr = srcs[lo];
         const double* b = sr.coef + (size_t)(sr.lb + (slot - sr.base)) * BS;
-        for (int e = threadIdx.x; e < BS; e += blockDim.x) blk[e] = b[e];
+        for (int e = threadIdx.x; e < BS; e += blockDim.x) blk[(e / K2) * LDR + e % K2] = b[e];
     } else {
         const double* g = gblk + (size_t)(slot - nreal) * KKK;
         for (int e = threadIdx.x; e < BS; e += blockDim.x) {
             const int a = e % K2, bb = (e / K2) % K2, c = e / (K2 * K2);
-            blk[e] = (a < K && bb < K && c < K) ? g[a + K * (bb + K * c)] : 0.0;
+            blk[(e / K2) * LDR + a] = (a < K && bb < K && c < K) ? g[a + K * (bb + K * c)] : 0.0;
         }
     }
     __syncthreads();
@@ -132,12 +133,20 @@ __global__ void __launch_bounds__(256) k_simage(const ImgSrc* __restrict__ srcs,
         *reinterpret_cast<uint4*>(out + ((size_t)chunk * R + r) * 16) = make_uint4(w[0], w[1], w[2], w[3]);
     };
     for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        const double* row = blk + r * LDR;
+        double m = 0.0;
+#pragma unroll
+        for (int x = 0; x < K2; ++x) m = fmax(m, fabs(row[x]));
+        int e = 0;
+        if (m > 0.0) frexp(m, &e);
+        const double scale = ldexp(1.0, -e);
+        const float inv256 = ldexpf(1.0f, e - 8);
         float s[3][16 + 8 * NCHM];
 #pragma unroll
-        for (int q = 0; q < 3; ++q)
-#pragma unroll
-            for (int x = 0; x < 16 + 8 * NCHM; ++x) s[q][x] = 0.0f;
-        slice3_row(blk + (size_t)K2 * r, K2, 1, s[0], s[1], s[2]);
+        for (int x = 0; x < 16 + 8 * NCHM; ++x) {
+            if (x < K2) slice3_value(row[x], scale, inv256, s[0][x], s[1][x], s[2][x]);
+            else s[0][x] = s[1][x] = s[2][x] = 0.0f;
+        }
 #pragma unroll
         for (int q = 0; q < 3; ++q)
 #pragma unroll
@@ -145,7 +154,7 @@ __global__ void __launch_bounds__(256) k_simage(const ImgSrc* __restrict__ srcs,
         if constexpr (C::PACK) {  // [s0 | s1 | s2 | 0] of x = 16 .., four K slots per slice
             float pk[16];
 #pragma unroll
-            for (int e = 0; e < 16; ++e) pk[e] = (e < 12 && 16 + (e & 3) < K2) ? s[e >> 2][16 + (e & 3)] : 0.0f;
+            for (int e2 = 0; e2 < 16; ++e2) pk[e2] = (e2 < 12 && 16 + (e2 & 3) < K2) ? s[e2 >> 2][16 + (e2 & 3)] : 0.0f;
             put(3 * NCHM, r, pk);
             put(3 * NCHM + 1, r, pk + 8);
         }
@@ -311,43 +320,32 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
             // its first TILES_GEN tiles and first K step, but the first triple of a line clears every tile;
             // below the root also the s->s block's sums (x', x < k; first TILES_GEN tiles)
             constexpr uint32_t idesc = umma_idesc_bf16(128, C::NCOL);
-            constexpr uint32_t idesc2 = umma_idesc_bf16(128, C::NCOL2);
+            constexpr uint32_t idesc2 = umma_idesc_bf16(128, C::NBQ);
             auto issue = [&](int b, bool first, bool gen) {
                 const uint32_t base = sbase + (uint32_t)(b * C::BUF);
                 const uint64_t da = umma_sdesc(base, R * 16, 128);
-                const uint64_t db = umma_sdesc(base + C::IMGB, C::NB * 16, 128);
+                const uint64_t dbq = umma_sdesc(base + C::IMGB, C::NBQ * 16, 128);
                 const uint64_t dq = umma_sdesc(base + C::IMGB + C::OPB_A, C::NCOL * 16, 128);
                 static_for<C::TILES>([&](auto TL) {
                     constexpr int tl = decltype(TL)::value;
                     const bool live = !gen || tl < C::TILES_GEN;
-                    static_for<3>([&](auto SQ) {  // x = 0 .. 15 of data slice sq against [m0|m1|m2] shifted
+                    // below the root the first tiles also take the s->s block's sums (N = NCOL + NCOL2)
+                    const uint32_t id = (!root && tl < C::TILES_GEN) ? idesc2 : idesc;
+                    static_for<3>([&](auto SQ) {  // x = 0 .. 15 of data slice sq against its operand
                         constexpr int sq = decltype(SQ)::value;
                         const bool init = first && sq == 0;
                         if (!live && !init) return;
                         const uint64_t ad = da + (uint64_t)((sq * C::NCHM * R * 16 + tl * 2048) >> 4);
-                        const uint64_t bd = db + (uint64_t)(((2 - sq) * W * 16) >> 4);
-                        umma_bf16(tbase + (uint32_t)(tl * C::TSTR), ad, bd, idesc, init ? 0u : 1u);
+                        const uint64_t bd = dbq + (uint64_t)((sq * C::OPB_Q) >> 4);
+                        umma_bf16(tbase + (uint32_t)C::tcol(tl), ad, bd, id, init ? 0u : 1u);
                     });
-                    if constexpr (C::PACK) {  // x = 16 .. K2-1 of all slices in one step
+                    if constexpr (C::PACK) {  // x = 16 .. K2-1 of all slices in one step (whole matrix only)
                         if (!gen) {
                             const uint64_t ad = da + (uint64_t)((3 * C::NCHM * R * 16 + tl * 2048) >> 4);
-                            umma_bf16(tbase + (uint32_t)(tl * C::TSTR), ad, dq, idesc, 1u);
+                            umma_bf16(tbase + (uint32_t)C::tcol(tl), ad, dq, idesc, 1u);
                         }
                     }
                 });
-                if (!root) {
-                    const uint64_t dc = umma_sdesc(base + C::IMGB + C::OPB_A + C::OPB_B, C::NB2 * 16, 128);
-                    static_for<C::TILES_GEN>([&](auto TL) {
-                        constexpr int tl = decltype(TL)::value;
-                        static_for<3>([&](auto SQ) {
-                            constexpr int sq = decltype(SQ)::value;
-                            const uint64_t ad = da + (uint64_t)((sq * C::NCHM * R * 16 + tl * 2048) >> 4);
-                            const uint64_t bd = dc + (uint64_t)(((2 - sq) * W2 * 16) >> 4);
-                            umma_bf16(tbase + (uint32_t)(C::COLC + tl * C::TSTR2), ad, bd, idesc2,
-                                      (first && sq == 0) ? 0u : 1u);
-                        });
-                    });
-                }
             };
             if (ntri > 0) stage(rec(ch.c0), 0);
             if (ntri > 1) stage(rec(ch.c0 + 1), 1);
@@ -456,7 +454,7 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
 #pragma unroll 1
                 for (int tl = warp >> 2; tl < C::TILES; tl += nq) {
                     uint32_t v[3 * W];
-                    tmem_span_ld<0, 3 * W>(tlane + (uint32_t)(tl * C::TSTR), v);
+                    tmem_span_ld<0, 3 * W>(tlane + (uint32_t)C::tcol(tl), v);
                     tmem_span_wait<0, 3 * W>(v);
                     const int r = 128 * tl + 32 * quarter + lane;
                     if (r < R) {
@@ -480,7 +478,7 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
 #pragma unroll 1
                     for (int tl = warp >> 2; tl < C::TILES_GEN; tl += nq) {
                         uint32_t v[3 * W2];
-                        tmem_span_ld<0, 3 * W2>(tlane + (uint32_t)(C::COLC + tl * C::TSTR2), v);
+                        tmem_span_ld<0, 3 * W2>(tlane + (uint32_t)(C::tcol(tl) + C::NCOL), v);
                         tmem_span_wait<0, 3 * W2>(v);
                         const int r = 128 * tl + 32 * quarter + lane;
                         const int y = r % K2, z = r / K2;

@@ -42,6 +42,23 @@ MWB_HD inline void slice3_row(const double* v, int n, int stride, float* s0, flo
     }
 }
 
+// Same slices with the remainder after the first slice carried in FP32: r1 = u - s0 (|r1| <= 2^-9 |m|) is
+// exact in FP64 and rounded to FP32 once (relative 2^-24, i.e. 2^-33 of the row maximum, far below the
+// last slice's quantum 2^-24); the rest is exact in FP32.  Equal to slice3_row except for rows whose
+// remainders round at that level; used by the device image kernel (one FP64 multiply, rounding and
+// FMA per value).
+MWB_HD inline void slice3_value(double v, double scale, float inv256, float& s0, float& s1, float& s2) {
+    const double u = v * scale;  // |u| < 1, exact (power-of-two scale)
+    const double a = rint(u * 256.0);
+    const float r1 = (float)fma(a, -1.0 / 256.0, u);
+    const float b = rintf(r1 * 65536.0f);
+    const float r2 = fmaf(b, -1.0f / 65536.0f, r1);
+    const float c = rintf(r2 * 16777216.0f);
+    s0 = (float)a * inv256;
+    s1 = b * (inv256 * (1.0f / 256.0f));
+    s2 = c * (inv256 * (1.0f / 65536.0f));
+}
+
 // BF16 bits of a float with at most 8 significant bits (the low 16 bits of its pattern are zero)
 MWB_HD inline uint16_t bf16_bits_exact(float x) {
     uint32_t u;
@@ -58,22 +75,25 @@ MWB_HD inline uint16_t bf16_bits_exact(float x) {
 //   data block image: slices 0, 1, 2, each NCHM chunks holding x = 0 .. 8 NCHM - 1 (zero for x >= K2);
 //   then, when K2 > 16, two packed chunks holding per row [s0 | s1 | s2 | 0] of x = 16 .. K2 - 1
 //   (LO = K2 - 16 values per slice), so that one 16-deep MMA step covers the rest of x for all slices;
-//   operator image, one per NS matrix M[x'][x]: (a) NCHM chunks of NB rows: rows [2W, 3W) / [3W, 4W) /
-//   [4W, 5W) = slices 0 / 1 / 2 of M[x'][0 .. 8 NCHM), other rows zero; (b) when K2 > 16, two chunks
-//   of NCOL rows for the packed step: row n = b W + x' of column block b (b = 0, 1, 2) holds, at K
-//   offset 4 q (q = 0, 1, 2), slice b - q of M[x'][16 ..] when 0 <= b - q, else zero; (c) the top-left
-//   k x k block (x', x < k), 2 chunks of NB2 rows, rows [2W2, 3W2) / ... = slices of M[x'][0 .. k).
+//   operator image, one per NS matrix M[x'][x]: (a) for each data slice q = 0, 1, 2 an operand of
+//   NCH2 = NCOL + NCOL2 rows x NCHM chunks: row b W + x' (column block b = 0, 1, 2 of the whole matrix)
+//   holds slice b - q of M[x'][0 .. 8 NCHM) when b >= q, and row NCOL + b W2 + x' (x' < k) holds slice
+//   b - q of the s->s block row M[x'][0 .. k), zero elsewhere (slice pairs of equal weight land in equal
+//   output columns); (b) when K2 > 16, the packed step's operand, two chunks of NCOL rows: row b W + x'
+//   holds, at K offset 4 q (q = 0, 1, 2), slice b - q of M[x'][16 ..] when b >= q, else zero.
 struct XGeo {
-    int K2, R, TILES, NCHM, PACK, LO, W, NCOL, NB, IMGB, W2, NCOL2, NB2, OPB_A, OPB_B, OPB;
+    int K2, R, TILES, NCHM, PACK, LO, W, NCOL, W2, NCOL2, NBQ, IMGB, OPB_Q, OPB_A, OPB_B, OPB;
     MWB_HD explicit XGeo(int k2)
         : K2(k2), R(k2 * k2), TILES((k2 * k2 + 127) / 128), NCHM(k2 > 8 ? 2 : 1), PACK(k2 > 16 ? 1 : 0),
-          LO(k2 > 16 ? k2 - 16 : 0), W(k2), NCOL((3 * k2 + 15) / 16 * 16), NB(2 * k2 + (3 * k2 + 15) / 16 * 16),
-          IMGB((3 * (k2 > 8 ? 2 : 1) + (k2 > 16 ? 2 : 0)) * k2 * k2 * 16), W2(k2 / 2),
-          NCOL2((3 * (k2 / 2) + 15) / 16 * 16), NB2(k2 + (3 * (k2 / 2) + 15) / 16 * 16),
-          OPB_A((k2 > 8 ? 2 : 1) * (2 * k2 + (3 * k2 + 15) / 16 * 16) * 16),
+          LO(k2 > 16 ? k2 - 16 : 0), W(k2), NCOL((3 * k2 + 15) / 16 * 16), W2(k2 / 2),
+          NCOL2((3 * (k2 / 2) + 15) / 16 * 16),
+          NBQ((3 * k2 + 15) / 16 * 16 + (3 * (k2 / 2) + 15) / 16 * 16),
+          IMGB((3 * (k2 > 8 ? 2 : 1) + (k2 > 16 ? 2 : 0)) * k2 * k2 * 16),
+          OPB_Q((k2 > 8 ? 2 : 1) * ((3 * k2 + 15) / 16 * 16 + (3 * (k2 / 2) + 15) / 16 * 16) * 16),
+          OPB_A(3 * (k2 > 8 ? 2 : 1) * ((3 * k2 + 15) / 16 * 16 + (3 * (k2 / 2) + 15) / 16 * 16) * 16),
           OPB_B(k2 > 16 ? 2 * ((3 * k2 + 15) / 16 * 16) * 16 : 0),
-          OPB((k2 > 8 ? 2 : 1) * (2 * k2 + (3 * k2 + 15) / 16 * 16) * 16 +
-              (k2 > 16 ? 2 * ((3 * k2 + 15) / 16 * 16) * 16 : 0) + 2 * (k2 + (3 * (k2 / 2) + 15) / 16 * 16) * 16) {}
+          OPB(3 * (k2 > 8 ? 2 : 1) * ((3 * k2 + 15) / 16 * 16 + (3 * (k2 / 2) + 15) / 16 * 16) * 16 +
+              (k2 > 16 ? 2 * ((3 * k2 + 15) / 16 * 16) * 16 : 0)) {}
 };
 
 // Split column layout of the CUDA-core GEMM tiles (tile width NT in {4, 5}): column n of a row is stored

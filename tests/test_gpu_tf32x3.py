@@ -112,7 +112,7 @@ def test_tf32x3_unknown_flag_rejected(gpu_mod):
     inp = G.FunctionTree(m)
     G.project(1e-3, inp, two_gaussians(G))
     with pytest.raises(G.MWError):
-        G.apply(1e-3, G.FunctionTree(m), G.PoissonOperator(m, 1e-3), inp, 3)
+        G.apply(1e-3, G.FunctionTree(m), G.PoissonOperator(m, 1e-3), inp, 4)
 
 
 def test_tf32x3_fine_precision_takes_fp32_engine(gpu_mod):
