@@ -136,9 +136,10 @@ int mw_dot(mw_tree a, mw_tree b, double* out);
 int mw_tree_distance(mw_tree a, mw_tree b, double* out);
 
 /* Allocation-free inner product <a|b>.  No counterpart in the reference: it serves callers that
- * cannot allocate device memory when they need the result -- a thread recording a CUDA graph
- * (allocation is not capturable), code under a fixed, pre-reserved memory budget, or a host whose
- * device memory pool belongs to another framework.  Same result as mw_dot (which allocates two
+ * cannot allocate device memory when they need the result -- code under a fixed, pre-reserved memory
+ * budget, a host whose device memory pool belongs to another framework, or a thread that must leave
+ * the allocator alone while other work on its device is being recorded.  The call itself ends with a
+ * blocking read of the result, so it is not made inside a stream capture.  Same result as mw_dot (which allocates two
  * small scratch buffers per call), computed with a fixed scratch array compiled into the library:
  * 8 MiB per GPU that loads the library, held until process exit.
  *   - `a` may have at most 1048576 (2^20) nodes; larger trees return MW_ERR_CAPACITY.

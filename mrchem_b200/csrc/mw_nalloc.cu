@@ -1,11 +1,12 @@
 // mw_nalloc.cu -- inner product of two trees that allocates no device memory.
 //
-// Why it exists: some callers cannot allocate device memory at the moment they need a result -- a
-// host thread that is recording work into a CUDA graph (cudaMalloc is not capturable), code running
-// under a fixed memory budget that pre-reserves everything at start-up, or a caller that has handed
-// the whole device memory pool to another framework.  mw_dot() allocates two small scratch buffers
-// from the stream-ordered pool on every call; mw_nalloc_dot() computes the same sum with its scratch
-// in a fixed, file-scope device array instead.
+// Why it exists: some callers cannot allocate device memory at the moment they need a result -- code
+// running under a fixed memory budget that pre-reserves everything at start-up, a caller that has
+// handed the whole device memory pool to another framework, or a thread that must not touch the
+// allocator while other work is being recorded on its device.  mw_dot() allocates two small scratch
+// buffers from the stream-ordered pool on every call; mw_nalloc_dot() computes the same sum with its
+// scratch in a fixed, file-scope device array instead.  The call itself ends with a blocking read of
+// the result into host memory, so it is not a call to place inside a CUDA graph capture.
 //
 // The array g_nalloc_scratch holds kNallocMaxNodes per-node partial sums plus one slot for the
 // total (8 MiB + 256 B).  Every GPU that loads this library holds it until the process exits.  Its
@@ -15,6 +16,7 @@
 #include <string>
 
 #include "../../include/mwb200.h"
+#include "mw_device.cuh"
 #include "mw_internal.hpp"
 
 namespace mwb {
@@ -49,26 +51,6 @@ double* nalloc_scratch(int device) {
     return g_nalloc_ptr[device];
 }
 
-__device__ inline uint32_t na_hslot(uint64_t k, uint32_t mask) {
-    k ^= k >> 33;
-    k *= 0xff51afd7ed558ccdull;
-    k ^= k >> 33;
-    k *= 0xc4ceb9fe1a85ec53ull;
-    k ^= k >> 33;
-    return (uint32_t)k & mask;
-}
-__device__ inline int na_lookup(const uint64_t* hk, const int* hv, uint32_t cap, uint64_t key) {
-    const uint32_t mask = cap - 1;
-    uint32_t h = na_hslot(key, mask);
-    for (uint32_t i = 0; i < cap; ++i) {
-        const uint64_t s = hk[h];
-        if (s == key) return hv[h];
-        if (s == mwb::kEmptyKey) return -1;
-        h = (h + 1) & mask;
-    }
-    return -1;
-}
-
 // one warp per node of a: <a_node|b_node> over the wavelet part (all components at the root
 // depth); every partial in [0, na) is written, so no slot needs clearing between calls
 __global__ void k_nalloc_dot_nodes(const uint64_t* __restrict__ akey, const double* __restrict__ acoef, int na,
@@ -79,10 +61,10 @@ __global__ void k_nalloc_dot_nodes(const uint64_t* __restrict__ akey, const doub
     if (node >= na) return;
     const int K2 = 2 * k, BS = K2 * K2 * K2;
     const uint64_t key = akey[node];
-    const int j = na_lookup(hk, hv, hcap, key);
+    const int j = mwb::hlookup(hk, hv, hcap, key);  // the trees' own hash index (mw_device.cuh)
     double s = 0.0;
     if (j >= 0) {
-        const bool root = (key >> 59) == 0;
+        const bool root = mwb::key_depth(key) == 0;
         const double* x = acoef + (size_t)node * BS;
         const double* y = bcoef + (size_t)j * BS;
         for (int e = lane; e < BS; e += 32) {

@@ -1,8 +1,8 @@
 """The allocation-free inner product (mw_nalloc_dot) agrees with mw_dot.
 
 mw_nalloc_dot exists for callers that cannot allocate device memory when they need an inner
-product (for example while recording a CUDA graph, or under a pre-reserved memory budget); it keeps
-its scratch in a fixed array compiled into the library.  This file runs last (pytest collects files
+product (for example under a pre-reserved memory budget, or with the device pool owned by another
+framework); it keeps its scratch in a fixed array compiled into the library.  This file runs last (pytest collects files
 in name order) and also passes on its own in a fresh process.
 """
 import numpy as np
