@@ -166,6 +166,15 @@ int mw_apply_derivative(mw_tree out, mw_op op, mw_tree inp, int dir, int flags);
 int mw_op_destroy(mw_op op);
 int mw_op_nterms(mw_op op, int* n);
 int mw_op_terms(mw_op op, double* alpha, double* beta);
+/* The operator's 1-D matrices as the contraction uses them (for verification against independent
+ * quadrature; no reference counterpart, MRCPP keeps them internal to its OperatorCalculator):
+ * T^n(l) (k x k, row-major) of exp(-alpha x^2) between scaling functions at scale n, translation
+ * offset l -- entry (i, j) = 2^-n int_0^1 int_0^1 phi_i(u) phi_j(v) exp(-alpha 4^-n (u - v + l)^2);
+ * and the non-standard-form matrix (2k x 2k, rows = output scaling|wavelet, columns = input) of term
+ * `term` at scale n, offset l: F [[T(2l) T(2l-1)]; [T(2l+1) T(2l)]]_{n+1} F^T with the world's two-scale
+ * filter F (mw_mra_filter). */
+int mw_op_scaling_matrix(mw_op op, double alpha, int n, long long l, double* T);
+int mw_op_ns_matrix(mw_op op, int term, int n, long long l, double* NS);
 
 /* out = op * inp, adaptive.  Replaces mrcpp::apply(prec, out, op, inp): reference
  * src/scf_solver/HelmholtzVector.cpp:176,180, src/qmoperators/two_electron/CoulombPotential.cpp:85,

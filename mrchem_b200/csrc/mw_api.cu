@@ -1579,6 +1579,25 @@ int mw_op_terms(mw_op op, double* alpha, double* beta) {
     })
 }
 
+int mw_op_scaling_matrix(mw_op op, double alpha, int n, long long l, double* T) {
+    MW_TRY({
+        MW_ARG(op && T, "null pointer");
+        MW_ARG(op->kind == 0 && op->builder, "not a separated-Gaussian convolution operator");
+        MW_ARG(alpha > 0.0, "alpha must be positive");
+        op->builder->scaling(alpha, n, (long)l, T);
+    })
+}
+
+int mw_op_ns_matrix(mw_op op, int term, int n, long long l, double* NS) {
+    MW_TRY({
+        MW_ARG(op && NS, "null pointer");
+        MW_ARG(op->kind == 0 && op->builder, "not a separated-Gaussian convolution operator");
+        MW_ARG(term >= 0 && term < (int)op->terms.size(), "term index out of range");
+        std::vector<std::pair<long, std::vector<double>>> cache;
+        op->builder->ns(op->terms[term].alpha, n, (long)l, NS, cache);
+    })
+}
+
 int mw_apply(double prec, mw_tree out, mw_op op, mw_tree inp, int flags) {
     MW_TRY({
         MW_ARG(out && op && inp, "null pointer");

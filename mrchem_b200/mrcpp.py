@@ -58,6 +58,8 @@ SYMBOLS = [
     ("mw_mra_create", ctypes.c_int, [_vp, ctypes.c_int, _ip, _ip, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vpp]),
     ("mw_mra_destroy", ctypes.c_int, [_vp]),
     ("mw_mra_filter", ctypes.c_int, [_vp, _dp]),
+    ("mw_op_scaling_matrix", ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_longlong, _dp]),
+    ("mw_op_ns_matrix", ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_longlong, _dp]),
     ("mw_mra_max_depth", ctypes.c_int, [_vp, _ip]),
     ("mw_tree_create", ctypes.c_int, [_vp, _vpp]),
     ("mw_tree_destroy", ctypes.c_int, [_vp]),
@@ -400,6 +402,20 @@ class ConvolutionOperator:
         b = np.zeros(n.value)
         _check(_lib.mw_op_terms(self._h, _d(a), _d(b)))
         return a, b
+
+    def scaling_matrix(self, alpha, n, l):
+        """T^n(l) of exp(-alpha x^2), k x k (see mw_op_scaling_matrix)"""
+        k = self.mra.k
+        T = np.zeros((k, k))
+        _check(_lib.mw_op_scaling_matrix(self._h, float(alpha), int(n), int(l), _d(T)))
+        return T
+
+    def ns_matrix(self, term, n, l):
+        """non-standard-form matrix of a term at scale n, offset l, 2k x 2k (see mw_op_ns_matrix)"""
+        k = self.mra.k
+        NS = np.zeros((2 * k, 2 * k))
+        _check(_lib.mw_op_ns_matrix(self._h, int(term), int(n), int(l), _d(NS)))
+        return NS
 
 
 class PoissonOperator(ConvolutionOperator):

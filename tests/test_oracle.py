@@ -162,6 +162,50 @@ def test_coulomb_kat_reference_values_at_prec_1e3(oracle_mod):
         assert abs(val - ref) / ref < tol, (key, val, ref)
 
 
+def _hessian_setup(O, prec, order):
+    """Response Coulomb potential of tests/qmoperators/coulomb_hessian.cpp: V = P[rho_1] with
+    rho_1 = 4 (1s 2s + 2s 2p1) (density_utils.cpp:226-260, paired occupation 2, X = Y)."""
+    kat = json.load(open(os.path.join(HERE, "golden", "reference_kats.json")))
+    w = kat["world"]
+    m = O.MultiResolutionAnalysis(w["min_scale"], w["corner"], w["boxes"], order, w["max_depth"])
+    phi = [tuple(o) for o in kat["hessian"]["phi"]]
+    x = [tuple(o) for o in kat["hessian"]["x"]]
+    rho = O.FunctionTree(m)
+    O.project(prec, rho, O.hydrogen_params([(4.0, p, q) for p, q in zip(phi, x)]))
+    V = O.FunctionTree(m)
+    O.apply(prec / np.sqrt(rho.square_norm()), V, O.PoissonOperator(m, prec), rho)  # CoulombPotential.cpp:80-85
+    return kat, m, phi, V
+
+
+def test_coulomb_hessian_kat_converges_to_analytic(oracle_mod):
+    """tests/qmoperators/coulomb_hessian.cpp:95-98: the E_P quantities converge to the exact hydrogenic
+    integrals 4[1s1s|1s2s], 4[1s2s|1s2s], 4[2s2s|1s2s] (to 1e-4 at order 9, prec 1e-6)."""
+    O = oracle_mod
+    kat, m, phi, V = _hessian_setup(O, 1e-6, 9)
+    for key, expr in kat["analytic_hessian_E_P"].items():
+        i, j = map(int, key.split(","))
+        exact = eval(expr)  # closed forms from the fixture
+        val = _expect(O, m, V, phi[i], phi[j])
+        assert abs(val - exact) / exact < 1e-4, (key, val, exact)
+
+
+def test_coulomb_hessian_kat_reference_values(oracle_mod):
+    """The reference's E_P values (MRCPP at prec 1e-3) lie within 0.5 % of the converged oracle values
+    (they are that precision's approximation of the exact integrals: 0.28 % / 0.46 % / 0.47 % away);
+    at the reference's own setting (order 5, prec 1e-3) the oracle agrees with them to 8 %."""
+    O = oracle_mod
+    kat, m, phi, V = _hessian_setup(O, 1e-5, 7)
+    for key, ref in kat["coulomb_hessian_E_P"].items():
+        i, j = map(int, key.split(","))
+        val = _expect(O, m, V, phi[i], phi[j])
+        assert abs(val - ref) / ref < 5e-3, (key, val, ref)
+    kat, m, phi, V = _hessian_setup(O, 1e-3, 5)
+    for key, ref in kat["coulomb_hessian_E_P"].items():
+        i, j = map(int, key.split(","))
+        val = _expect(O, m, V, phi[i], phi[j])
+        assert abs(val - ref) / ref < 0.08, (key, val, ref)
+
+
 def test_projected_hydrogen_orbitals_are_normalised(oracle_mod):
     """tests/qmfunctions/orbital_vector.cpp:145: projected hydrogen orbitals have norm 1 (Approx)."""
     O = oracle_mod
