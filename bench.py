@@ -49,6 +49,9 @@ def parse():
     p.add_argument("--mixed-engine", default="bf16x3", choices=["bf16x3", "fp32"],
                    help="contraction of the mixed path: BF16x3 (x step on the tensor cores) or FP32 CUDA cores")
     p.add_argument("--tf32x3", action="store_true", help="also time the split-TF32 tensor-core engine")
+    p.add_argument("--shard", action="store_true",
+                   help="N > 1: split one batch over the ranks by input node count (strong scaling) "
+                        "instead of one batch per rank (weak scaling)")
     p.add_argument("--reserve-gib", type=int, default=64,
                    help="device memory pool reserved up front (GiB): the working set of the step")
     p.add_argument("--workload", default="helmholtz", choices=["helmholtz", "exchange", "density_sweep"],
@@ -220,7 +223,8 @@ def run_gpu(args):
     ctx.reserve(args.reserve_gib << 30)  # the whole working set, so that no timed step grows the pool
     m = G.MultiResolutionAnalysis(W.WORLD["min_scale"], W.WORLD["corner"], W.WORLD["boxes"], args.order, 15,
                                   ctx=ctx)
-    orbs, mus = workload(rank, args.orbitals)
+    shard = args.shard and world > 1
+    orbs, mus = workload(0 if shard else rank, args.orbitals)
     inps, ops, outs = [], [], []
     for i in range(args.orbitals):
         t = G.FunctionTree(m)
@@ -228,6 +232,16 @@ def run_gpu(args):
         inps.append(t)
         ops.append(G.HelmholtzOperator(m, mus[i], args.prec))
         outs.append(G.FunctionTree(m))
+    shard_range = (0, args.orbitals)
+    if shard:  # this rank's contiguous range of the one batch, balanced by input node count
+        from mrchem_b200.replicas import shard_ranges
+
+        shard_range = shard_ranges([t.nnodes() for t in inps], world)[rank]
+        b_, e_ = shard_range
+        inps, ops, outs, orbs, mus = inps[b_:e_], ops[b_:e_], outs[b_:e_], orbs[b_:e_], mus[b_:e_]
+    nloc = len(inps)
+    # applies of the whole job per step: the one batch (strong) or one batch per rank (weak)
+    job_applies = args.orbitals if shard else args.orbitals * world
     in_bytes = sum(t.nnodes() for t in inps) * (2 * m.k) ** 3 * 8
 
     def barrier():
@@ -276,7 +290,7 @@ def run_gpu(args):
     # learned tree proposal: trained (untimed) on plain applies of a disjoint seeded orbital set
     t_train = time.perf_counter()
     net = G.ProposalNet(ctx=ctx, hidden_layers=3, width=128, seed=5)
-    tr_orbs, tr_mus = workload(rank, args.orbitals, seed=1000 + 7)
+    tr_orbs, tr_mus = workload(0 if shard else rank, max(nloc, 1), seed=1000 + 7)
     tr_in = []
     for f in tr_orbs:
         t = G.FunctionTree(m)
@@ -302,7 +316,7 @@ def run_gpu(args):
     if args.tf32x3:
         engines.append(("tf32x3", G.APPLY_TF32X3))
     for name, fl in engines:
-        tune_out = [G.FunctionTree(m) for _ in range(args.orbitals)]
+        tune_out = [G.FunctionTree(m) for _ in range(nloc)]
 
         def tune_run(fl=fl, tune_out=tune_out):
             G.apply_batched(args.prec, tune_out, ops, inps, fl)
@@ -314,13 +328,13 @@ def run_gpu(args):
     # and z steps, FP64 accumulation; or the FP32 CUDA-core engine), and mixed + learned proposal, same
     # inputs, same operators
     ms64, trip64, prof64, _ = timed(lambda: G.apply_batched(args.prec, outs, ops, inps, G.APPLY_FP64), "plain_fp64")
-    outs32 = [G.FunctionTree(m) for _ in range(args.orbitals)]
+    outs32 = [G.FunctionTree(m) for _ in range(nloc)]
     ms32, trip32, prof32m, _ = timed(lambda: G.apply_batched(args.prec, outs32, ops, inps, MIXED), "mixed")
-    outsS = [G.FunctionTree(m) for _ in range(args.orbitals)]
+    outsS = [G.FunctionTree(m) for _ in range(nloc)]
     other = G.APPLY_FP32 if MIXED == G.APPLY_BF16X3 else G.APPLY_BF16X3
     msS, tripS, profS, _ = timed(lambda: G.apply_batched(args.prec, outsS, ops, inps, other), "mixed_other_engine")
     errS = [G.distance(a, b) / np.sqrt(b.square_norm()) for a, b in zip(outsS, outs)]
-    outsL = [G.FunctionTree(m) for _ in range(args.orbitals)]
+    outsL = [G.FunctionTree(m) for _ in range(nloc)]
     lstats = {}
 
     def run_learned():
@@ -331,7 +345,7 @@ def run_gpu(args):
     ms, triples, prof32, clocks = timed(run_learned, "mixed_learned")
     launches, apply_launches, apply_ms, apply_ctas = prof32
     if args.tf32x3:  # the split-TF32 tensor-core contraction on the same batch, no learned proposal
-        outsT = [G.FunctionTree(m) for _ in range(args.orbitals)]
+        outsT = [G.FunctionTree(m) for _ in range(nloc)]
         msT, tripT, profT, _ = timed(lambda: G.apply_batched(args.prec, outsT, ops, inps, G.APPLY_TF32X3), "tensor_core")
         errT = [G.distance(a, b) / np.sqrt(b.square_norm()) for a, b in zip(outsT, outs)]
     # error of the mixed + learned result against the FP64 one: ||g - g64|| / ||g64|| per orbital
@@ -342,7 +356,7 @@ def run_gpu(args):
         rel_err = max(rel_err, G.distance(a, b) / np.sqrt(b.square_norm()))
         same_tree &= a.nnodes() == b.nnodes()
     rel_err_mixed = max(G.distance(a, b) / np.sqrt(b.square_norm()) for a, b in zip(outs32, outs))
-    total_applies = args.orbitals * args.steps * world
+    total_applies = job_applies * args.steps
     value = total_applies / (ms / 1e3)
 
     # end to end through the public API from host buffers: every step uploads the input trees from
@@ -370,7 +384,7 @@ def run_gpu(args):
     n_e2e = min(16, max(8, args.steps))  # a stream of batches: pipeline fill and drain amortised over 8+ steps
     h2d = sum(sum(v.nbytes for v in h.values()) for h in host)
     node_bytes = 4 + 24 + 4 + 4 + 8 * bs_k
-    nb = args.orbitals
+    nb = nloc
 
     # Pipeline of three host threads (the library releases the interpreter lock in every call):
     #   upload:   pinned host -> staging input trees of a side context (stream), double-buffered;
@@ -495,7 +509,7 @@ def run_gpu(args):
         e2e_same &= nn == outsL[i].nnodes() and np.array_equal(out_bufs[i]["depth"][:nn], ex["depth"]) and \
             np.array_equal(out_bufs[i]["coef"][:nn * bs_k], ex["coef"].ravel())
     e2e_s = max_over_ranks(e2e_s, device=f"cuda:{local}")
-    e2e_val = args.orbitals * n_e2e * world / e2e_s
+    e2e_val = job_applies * n_e2e / e2e_s
 
     peaks = measured_peaks()
     k = m.k
@@ -532,14 +546,17 @@ def run_gpu(args):
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "applies/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "strong" if shard else "weak",
             "vs_baseline": None, "data": "synthetic",
             "dtype": ("bf16x3 fixed-point slices (x step, tensor cores) / f32 (y, z steps), f64 accumulation"
                       if MIXED == G.APPLY_BF16X3 else "f32 products, f64 accumulation"),
             "config": {"workload": "helmholtz_batch_32orb_k10_prec1e-6", "orbitals": args.orbitals,
                        "order": args.order, "k": k, "prec": args.prec, "mu": "U[0.5,3]", "world": "[-20,20]^3",
                        "path": f"mixed ({args.mixed_engine} contraction, FP64 accumulation) + learned tree proposal; batched",
-                       "parallelism": f"replicas x{world}",
+                       "parallelism": (f"one batch sharded over {world} ranks by input node count "
+                                       f"(this rank: trees {shard_range[0]}..{shard_range[1] - 1})") if shard
+                       else f"replicas x{world}",
                        "l2": f"inputs larger than L2 ({in_bytes / 1e9:.2f} GB of input blocks per step)"},
             "e2e": {"value": e2e_val, "unit": "applies/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "host_memory": "pinned, allocated once",
@@ -549,14 +566,14 @@ def run_gpu(args):
                             "so a step's transfers overlap the previous and next steps' compute",
                     "steps": n_e2e,
                     "outputs_equal_headline": bool(e2e_same)},
-            "plain_fp64": {"value": args.orbitals * args.steps * world / (ms64 / 1e3), "unit": "applies/s",
+            "plain_fp64": {"value": job_applies * args.steps / (ms64 / 1e3), "unit": "applies/s",
                            "ms_per_step": ms64 / args.steps, "kernel_ms_per_step": prof64[2] / args.steps,
                            "triples_per_step": trip64 // max(1, args.steps)},
             "mixed_no_learning": {"engine": args.mixed_engine,
-                                  "value": args.orbitals * args.steps * world / (ms32 / 1e3), "unit": "applies/s",
+                                  "value": job_applies * args.steps / (ms32 / 1e3), "unit": "applies/s",
                                   "ms_per_step": ms32 / args.steps, "kernel_ms_per_step": prof32m[2] / args.steps},
             "mixed_other_engine": {"engine": "fp32" if MIXED == G.APPLY_BF16X3 else "bf16x3",
-                                   "value": args.orbitals * args.steps * world / (msS / 1e3), "unit": "applies/s",
+                                   "value": job_applies * args.steps / (msS / 1e3), "unit": "applies/s",
                                    "ms_per_step": msS / args.steps, "kernel_ms_per_step": profS[2] / args.steps,
                                    "rel_error_vs_fp64_max": max(errS),
                                    "same_node_count_as_fp64": all(a.nnodes() == b.nnodes() for a, b in zip(outsS, outs))},
@@ -589,7 +606,7 @@ def run_gpu(args):
         }
         if args.tf32x3:
             line["tensor_core_tf32x3"] = {
-                "value": args.orbitals * args.steps * world / (msT / 1e3), "unit": "applies/s",
+                "value": job_applies * args.steps / (msT / 1e3), "unit": "applies/s",
                 "ms_per_step": msT / args.steps, "kernel": f"k_tapply<{m.k}>", "kernel_ms_per_step": profT[2] / args.steps,
                 "rel_error_vs_fp64_max": max(errT), "rel_error_vs_fp64_median": float(np.median(errT)),
                 "same_node_count_as_fp64": all(a.nnodes() == b.nnodes() for a, b in zip(outsT, outs))}

@@ -50,6 +50,45 @@ def max_over_ranks(value, device=None):
     return float(t.item())
 
 
+def apply_batched_sharded(prec, outs, ops, inps, flags=0, apply=None, group=None):
+    """One batch split over the ranks of the process group (strong scaling): rank r applies the
+    contiguous range shard_ranges(input node counts)[r] of the batch -- the orbitals it owns, as in the
+    reference's per-rank loop (src/scf_solver/HelmholtzVector.cpp:77, ownership from
+    src/parallel.cpp:118-120) -- and the per-tree results are then gathered for every rank.
+
+    `outs`, `ops`, `inps`: the whole batch (every rank holds the input trees; only its own range is
+    computed).  `apply(prec, outs, ops, inps, flags)` applies a list of trees; the default is
+    mrchem_b200.mrcpp.apply_batched.  Returns (ranges, results) with results[i] = (square norm,
+    node count) of output tree i, identical on every rank.  Without a process group this is one
+    apply of the whole batch.  The only collective is the all-gather of those results: the apply
+    itself exchanges nothing."""
+    if apply is None:
+        from mrchem_b200 import mrcpp as G
+
+        apply = G.apply_batched
+    import torch.distributed as dist
+
+    dist_on = dist.is_available() and dist.is_initialized()
+    world = dist.get_world_size(group) if dist_on else 1
+    rank = dist.get_rank(group) if dist_on else 0
+    n = len(inps)
+    if not (len(outs) == len(ops) == n):
+        raise ValueError("outs, ops and inps must have the same length")
+    ranges = shard_ranges([t.nnodes() for t in inps], world)
+    b, e = ranges[rank]
+    if e > b:
+        apply(prec, outs[b:e], ops[b:e], inps[b:e], flags)
+    local = [(float(outs[i].square_norm()), int(outs[i].nnodes())) for i in range(b, e)]
+    if world == 1:
+        return ranges, local
+    parts = [None] * world
+    dist.all_gather_object(parts, local, group=group)
+    results = [x for part in parts for x in part]
+    if len(results) != n:
+        raise RuntimeError("sharded batch: gathered results do not cover the batch")
+    return ranges, results
+
+
 def rank_seed(base, rank):
     """Seed of a rank's own batch in the weak-scaling runs: every rank applies a different batch."""
     return base + 1000 * rank
