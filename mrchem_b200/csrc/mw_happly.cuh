@@ -42,6 +42,13 @@
 
 namespace mwb {
 
+// columns per correction tile: the smallest divisor d of k^2 with 2 k^2 / d tiles fitting `nthr` threads
+__host__ __device__ constexpr int hc_nc(int k, int nthr) {
+    int d = 1;
+    while (d < k * k && ((k * k) % d != 0 || 2 * k * k / d > nthr)) ++d;
+    return d;
+}
+
 template <int K>
 struct HCfg {
     static constexpr int K2 = 2 * K;
@@ -84,14 +91,17 @@ struct HCfg {
     static constexpr int TCOLS = TCOLS_NEED <= 128 ? 128 : TCOLS_NEED <= 256 ? 256 : 512;
     // s->s correction of the y and z steps
     static constexpr int KK = K * K, KKK = K * K * K;
-    static constexpr int NC = gcfg_nc(K, NTHR_S);
+    // correction tiles (MT rows x NC columns) on the warps of lane quarters 2 and 3 only (warps 2, 3, 6, 7):
+    // quarters 0 and 1 hold one more GEMM warp each when NWARP = 10
+    static constexpr int NCW = 128;  // threads that take correction tiles
+    static constexpr int NC = hc_nc(K, NCW);
     static constexpr int NCT = KK / NC;
     static constexpr int MAXT = 256;  // triples per chunk whose records are kept in shared memory
     static constexpr size_t SMEM = 2 * (size_t)BUF + sizeof(float) * (2 * (size_t)KP * LDT + 2 * MATP + 3 * KKK) +
                                    MAXT * 24 + 128;
     // the last tile reads (TILES 128 - R) rows past the last chunk: they land in the operator image
     static constexpr bool FITS = (KP == 16 || KP == 20) && K <= 10 && K2 > 8 && NCOL <= 256 && TCOLS_NEED <= 512 &&
-                                 SMEM + 1024 <= 232448 && 2 * NCT <= NTHR_S && (TILES * 128 - R) * 16 <= OPB;
+                                 SMEM + 1024 <= 232448 && 2 * NCT <= NCW && NWARP >= 8 && (TILES * 128 - R) * 16 <= OPB;
 };
 
 // Block images of the tensor-core x step, one CTA per block: the FP64 block (or the generated k^3
@@ -393,8 +403,11 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
         const int rt = lane & 3, ct = warp * 8 + (lane >> 2);
         const int o0 = rt * MT, n0 = ct * NT;
         const int tb0 = n0 % KP, tc0 = n0 / KP;  // y tile: first a', c;  z tile: first a', b'
-        const int crt = tid & 1, cct = tid >> 1;
-        const bool cown = !root && cct < C::NCT;
+        // correction tiles: warps of lane quarters 2 and 3 (warps 2, 3, 6, 7)
+        const bool cwarp = (warp & 3) >= 2 && warp < 8;
+        const int cid = (((warp >> 2) << 1) | (warp & 1)) * 32 + lane;
+        const int crt = cid & 1, cct = cid >> 1;
+        const bool cown = !root && cwarp && cct < C::NCT;
         const int co0 = crt * MT, cn0 = cown ? cct * NC : 0;
         auto opos = [](int o) { return split_pos(o, MT, 4); };  // operator column of output index o
         const uint32_t tlane = tbase + ((uint32_t)(32 * quarter) << 16);
@@ -451,32 +464,37 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
             tmem_fence_after_sync();
             // ---- epilogue: the line's x sums (three column blocks) -> T1 [y][x' + P z], s->s sums -> U1
             if (!bad) {
+                // units of this lane quarter: the main x sums of every tile with rows here, then (below the
+                // root) the s->s sums of the first tiles; round-robin over the quarter's warps
+                constexpr int NU_MAX = C::TILES + C::TILES_GEN;
+                const int ntl = min(C::TILES, (R - 32 * quarter + 127) / 128);  // tiles with rows in this quarter
+                const int nunits = ntl + (root ? 0 : C::TILES_GEN);
 #pragma unroll 1
-                for (int tl = warp >> 2; tl < C::TILES; tl += nq) {
-                    uint32_t v[3 * W];
-                    tmem_span_ld<0, 3 * W>(tlane + (uint32_t)C::tcol(tl), v);
-                    tmem_span_wait<0, 3 * W>(v);
-                    const int r = 128 * tl + 32 * quarter + lane;
-                    if (r < R) {
-                        const int y = r % K2, z = r / K2;
-                        float o[KP];
+                for (int u = warp >> 2; u < nunits && u < NU_MAX; u += nq) {
+                    if (u < ntl) {
+                        const int tl = u;
+                        uint32_t v[3 * W];
+                        tmem_span_ld<0, 3 * W>(tlane + (uint32_t)C::tcol(tl), v);
+                        tmem_span_wait<0, 3 * W>(v);
+                        const int r = 128 * tl + 32 * quarter + lane;
+                        if (r < R) {
+                            const int y = r % K2, z = r / K2;
+                            float o[KP];
 #pragma unroll
-                        for (int x = 0; x < KP; ++x)
-                            o[x] = x < W ? __uint_as_float(v[x]) + (__uint_as_float(v[W + x]) + __uint_as_float(v[2 * W + x]))
-                                         : 0.0f;
-                        float* row = T1 + y * LDT;
-                        constexpr int TPR = KP / NT;  // column tiles per z
+                            for (int x = 0; x < KP; ++x)
+                                o[x] = x < W ? __uint_as_float(v[x]) + (__uint_as_float(v[W + x]) + __uint_as_float(v[2 * W + x]))
+                                             : 0.0f;
+                            float* row = T1 + y * LDT;
+                            constexpr int TPR = KP / NT;  // column tiles per z
 #pragma unroll
-                        for (int u = 0; u < TPR; ++u)
-                            *reinterpret_cast<float4*>(row + 4 * (TPR * z + u)) =
-                                make_float4(o[NT * u], o[NT * u + 1], o[NT * u + 2], o[NT * u + 3]);
-                        if constexpr (NT == 5)
-                            *reinterpret_cast<float4*>(row + 4 * NTILE + TPR * z) = make_float4(o[4], o[9], o[14], o[19]);
-                    }
-                }
-                if (!root) {
-#pragma unroll 1
-                    for (int tl = warp >> 2; tl < C::TILES_GEN; tl += nq) {
+                            for (int uu = 0; uu < TPR; ++uu)
+                                *reinterpret_cast<float4*>(row + 4 * (TPR * z + uu)) =
+                                    make_float4(o[NT * uu], o[NT * uu + 1], o[NT * uu + 2], o[NT * uu + 3]);
+                            if constexpr (NT == 5)
+                                *reinterpret_cast<float4*>(row + 4 * NTILE + TPR * z) = make_float4(o[4], o[9], o[14], o[19]);
+                        }
+                    } else {
+                        const int tl = u - ntl;
                         uint32_t v[3 * W2];
                         tmem_span_ld<0, 3 * W2>(tlane + (uint32_t)(C::tcol(tl) + C::NCOL), v);
                         tmem_span_wait<0, 3 * W2>(v);
