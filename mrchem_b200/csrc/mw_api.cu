@@ -570,6 +570,10 @@ static const OpDepth& op_depth(Op& op, int depth, int dir = 0) {
                                 const int kk = 4 * q + l, row = b * xg.W + o;
                                 pk[((size_t)(kk / 8) * xg.NCOL + row) * 8 + kk % 8] = bf16_bits_exact(sl[b - q][16 + l]);
                             }
+                    for (int l = 0; l < xg.LO; ++l) {  // data slice 3 against operator slice 0, into block 2
+                        const int kk = 12 + l, row = 2 * xg.W + o;
+                        pk[((size_t)(kk / 8) * xg.NCOL + row) * 8 + kk % 8] = bf16_bits_exact(sl[0][16 + l]);
+                    }
                 }
             }
         }

@@ -1308,10 +1308,11 @@ __global__ void __launch_bounds__(256) k_breduce(const Chunk* __restrict__ chunk
                                                  const BTree* __restrict__ trees, const double* __restrict__ partials) {
     using G = Geo<K>;
     __shared__ double red[64];
-    const int w = multi_items[blockIdx.x];
+    const int w = multi_items ? multi_items[blockIdx.x] : blockIdx.x;  // no list: one block per item
+    const int cb = choff[w], ce = choff[w + 1];
+    if (ce - cb < 2) return;  // a single chunk wrote the node itself
     const Item it = items[w];
     const BTree& TR = trees[it.tree];
-    const int cb = choff[w], ce = choff[w + 1];
     double n2 = 0.0, w2 = 0.0;
     for (int e = threadIdx.x; e < G::BS; e += blockDim.x) {
         double v = 0.0;
@@ -1327,16 +1328,6 @@ __global__ void __launch_bounds__(256) k_breduce(const Chunk* __restrict__ chunk
         TR.ownorm2[it.node] = w2;
     }
 }
-__global__ void k_multi_flags(const int* __restrict__ choff, int nitems, int* flags) {
-    const int w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= nitems) return;
-    flags[w] = (choff[w + 1] - choff[w] > 1) ? 1 : 0;
-}
-__global__ void k_list_from_flags(const int* __restrict__ flags, const int* __restrict__ pos, int n, int* list) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    if (flags[i]) list[pos[i]] = i;
-}
 
 // ---------------------------------------------------------------------------------------------
 // 6. per-tree root norms, split flags
@@ -1350,6 +1341,14 @@ __global__ void k_tree_item_norm2(const Item* __restrict__ items, const int* __r
     block_sum2(s, d, red);
     if (threadIdx.x == 0) out[t] = s;
 }
+// split thresholds of the root entries from their output norms: prec g0 with g0 the square root of the
+// root level's square norm (the same operations as the host's prec g0 2^(-depth/2) at depth 0)
+__global__ void k_root_thr(BTree* trees, const double* __restrict__ g, const double* __restrict__ prec, int nt) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt || trees[t].depth != 0) return;
+    const double g0 = sqrt(g[t]);
+    trees[t].thr = (prec[t] > 0.0 && g0 > 0.0) ? prec[t] * g0 : INFINITY;
+}
 __global__ void k_bsplit_flags(const Item* __restrict__ items, int nitems, const BTree* __restrict__ trees,
                                int* flags) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1357,16 +1356,6 @@ __global__ void k_bsplit_flags(const Item* __restrict__ items, int nitems, const
     const Item it = items[i];
     const BTree& T = trees[it.tree];
     flags[i] = (T.depth < T.depth_limit && sqrt(T.ownorm2[it.node]) > T.thr) ? 1 : 0;
-}
-__global__ void k_bsplit_list(const int* __restrict__ flags, const int* __restrict__ pos, const Item* __restrict__ items,
-                              int n, int* list) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    if (flags[i]) list[pos[i]] = items[i].node;
-}
-__global__ void k_gather_int(const int* __restrict__ src, const int* __restrict__ idx, int n, int* dst) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) dst[i] = src[idx[i]];
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1390,6 +1379,14 @@ static T* upload(Ctx* ctx, const std::vector<T>& v) {
     T* d = (T*)dalloc(ctx, sizeof(T) * std::max<size_t>(1, v.size()));
     if (!v.empty()) MWB_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, ctx->stream));
     return d;
+}
+// exclusive sum of d_in[0 .. n] into d_out (the total lands in d_out[n]); no host read-back
+static void scan_only(Ctx* ctx, const int* d_in, int* d_out, int n) {
+    size_t tmp = 0;
+    MWB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, d_in, d_out, n + 1, ctx->stream));
+    void* d_tmp = dalloc(ctx, tmp);
+    MWB_CUDA(cub::DeviceScan::ExclusiveSum(d_tmp, tmp, d_in, d_out, n + 1, ctx->stream));
+    dfree(ctx, d_tmp);
 }
 static int scan_total(Ctx* ctx, const int* d_in, int* d_out, int n) {
     size_t tmp = 0;
@@ -1488,7 +1485,9 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         d.nprefix = b.nprefix;
         d.root = b.depth == 0;
         d.theta = b.theta;
-        d.thr = 0.0;
+        // split threshold: deeper entries from the root pass's norm; root entries get theirs on the device
+        d.thr = b.depth == 0 ? 0.0
+                             : ((b.prec > 0.0 && b.g0 > 0.0) ? b.prec * b.g0 * std::pow(2.0, -0.5 * b.depth) : INFINITY);
         d.depth = b.depth;
         d.depth_limit = m.depth_limit;
         for (int q = 0; q < 3; ++q) d.ext[q] = (long long)m.boxes[q] << b.depth;
@@ -1645,15 +1644,19 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
                                                    nullptr, nullptr);
         k_multi_slots<<<(ni + 127) / 128, 128, 0, s>>>(d_nchunk, ni, d_nslot);
         count(ctx, 2);
-        nchunks = scan_total(ctx, d_nchunk, d_choff, ni);
-        nslots = scan_total(ctx, d_nslot, d_slotoff, ni);
+        scan_only(ctx, d_nchunk, d_choff, ni);
+        scan_only(ctx, d_nslot, d_slotoff, ni);
+        int tot[3] = {0, 0, 0};  // chunks, partial slots, the expansion's error word: one read-back
+        MWB_CUDA(cudaMemcpyAsync(&tot[0], d_choff + ni, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MWB_CUDA(cudaMemcpyAsync(&tot[1], d_slotoff + ni, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MWB_CUDA(cudaMemcpyAsync(&tot[2], d_terr, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MWB_CUDA(cudaStreamSynchronize(s));
+        if (tot[2] != 0) throw Error(-3, "input tree nodes are not in level order");
+        nchunks = tot[0];
+        nslots = tot[1];
         d_chunks = (Chunk*)dalloc(ctx, sizeof(Chunk) * std::max(1, nchunks));
         k_tchunks<<<(ni * 32 + 127) / 128, 128, 0, s>>>(d_offs, d_toff, ni, d_tkey, chunk_limit, 1, d_nchunk, d_choff,
                                                    d_slotoff, d_chunks);
-        int terr = 0;
-        MWB_CUDA(cudaMemcpyAsync(&terr, d_terr, sizeof(int), cudaMemcpyDeviceToHost, s));
-        MWB_CUDA(cudaStreamSynchronize(s));
-        if (terr != 0) throw Error(-3, "input tree nodes are not in level order");
         // block images of this pass's input nodes (the entries' depth levels) and generated nodes
         const long long nimg = nreal + nu;
         if (nimg > 0) {
@@ -1688,8 +1691,14 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
                                                    nullptr);
         k_multi_slots<<<(ni + 127) / 128, 128, 0, s>>>(d_nchunk, ni, d_nslot);
         count(ctx, 2);
-        nchunks = scan_total(ctx, d_nchunk, d_choff, ni);
-        nslots = scan_total(ctx, d_nslot, d_slotoff, ni);
+        scan_only(ctx, d_nchunk, d_choff, ni);
+        scan_only(ctx, d_nslot, d_slotoff, ni);
+        int tot[2] = {0, 0};
+        MWB_CUDA(cudaMemcpyAsync(&tot[0], d_choff + ni, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MWB_CUDA(cudaMemcpyAsync(&tot[1], d_slotoff + ni, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MWB_CUDA(cudaStreamSynchronize(s));
+        nchunks = tot[0];
+        nslots = tot[1];
         d_chunks = (Chunk*)dalloc(ctx, sizeof(Chunk) * std::max(1, nchunks));
         k_bchunks<<<(ni + 127) / 128, 128, 0, s>>>(d_offs, ni, d_ntrip, chunk_limit, 1, d_nchunk, d_choff, d_slotoff,
                                                    d_chunks);
@@ -1746,25 +1755,39 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     count(ctx);
     ctx->apply_launches++;
     ctx->apply_ctas += nchunks;
-    if (nslots > 0) {
-        int* d_mflags = (int*)dalloc(ctx, sizeof(int) * (ni + 1));
-        int* d_mpos = (int*)dalloc(ctx, sizeof(int) * (ni + 1));
-        MWB_CUDA(cudaMemsetAsync(d_mflags, 0, sizeof(int) * (ni + 1), s));
-        k_multi_flags<<<(ni + 255) / 256, 256, 0, s>>>(d_choff, ni, d_mflags);
-        const int nmulti = scan_total(ctx, d_mflags, d_mpos, ni);
-        int* d_mlist = (int*)dalloc(ctx, sizeof(int) * std::max(1, nmulti));
-        k_list_from_flags<<<(ni + 255) / 256, 256, 0, s>>>(d_mflags, d_mpos, ni, d_mlist);
-#define L_RED(KK) k_breduce<KK><<<nmulti, 256, 0, s>>>(d_chunks, d_choff, d_mlist, d_items, d_trees, d_partials);
+    if (nslots > 0) {  // one block per item; items whose node took one chunk leave at once
+#define L_RED(KK) k_breduce<KK><<<ni, 256, 0, s>>>(d_chunks, d_choff, nullptr, d_items, d_trees, d_partials);
         MWB_DISPATCH_K(K, L_RED)
 #undef L_RED
         MWB_CUDA(cudaGetLastError());
-        count(ctx, 3);
-        dfree(ctx, d_mflags);
-        dfree(ctx, d_mpos);
-        dfree(ctx, d_mlist);
+        count(ctx);
     }
+
+    // 6. root norms and thresholds (root entries), split flags; one read-back for the pass's results
+    bool any_root = false;
+    for (int t = 0; t < nt; ++t) any_root |= bp.trees[t].depth == 0;
+    double* d_g = nullptr;
+    if (any_root) {
+        d_g = (double*)dalloc(ctx, sizeof(double) * nt);
+        std::vector<double> precs(nt);
+        for (int t = 0; t < nt; ++t) precs[t] = bp.trees[t].prec;
+        double* d_prec = upload(ctx, precs);
+        k_tree_item_norm2<<<nt, 256, 0, s>>>(d_items, d_item_off, d_trees, d_g);
+        k_root_thr<<<(nt + 127) / 128, 128, 0, s>>>(d_trees, d_g, d_prec, nt);
+        MWB_CUDA(cudaGetLastError());
+        count(ctx, 2);
+        dfree(ctx, d_prec);
+    }
+    int* d_sflags = (int*)dalloc(ctx, sizeof(int) * (ni + 1));
+    k_bsplit_flags<<<(ni + 255) / 256, 256, 0, s>>>(d_items, ni, d_trees, d_sflags);
+    MWB_CUDA(cudaGetLastError());
+    count(ctx);
     unsigned long long ntot[2] = {0, 0};
+    std::vector<int> sflags(ni);
+    std::vector<double> g(any_root ? nt : 0);
     MWB_CUDA(cudaMemcpyAsync(ntot, d_ntrip_tot, sizeof(ntot), cudaMemcpyDeviceToHost, s));
+    MWB_CUDA(cudaMemcpyAsync(sflags.data(), d_sflags, sizeof(int) * ni, cudaMemcpyDeviceToHost, s));
+    if (any_root) MWB_CUDA(cudaMemcpyAsync(g.data(), d_g, sizeof(double) * nt, cudaMemcpyDeviceToHost, s));
     MWB_CUDA(cudaStreamSynchronize(s));
     if ((ntot[1] & 0xffffffffull) != 0)
         throw Error(-2, "tensor-core contraction: an MMA or copy completion wait exceeded its time limit");
@@ -1774,51 +1797,17 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         ctx->apply_ms += ms;
     }
     bp.triples = (long long)ntot[0];
-
-    // 6. root norms (g0 per root entry), then split lists per entry
-    bool any_root = false;
-    for (int t = 0; t < nt; ++t) any_root |= bp.trees[t].depth == 0;
-    if (any_root) {
-        double* d_g = (double*)dalloc(ctx, sizeof(double) * nt);
-        k_tree_item_norm2<<<nt, 256, 0, s>>>(d_items, d_item_off, d_trees, d_g);
-        count(ctx);
-        std::vector<double> g(nt);
-        MWB_CUDA(cudaMemcpyAsync(g.data(), d_g, sizeof(double) * nt, cudaMemcpyDeviceToHost, s));
-        MWB_CUDA(cudaStreamSynchronize(s));
-        for (int t = 0; t < nt; ++t)
-            if (bp.trees[t].depth == 0) bp.trees[t].g0 = std::sqrt(g[t]);
-        dfree(ctx, d_g);
-    }
-    for (int t = 0; t < nt; ++t) {
-        const BatchTree& b = bp.trees[t];
-        bt[t].thr = (b.prec > 0.0 && b.g0 > 0.0) ? b.prec * b.g0 * std::pow(2.0, -0.5 * b.depth) : INFINITY;
-    }
-    MWB_CUDA(cudaMemcpyAsync(d_trees, bt.data(), sizeof(BTree) * nt, cudaMemcpyHostToDevice, s));
-    int* d_sflags = (int*)dalloc(ctx, sizeof(int) * (ni + 1));
-    int* d_spos = (int*)dalloc(ctx, sizeof(int) * (ni + 1));
-    MWB_CUDA(cudaMemsetAsync(d_sflags, 0, sizeof(int) * (ni + 1), s));
-    k_bsplit_flags<<<(ni + 255) / 256, 256, 0, s>>>(d_items, ni, d_trees, d_sflags);
-    count(ctx);
-    const int nsplit = scan_total(ctx, d_sflags, d_spos, ni);
+    for (int t = 0; t < nt; ++t)
+        if (bp.trees[t].depth == 0) bp.trees[t].g0 = std::sqrt(g[t]);
     bp.split_lists.assign(nt, {});
-    if (nsplit > 0) {
-        int* d_slist = (int*)dalloc(ctx, sizeof(int) * nsplit);
-        k_bsplit_list<<<(ni + 255) / 256, 256, 0, s>>>(d_sflags, d_spos, d_items, ni, d_slist);
-        int* d_bpos = (int*)dalloc(ctx, sizeof(int) * (nt + 1));
-        k_gather_int<<<1, 256, 0, s>>>(d_spos, d_item_off, nt + 1, d_bpos);
-        count(ctx, 2);
-        std::vector<int> bpos(nt + 1), slist(nsplit);
-        MWB_CUDA(cudaMemcpyAsync(bpos.data(), d_bpos, sizeof(int) * (nt + 1), cudaMemcpyDeviceToHost, s));
-        MWB_CUDA(cudaMemcpyAsync(slist.data(), d_slist, sizeof(int) * nsplit, cudaMemcpyDeviceToHost, s));
-        MWB_CUDA(cudaStreamSynchronize(s));
-        for (int t = 0; t < nt; ++t) bp.split_lists[t].assign(slist.begin() + bpos[t], slist.begin() + bpos[t + 1]);
-        dfree(ctx, d_slist);
-        dfree(ctx, d_bpos);
-    }
+    for (int t = 0; t < nt; ++t)
+        for (int i = item_off[t]; i < item_off[t + 1]; ++i)
+            if (sflags[i]) bp.split_lists[t].push_back(items[i].node);
+    dfree(ctx, d_g);
     for (void* p : std::initializer_list<void*>{d_items, d_trees, d_item_off, d_count, d_offs, d_ngreq, d_cdelta, d_csrc,
                                                 d_greq_key, d_greq_leaf, d_ukey, d_uleaf, d_gblk, d_gnorm2, d_cand_item,
                                                 d_ntrip, d_nchunk, d_choff, d_nslot, d_slotoff, d_chunks, d_partials,
-                                                d_ntrip_tot, d_sflags, d_spos, d_toff, d_tkey, d_tval, d_terr, d_ximg})
+                                                d_ntrip_tot, d_sflags, d_toff, d_tkey, d_tval, d_terr, d_ximg})
         dfree(ctx, p);
     bp.nchunks = nchunks;
     bp.nslots = nslots;

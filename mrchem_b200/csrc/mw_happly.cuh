@@ -11,15 +11,17 @@
 //
 // x step (tensor cores).  One GEMM per triple, D[(y, z)][x'] += sum_x X[(y, z)][x] Mx[x'][x], with
 // M = the R = (2k)^2 data rows (y, z) in tiles of 128 TMEM lanes, K = x (16 per instruction) and
-// N = three column blocks of 2k: the data block and the operator are each written as three BF16 slices
-// of a per-row fixed-point form (mw_slice.hpp), and the operator slices are stacked along N so that
-//     data slice 0 x [m0 | m1 | m2],   data slice 1 x [0 | m0 | m1],   data slice 2 x [0 | 0 | m0]
-// put the products of equal weight 2^-16 / 2^-24 / 2^-32 into column blocks 0 / 1 / 2.  Within one
-// block row every block holds exact multiples of one quantum below 2^24 quanta, so the tensor core's
-// FP32 accumulation is exact inside a triple; the triples of a line accumulate in TMEM (the MMA
-// accumulate flag), and the line's epilogue adds the three blocks (round to nearest) into the y step's
-// operand.  Products dropped by the scheme (slice pairs of weight <= 2^-40 of the row scales) and the
-// slicing remainder (2^-25 of the row maximum) are below FP32 rounding of the same products.
+// N = three column blocks of 2k: the data block is written as four and the operator as three BF16
+// slices of a per-row fixed-point form (mw_slice.hpp), and the operator slices are stacked along N so that
+//     data slice 0 x [m0 | m1 | m2],   data slice 1 x [0 | m0 | m1],   data slices 2, 3 x [0 | 0 | m0]
+// put the products of weight 2^-16 / 2^-24 / 2^-32 (and 2^-40) into column blocks 0 / 1 / 2.  Within one
+// block row blocks 0 and 1 hold exact multiples of one quantum below 2^24 quanta, so the tensor core's
+// FP32 accumulation is exact there inside a triple; block 2 rounds at 2^-24 of its own size, itself
+// below 2^-9 of the products.  The triples of a line accumulate in TMEM (the MMA accumulate flag), and
+// the line's epilogue adds the three blocks (round to nearest) into the y step's operand.  Products
+// dropped by the scheme (slice pairs of weight <= 2^-40 of the row scales), the operator's slicing
+// remainder (2^-25 of its row maximum) and the data's (2^-33) are below FP32 rounding of the products;
+// the data's fourth slice matters because a block's slicing error repeats in every triple that reads it.
 // Staging: each triple's data image (built once per pass by k_simage) and operator image travel by one
 // 1-D bulk copy each (cp.async.bulk, completion on an mbarrier) into one of two buffers; the copy for
 // the next triple overlaps the current triple's MMAs.  At a line's end the MMAs of the next line's first
@@ -69,7 +71,7 @@ struct HCfg {
     static constexpr int PACK = K2 > 16 ? 1 : 0;  // the packed step over x = 16 .. K2-1
     static constexpr int W = K2;
     static constexpr int NCOL = (3 * W + 15) / 16 * 16;
-    static constexpr int IMGB = (3 * NCHM + 2 * PACK) * R * 16;
+    static constexpr int IMGB = (4 * NCHM + 2 * PACK) * R * 16;  // four data slices
     static constexpr int W2 = K;  // s->s block of the x step (x', x < k; data rows y, z < k)
     static constexpr int NCOL2 = (3 * W2 + 15) / 16 * 16;
     static constexpr int NBQ = NCOL + NCOL2;  // rows of one data slice's operand: whole matrix, then s->s block
@@ -96,12 +98,13 @@ struct HCfg {
     static constexpr int NCW = 128;  // threads that take correction tiles
     static constexpr int NC = hc_nc(K, NCW);
     static constexpr int NCT = KK / NC;
-    static constexpr int MAXT = 256;  // triples per chunk whose records are kept in shared memory
+    static constexpr int MAXT = 124;  // triples per chunk whose 16-byte records are kept in shared memory
     static constexpr size_t SMEM = 2 * (size_t)BUF + sizeof(float) * (2 * (size_t)KP * LDT + 2 * MATP + 3 * KKK) +
-                                   MAXT * 24 + 128;
+                                   MAXT * 16;
+    static constexpr int SMEM_STATIC = 64;  // the kernel's own __shared__ words (mbarriers, TMEM address, flag)
     // the last tile reads (TILES 128 - R) rows past the last chunk: they land in the operator image
     static constexpr bool FITS = (KP == 16 || KP == 20) && K <= 10 && K2 > 8 && NCOL <= 256 && TCOLS_NEED <= 512 &&
-                                 SMEM + 1024 <= 232448 && 2 * NCT <= NCW && NWARP >= 8 && (TILES * 128 - R) * 16 <= OPB;
+                                 SMEM + SMEM_STATIC <= 232448 && 2 * NCT <= NCW && NWARP >= 8 && (TILES * 128 - R) * 16 <= OPB;
 };
 
 // Block images of the tensor-core x step, one CTA per block: the FP64 block (or the generated k^3
@@ -113,6 +116,7 @@ __global__ void __launch_bounds__(512) k_simage(const ImgSrc* __restrict__ srcs,
                                                 long long nreal, unsigned char* __restrict__ img) {
     using C = HCfg<K>;
     constexpr int K2 = C::K2, R = C::R, NCHM = C::NCHM, BS = K2 * K2 * K2, KKK = K * K * K, LDR = K2 + 1;
+    constexpr int NLD = (BS + 511) / 512;  // values per thread (512 threads)
     extern __shared__ __align__(16) unsigned char smraw[];
     double* blk = reinterpret_cast<double*>(smraw);  // [R][LDR]
     const long long slot = blockIdx.x;
@@ -125,12 +129,30 @@ __global__ void __launch_bounds__(512) k_simage(const ImgSrc* __restrict__ srcs,
         }
         const ImgSrc sr = srcs[lo];
         const double* b = sr.coef + (size_t)(sr.lb + (slot - sr.base)) * BS;
-        for (int e = threadIdx.x; e < BS; e += blockDim.x) blk[(e / K2) * LDR + e % K2] = b[e];
+        double v[NLD];  // every load of this thread in flight before the first shared store
+#pragma unroll
+        for (int i = 0; i < NLD; ++i) {
+            const int e = threadIdx.x + 512 * i;
+            v[i] = e < BS ? __ldcs(b + e) : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < NLD; ++i) {
+            const int e = threadIdx.x + 512 * i;
+            if (e < BS) blk[(e / K2) * LDR + e % K2] = v[i];
+        }
     } else {
         const double* g = gblk + (size_t)(slot - nreal) * KKK;
-        for (int e = threadIdx.x; e < BS; e += blockDim.x) {
+        double v[NLD];
+#pragma unroll
+        for (int i = 0; i < NLD; ++i) {
+            const int e = threadIdx.x + 512 * i;
             const int a = e % K2, bb = (e / K2) % K2, c = e / (K2 * K2);
-            blk[(e / K2) * LDR + a] = (a < K && bb < K && c < K) ? g[a + K * (bb + K * c)] : 0.0;
+            v[i] = (e < BS && a < K && bb < K && c < K) ? g[a + K * (bb + K * c)] : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < NLD; ++i) {
+            const int e = threadIdx.x + 512 * i;
+            if (e < BS) blk[(e / K2) * LDR + e % K2] = v[i];
         }
     }
     __syncthreads();
@@ -151,22 +173,26 @@ __global__ void __launch_bounds__(512) k_simage(const ImgSrc* __restrict__ srcs,
         if (m > 0.0) frexp(m, &e);
         const double scale = ldexp(1.0, -e);
         const float inv256 = ldexpf(1.0f, e - 8);
-        float s[3][16 + 8 * NCHM];
 #pragma unroll
-        for (int x = 0; x < 16 + 8 * NCHM; ++x) {
-            if (x < K2) slice3_value(row[x], scale, inv256, s[0][x], s[1][x], s[2][x]);
-            else s[0][x] = s[1][x] = s[2][x] = 0.0f;
+        for (int c = 0; c < NCHM; ++c) {  // x = 8 c .. 8 c + 7 of the four slices
+            float s[4][8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (8 * c + j < K2) slice4_value(row[8 * c + j], scale, inv256, s[0][j], s[1][j], s[2][j], s[3][j]);
+                else s[0][j] = s[1][j] = s[2][j] = s[3][j] = 0.0f;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) put(q * NCHM + c, r, s[q]);
         }
-#pragma unroll
-        for (int q = 0; q < 3; ++q)
-#pragma unroll
-            for (int c = 0; c < NCHM; ++c) put(q * NCHM + c, r, &s[q][8 * c]);
-        if constexpr (C::PACK) {  // [s0 | s1 | s2 | 0] of x = 16 .., four K slots per slice
+        if constexpr (C::PACK) {  // [s0 | s1 | s2 | s3] of x = 16 .., four K slots per slice
             float pk[16];
 #pragma unroll
-            for (int e2 = 0; e2 < 16; ++e2) pk[e2] = (e2 < 12 && 16 + (e2 & 3) < K2) ? s[e2 >> 2][16 + (e2 & 3)] : 0.0f;
-            put(3 * NCHM, r, pk);
-            put(3 * NCHM + 1, r, pk + 8);
+            for (int l = 0; l < 4; ++l) {
+                if (16 + l < K2) slice4_value(row[16 + l], scale, inv256, pk[l], pk[4 + l], pk[8 + l], pk[12 + l]);
+                else pk[l] = pk[4 + l] = pk[8 + l] = pk[12 + l] = 0.0f;
+            }
+            put(4 * NCHM, r, pk);
+            put(4 * NCHM + 1, r, pk + 8);
         }
     }
 }
@@ -211,13 +237,15 @@ __device__ __forceinline__ void gemm_tile_split(const float* __restrict__ A, con
     }
 }
 
-// record of one triple of a chunk, kept in shared memory for the first MAXT triples
+// record of one triple of a chunk (16 bytes), kept in shared memory for the first MAXT triples; a
+// matrix index fits 27 bits (2^27 matrices of (2k)^2 FP64 values would exceed any device memory)
 struct HTri {
     int slot;  // block image slot of the input node
-    int mx, my, mz;
-    int flags;  // HT_* below
-    int pad;
+    int mx, my;
+    unsigned mz : 27;
+    unsigned flags : 5;  // HT_* below
 };
+static_assert(sizeof(HTri) == 16, "triple record");
 enum { HT_GEN = 1, HT_LSTART = 2, HT_LEND = 4, HT_PSTART = 8, HT_PEND = 16 };
 
 __device__ __forceinline__ void named_bar(int id, int nthr) {
@@ -288,10 +316,9 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
         h.slot = (int)(src < 0 ? gbase + (-src - 1) : TR.img_base + (src - TR.img_lb));
         h.mx = tr.mx;
         h.my = tr.my;
-        h.mz = tr.mz;
+        h.mz = (unsigned)tr.mz;
         h.flags = (src < 0 ? HT_GEN : 0) | (lp != lk ? HT_LSTART : 0) | (ln != lk ? HT_LEND : 0) |
                   ((lp >> 10) != (lk >> 10) ? HT_PSTART : 0) | ((ln >> 10) != (lk >> 10) ? HT_PEND : 0);
-        h.pad = 0;
         return h;
     };
     for (int e = tid; e < min(ntri, C::MAXT); e += C::NTHR) meta[e] = load_rec(ch.c0 + e);
@@ -341,17 +368,18 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
                     const bool live = !gen || tl < C::TILES_GEN;
                     // below the root the first tiles also take the s->s block's sums (N = NCOL + NCOL2)
                     const uint32_t id = (!root && tl < C::TILES_GEN) ? idesc2 : idesc;
-                    static_for<3>([&](auto SQ) {  // x = 0 .. 15 of data slice sq against its operand
+                    static_for<4>([&](auto SQ) {  // x = 0 .. 15 of data slice sq against its operand
                         constexpr int sq = decltype(SQ)::value;
+                        constexpr int oq = sq < 3 ? sq : 2;  // slice 3 takes slice 2's operand
                         const bool init = first && sq == 0;
                         if (!live && !init) return;
                         const uint64_t ad = da + (uint64_t)((sq * C::NCHM * R * 16 + tl * 2048) >> 4);
-                        const uint64_t bd = dbq + (uint64_t)((sq * C::OPB_Q) >> 4);
+                        const uint64_t bd = dbq + (uint64_t)((oq * C::OPB_Q) >> 4);
                         umma_bf16(tbase + (uint32_t)C::tcol(tl), ad, bd, id, init ? 0u : 1u);
                     });
                     if constexpr (C::PACK) {  // x = 16 .. K2-1 of all slices in one step (whole matrix only)
                         if (!gen) {
-                            const uint64_t ad = da + (uint64_t)((3 * C::NCHM * R * 16 + tl * 2048) >> 4);
+                            const uint64_t ad = da + (uint64_t)((4 * C::NCHM * R * 16 + tl * 2048) >> 4);
                             umma_bf16(tbase + (uint32_t)C::tcol(tl), ad, dq, idesc, 1u);
                         }
                     }

@@ -1,15 +1,18 @@
-// mw_slice.hpp -- three-slice BF16 fixed-point form of FP64 rows, and the shared-memory image layouts of
-// the tensor-core x step (k_happly).  Shared by the host (operator images) and the device (block images).
+// mw_slice.hpp -- BF16 fixed-point slices of FP64 rows, and the shared-memory image layouts of the
+// tensor-core x step (k_happly).  Shared by the host (operator images) and the device (block images).
 //
 // A row v[0 .. n) with largest magnitude m = f 2^e (f in [1/2, 1)) is written as
-//     v = 2^e (n1 2^-8 + n2 2^-16 + n3 2^-24) + r,   |r| <= 2^(e-25),
-// with integers |n1| <= 256, |n2|, |n3| <= 128 (each slice rounded to nearest from what the previous
-// ones leave).  Every slice value n 2^(e - 8 s) has at most 8 significant bits, so it is exact in BF16.
-// Products of a data slice and an operator slice are then exact multiples of one quantum per
-// (row, column, slice pair), and sums of up to 2^5 of them stay below 2^24 quanta: the tensor core's FP32
-// accumulation adds them without rounding.  This is the splitting idea of the Ozaki scheme (Ozaki,
-// Ogita, Oishi & Rump, Numer. Algorithms 59, 2012; on integer/low-precision matrix engines: Ootomo,
-// Ozaki & Yokota, IJHPCA 2024) with per-row power-of-two scales.
+//     v = 2^e (n1 2^-8 + n2 2^-16 + n3 2^-24 [+ n4 2^-32]) + r,
+// with integers |n1| <= 256, |n2|, |n3|, |n4| <= 128 (each slice rounded to nearest from what the previous
+// ones leave): |r| <= 2^(e-25) with three slices (operators), 2^(e-33) with four (data blocks).  Every
+// slice value n 2^(e - 8 s) has at most 8 significant bits, so it is exact in BF16.  Products of a data
+// slice and an operator slice are then exact multiples of one quantum per (row, column, slice pair), and
+// sums of up to 2^5 of them stay below 2^24 quanta: the tensor core's FP32 accumulation adds them without
+// rounding.  This is the splitting idea of the Ozaki scheme (Ozaki, Ogita, Oishi & Rump, Numer.
+// Algorithms 59, 2012; on integer/low-precision matrix engines: Ootomo, Ozaki & Yokota, IJHPCA 2024) with
+// per-row power-of-two scales.  The data side takes a fourth slice because a data block's slicing error
+// is the same in every triple that reads the block (it does not average out over the operator's terms),
+// while the remainder relative to the row maximum is coarse for the small entries of a row.
 #pragma once
 #include <cmath>
 #include <cstdint>
@@ -42,21 +45,23 @@ MWB_HD inline void slice3_row(const double* v, int n, int stride, float* s0, flo
     }
 }
 
-// Same slices with the remainder after the first slice carried in FP32: r1 = u - s0 (|r1| <= 2^-9 |m|) is
-// exact in FP64 and rounded to FP32 once (relative 2^-24, i.e. 2^-33 of the row maximum, far below the
-// last slice's quantum 2^-24); the rest is exact in FP32.  Equal to slice3_row except for rows whose
-// remainders round at that level; used by the device image kernel (one FP64 multiply, rounding and
-// FMA per value).
-MWB_HD inline void slice3_value(double v, double scale, float inv256, float& s0, float& s1, float& s2) {
+// Four slices of one value with the remainder after the first slice carried in FP32: r1 = u - s0
+// (|r1| <= 2^-9 |m|) is exact in FP64 and rounded to FP32 once (2^-33 of the row maximum, the size of the
+// last slice's half quantum); the later remainders are exact in FP32.  One FP64 multiply, rounding and FMA
+// per value; the first three slices equal slice3_row's except where r1 rounds at that level.
+MWB_HD inline void slice4_value(double v, double scale, float inv256, float& s0, float& s1, float& s2, float& s3) {
     const double u = v * scale;  // |u| < 1, exact (power-of-two scale)
     const double a = rint(u * 256.0);
     const float r1 = (float)fma(a, -1.0 / 256.0, u);
     const float b = rintf(r1 * 65536.0f);
     const float r2 = fmaf(b, -1.0f / 65536.0f, r1);
     const float c = rintf(r2 * 16777216.0f);
+    const float r3 = fmaf(c, -1.0f / 16777216.0f, r2);
+    const float d = rintf(r3 * 4294967296.0f);
     s0 = (float)a * inv256;
     s1 = b * (inv256 * (1.0f / 256.0f));
     s2 = c * (inv256 * (1.0f / 65536.0f));
+    s3 = d * (inv256 * (1.0f / 16777216.0f));
 }
 
 // BF16 bits of a float with at most 8 significant bits (the low 16 bits of its pattern are zero)
@@ -72,15 +77,17 @@ MWB_HD inline uint16_t bf16_bits_exact(float x) {
 
 // Image geometry of the tensor-core x step for 2k = K2 <= 20 (see k_happly).  A "chunk" is R rows x 16
 // bytes (8 BF16 values per row); row r = y + K2 z of the data.
-//   data block image: slices 0, 1, 2, each NCHM chunks holding x = 0 .. 8 NCHM - 1 (zero for x >= K2);
-//   then, when K2 > 16, two packed chunks holding per row [s0 | s1 | s2 | 0] of x = 16 .. K2 - 1
-//   (LO = K2 - 16 values per slice), so that one 16-deep MMA step covers the rest of x for all slices;
+//   data block image: slices 0, 1, 2, 3, each NCHM chunks holding x = 0 .. 8 NCHM - 1 (zero for x >= K2);
+//   then, when K2 > 16, two packed chunks holding per row [s0 | s1 | s2 | s3] of x = 16 .. K2 - 1
+//   (LO = K2 - 16 <= 4 values per slice), so that one 16-deep MMA step covers the rest of x for all slices;
 //   operator image, one per NS matrix M[x'][x]: (a) for each data slice q = 0, 1, 2 an operand of
-//   NCH2 = NCOL + NCOL2 rows x NCHM chunks: row b W + x' (column block b = 0, 1, 2 of the whole matrix)
+//   NBQ = NCOL + NCOL2 rows x NCHM chunks: row b W + x' (column block b = 0, 1, 2 of the whole matrix)
 //   holds slice b - q of M[x'][0 .. 8 NCHM) when b >= q, and row NCOL + b W2 + x' (x' < k) holds slice
 //   b - q of the s->s block row M[x'][0 .. k), zero elsewhere (slice pairs of equal weight land in equal
-//   output columns); (b) when K2 > 16, the packed step's operand, two chunks of NCOL rows: row b W + x'
-//   holds, at K offset 4 q (q = 0, 1, 2), slice b - q of M[x'][16 ..] when b >= q, else zero.
+//   output columns); data slice 3 takes the operand of slice 2 (column block 2 = operator slice 0, the
+//   products of weight 2^-40 added into block 2); (b) when K2 > 16, the packed step's operand, two chunks
+//   of NCOL rows: row b W + x' holds, at K offset 4 q (q = 0, 1, 2), slice b - q of M[x'][16 ..] when
+//   b >= q, and row 2 W + x' at K offset 12 (data slice 3) slice 0, zero elsewhere.
 struct XGeo {
     int K2, R, TILES, NCHM, PACK, LO, W, NCOL, W2, NCOL2, NBQ, IMGB, OPB_Q, OPB_A, OPB_B, OPB;
     MWB_HD explicit XGeo(int k2)
@@ -88,7 +95,7 @@ struct XGeo {
           LO(k2 > 16 ? k2 - 16 : 0), W(k2), NCOL((3 * k2 + 15) / 16 * 16), W2(k2 / 2),
           NCOL2((3 * (k2 / 2) + 15) / 16 * 16),
           NBQ((3 * k2 + 15) / 16 * 16 + (3 * (k2 / 2) + 15) / 16 * 16),
-          IMGB((3 * (k2 > 8 ? 2 : 1) + (k2 > 16 ? 2 : 0)) * k2 * k2 * 16),
+          IMGB((4 * (k2 > 8 ? 2 : 1) + (k2 > 16 ? 2 : 0)) * k2 * k2 * 16),
           OPB_Q((k2 > 8 ? 2 : 1) * ((3 * k2 + 15) / 16 * 16 + (3 * (k2 / 2) + 15) / 16 * 16) * 16),
           OPB_A(3 * (k2 > 8 ? 2 : 1) * ((3 * k2 + 15) / 16 * 16 + (3 * (k2 / 2) + 15) / 16 * 16) * 16),
           OPB_B(k2 > 16 ? 2 * ((3 * k2 + 15) / 16 * 16) * 16 : 0),
