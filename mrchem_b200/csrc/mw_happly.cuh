@@ -34,7 +34,9 @@
 // and one 4-byte load.
 //
 // Below the root the s->s block (T x T x T on the scaling part) is left out, as in k_gapply: the k^3
-// correction GEMMs run on the CUDA cores, their input rebuilt from the data slices.
+// correction GEMMs run on the CUDA cores (the x step's part as extra MMA columns).  Each plane's correction
+// block is added into FP64 sums in TMEM by the warps that compute it, and the sums are subtracted once,
+// when the chunk's block is written.
 //
 // Every mbarrier wait has a time limit: a wait that runs out sets the kernel's error word, and the CTA
 // leaves after waiting (again with a limit) for the copies and MMAs it started.
@@ -89,8 +91,7 @@ struct HCfg {
     __host__ __device__ static constexpr int tcol(int t) { return t < TILES_GEN ? t * TSTR_C : TILES_GEN * TSTR_C + (t - TILES_GEN) * TSTR; }
     static constexpr int ACC0 = TILES_GEN * TSTR_C + (TILES - TILES_GEN) * TSTR;
     static constexpr int NWQ = (NWARP + 3) / 4;
-    static constexpr int TCOLS_NEED = ACC0 + NWQ * 2 * ND;
-    static constexpr int TCOLS = TCOLS_NEED <= 128 ? 128 : TCOLS_NEED <= 256 ? 256 : 512;
+    static constexpr int CS0 = ACC0 + NWQ * 2 * ND;  // FP64 sums of the s->s corrections (correction warps)
     // s->s correction of the y and z steps
     static constexpr int KK = K * K, KKK = K * K * K;
     // correction tiles (MT rows x NC columns) on the warps of lane quarters 2 and 3 only (warps 2, 3, 6, 7):
@@ -98,13 +99,16 @@ struct HCfg {
     static constexpr int NCW = 128;  // threads that take correction tiles
     static constexpr int NC = hc_nc(K, NCW);
     static constexpr int NCT = KK / NC;
-    static constexpr int MAXT = 124;  // triples per chunk whose 16-byte records are kept in shared memory
-    static constexpr size_t SMEM = 2 * (size_t)BUF + sizeof(float) * (2 * (size_t)KP * LDT + 2 * MATP + 3 * KKK) +
+    static constexpr int CSW = 2 * MT * NC;  // TMEM words of one correction thread's sums
+    static constexpr int TCOLS_NEED = CS0 + 2 * CSW;  // two correction warps per lane quarter
+    static constexpr int TCOLS = TCOLS_NEED <= 128 ? 128 : TCOLS_NEED <= 256 ? 256 : 512;
+    static constexpr int MAXT = 372;  // triples per chunk whose 16-byte records are kept in shared memory
+    static constexpr size_t SMEM = 2 * (size_t)BUF + sizeof(float) * (2 * (size_t)KP * LDT + 2 * MATP + 2 * KKK) +
                                    MAXT * 16;
     static constexpr int SMEM_STATIC = 64;  // the kernel's own __shared__ words (mbarriers, TMEM address, flag)
     // the last tile reads (TILES 128 - R) rows past the last chunk: they land in the operator image
     static constexpr bool FITS = (KP == 16 || KP == 20) && K <= 10 && K2 > 8 && NCOL <= 256 && TCOLS_NEED <= 512 &&
-                                 SMEM + SMEM_STATIC <= 232448 && 2 * NCT <= NCW && NWARP >= 8 && (TILES * 128 - R) * 16 <= OPB;
+                                 SMEM + SMEM_STATIC <= 232448 && 2 * NCT <= NCW && 8 * KKK <= 4 * KP * LDT && NWARP >= 8 && (TILES * 128 - R) * 16 <= OPB;
 };
 
 // Block images of the tensor-core x step, one CTA per block: the FP64 block (or the generated k^3
@@ -294,8 +298,7 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
     float* Mz = My + MATP;
     float* U1 = Mz + MATP;  // [K][K][K]
     float* U2 = U1 + KKK;
-    float* Uc = U2 + KKK;
-    HTri* meta = reinterpret_cast<HTri*>(Uc + KKK);
+    HTri* meta = reinterpret_cast<HTri*>(U2 + KKK);
     const Chunk ch = chunks[blockIdx.x];
     const Item it = items[ch.item];
     const BTree& TR = trees[it.tree];
@@ -440,11 +443,15 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
         auto opos = [](int o) { return split_pos(o, MT, 4); };  // operator column of output index o
         const uint32_t tlane = tbase + ((uint32_t)(32 * quarter) << 16);
         const uint32_t tacc = tlane + (uint32_t)(C::ACC0 + (warp >> 2) * 2 * ND);
+        // the correction warps' FP64 sums of every plane's s->s correction, subtracted once at the end
+        const bool csum = !root && cwarp;  // warp-uniform (TMEM accesses are warp-collective)
+        const uint32_t tcs = tlane + (uint32_t)(C::CS0 + (warp >> 2) * C::CSW);
         {
             uint32_t z[2 * ND];
 #pragma unroll
             for (int q = 0; q < 2 * ND; ++q) z[q] = 0u;
             tmem_span_st<0, 2 * ND>(tacc, z);
+            if (csum) tmem_span_st<0, C::CSW>(tcs, z);
         }
         auto load_mat = [&](float* dst, const float* tab, int mi) {
             constexpr int NV = MATP * 4 / 16;
@@ -452,24 +459,13 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
             for (int e = tid; e < NV; e += NS) cp_async16(reinterpret_cast<char*>(dst) + 16 * e, src + 16 * e);
             cp_async_commit();
         };
-        // correction value of element (c' = o0 + i, a' = tb0 + j, b' = tc0) of this thread's z tile (zero
-        // outside the s->s block; a tile never wraps a row since NT divides KP)
+        // whether this thread's z tile holds elements of the s->s block (c', a', b' < k; a tile never wraps
+        // a row since NT divides KP)
         const bool tile_sss = o0 < K && tb0 < K && tc0 < K;
-        auto uc_at = [&](int i, int j) -> double {
-            return (o0 + i < K && tb0 + j < K) ? (double)Uc[(o0 + i) * KK + tb0 + j + K * tc0] : 0.0;
-        };
         float c2[MT][NC];
-        auto write_c2 = [&]() {
-            if (!cown) return;
-#pragma unroll
-            for (int i = 0; i < MT; ++i)
-#pragma unroll
-                for (int j = 0; j < NC; ++j)
-                    if (co0 + i < K) Uc[(co0 + i) * KK + cn0 + j] = c2[i][j];
-        };
         const int nq = (C::NWARP - quarter + 3) / 4;  // warps of this lane quarter
         uint32_t lph = 0;
-        bool pend2 = false, uc_valid = false, plane_gen = true, first_line = true;
+        bool plane_gen = true, first_line = true;
         float yacc[MT][NT];
         bool lgen = true;
         for (int t = ch.c0; t < ch.c1; ++t) {
@@ -543,11 +539,6 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
             if (tid == 0) mbar_arrive(&bars[5]);  // the producer may start the next line's MMAs
             if (bad) break;
             // ---- y: T2[c][a' + P b'] (+)= sum_b My[b'][b] T1[b][a' + P c]   (a plane sums its lines)
-            if (pend2) {  // the previous plane's correction block, subtracted in this plane's z phase
-                write_c2();
-                pend2 = false;
-                uc_valid = true;
-            }
             {
                 // this thread's y tile, summed over the plane's lines in registers (a tile of a generated
                 // line is zero when its z index c >= k)
@@ -604,7 +595,7 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
             }
             first_line = false;
             if (!pend) continue;
-            named_bar(1, NS);  // T2, U2 and Uc of the plane are complete
+            named_bar(1, NS);  // T2 and U2 of the plane are complete
             // ---- z: acc[c'][a' + P b'] += sum_c (beta Mz)[c'][c] T2[c][a' + P b']  (- previous correction)
             {
                 // FP64 accumulators in TMEM: one read of all this thread's words, issued ahead of the GEMM
@@ -616,19 +607,15 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
                 if (plane_gen) gemm_tile_split<MT, NT, NTILE, KP, LDT, K>(Mz, T2, rt, ct, c);
                 else gemm_tile_split<MT, NT, NTILE, KP, LDT, K2>(Mz, T2, rt, ct, c);
                 tmem_span_wait<0, 2 * ND>(r);
-                const bool fold = uc_valid && tile_sss;
 #pragma unroll
                 for (int i = 0; i < MT; ++i)
 #pragma unroll
                     for (int j = 0; j < NT; ++j) {
                         const int d = i * NT + j;
-                        double v = words_to_double(r[2 * d], r[2 * d + 1]) + (double)c[i][j];
-                        if (fold) v -= uc_at(i, j);
-                        double_to_words(v, r[2 * d], r[2 * d + 1]);
+                        double_to_words(words_to_double(r[2 * d], r[2 * d + 1]) + (double)c[i][j], r[2 * d], r[2 * d + 1]);
                     }
                 tmem_span_st<0, 2 * ND>(tacc, r);
             }
-            uc_valid = false;
             if (cown) {  // c2[c'][a' + k b'] = sum_{c<k} (beta Tz)[c'][c] U2[c][a' + k b']
 #pragma unroll
                 for (int i = 0; i < MT; ++i)
@@ -643,12 +630,39 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
                     }
                 }
             }
-            pend2 = !root;
+            if (csum) {  // add the plane's correction block into this thread's FP64 sums
+                uint32_t w[C::CSW];
+                tmem_wait_st();
+                tmem_span_ld<0, C::CSW>(tcs, w);
+                tmem_span_wait<0, C::CSW>(w);
+                if (cown) {
+#pragma unroll
+                    for (int i = 0; i < MT; ++i)
+#pragma unroll
+                        for (int j = 0; j < NC; ++j) {
+                            const int q = 2 * (i * NC + j);
+                            double_to_words(words_to_double(w[q], w[q + 1]) + (double)c2[i][j], w[q], w[q + 1]);
+                        }
+                }
+                tmem_span_st<0, C::CSW>(tcs, w);
+            }
         }
         cp_async_wait_all();
-        named_bar(1, NS);
-        if (!bad && pend2) write_c2();
-        uc_valid = pend2;
+        named_bar(1, NS);  // T1 is no longer read: it takes the s->s correction sums (FP64 [c'][a' + k b'])
+        double* Usum = reinterpret_cast<double*>(T1);
+        if (!bad && csum) {
+            uint32_t w[C::CSW];
+            tmem_wait_st();
+            tmem_span_ld<0, C::CSW>(tcs, w);
+            tmem_span_wait<0, C::CSW>(w);
+            if (cown) {
+#pragma unroll
+                for (int i = 0; i < MT; ++i)
+#pragma unroll
+                    for (int j = 0; j < NC; ++j)
+                        if (co0 + i < K) Usum[(co0 + i) * KK + cn0 + j] = words_to_double(w[2 * (i * NC + j)], w[2 * (i * NC + j) + 1]);
+            }
+        }
         named_bar(1, NS);
         if (!bad) {
             double* dst = ch.slot < 0 ? TR.ocoef + (size_t)it.node * BS : partials + (size_t)ch.slot * BS;
@@ -664,7 +678,7 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
                     const int d = i * NT + j;
                     double v = words_to_double(r[2 * d], r[2 * d + 1]);
                     const int cz = o0 + i, ax = tb0 + j, by = tc0;
-                    if (uc_valid && tile_sss) v -= uc_at(i, j);
+                    if (!root && tile_sss && cz < K && ax < K) v -= Usum[cz * KK + ax + K * by];
                     if (cz < K2 && ax < K2 && by < K2) {
                         dst[ax + K2 * (by + K2 * cz)] = v;
                         n2 += v * v;
