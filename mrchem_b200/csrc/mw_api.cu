@@ -31,6 +31,30 @@ void* dalloc(Ctx* ctx, size_t bytes) {
 void dfree(Ctx* ctx, void* p) {
     if (p) cudaFreeAsync(p, ctx->stream);
 }
+void upload_bytes(Ctx* ctx, void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return;
+    constexpr size_t kArena = 32u << 20;
+    if (!ctx->pin && bytes <= kArena / 4) {
+        MWB_CUDA(cudaMallocHost(&ctx->pin, kArena));
+        MWB_CUDA(cudaEventCreateWithFlags(&ctx->pin_ev, cudaEventDisableTiming));
+        ctx->pin_cap = kArena;
+        ctx->pin_off = 0;
+    }
+    if (!ctx->pin || bytes > ctx->pin_cap / 4) {  // large: pageable copy
+        MWB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        return;
+    }
+    if (ctx->pin_off + bytes > ctx->pin_cap) {  // wrap: every earlier copy from the arena has completed
+        if (ctx->pin_pending) MWB_CUDA(cudaEventSynchronize(ctx->pin_ev));
+        ctx->pin_off = 0;
+    }
+    char* h = ctx->pin + ctx->pin_off;
+    std::memcpy(h, src, bytes);
+    MWB_CUDA(cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    MWB_CUDA(cudaEventRecord(ctx->pin_ev, ctx->stream));
+    ctx->pin_pending = true;
+    ctx->pin_off += (bytes + 255) & ~(size_t)255;
+}
 
 // ---------------------------------------------------------------------------------------------
 // screening constants of the apply (same values as the CPU oracle)
@@ -107,12 +131,11 @@ void tree_make_roots(Tree& t) {
     launch_hash_reset(t, s);
     const int n = (int)keys.size();
     std::vector<int> par(n, -1);
-    MWB_CUDA(cudaMemcpyAsync(t.key, keys.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s));
-    MWB_CUDA(cudaMemcpyAsync(t.parent, par.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
-    MWB_CUDA(cudaMemcpyAsync(t.child0, par.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    upload_bytes(m.ctx, t.key, keys.data(), sizeof(uint64_t) * n);  // staged: the host vectors may go
+    upload_bytes(m.ctx, t.parent, par.data(), sizeof(int) * n);
+    upload_bytes(m.ctx, t.child0, par.data(), sizeof(int) * n);
     MWB_CUDA(cudaMemsetAsync(t.norm2, 0, sizeof(double) * n, s));
     MWB_CUDA(cudaMemsetAsync(t.wnorm2, 0, sizeof(double) * n, s));
-    MWB_CUDA(cudaStreamSynchronize(s));  // host vectors leave scope
     t.n = n;
     t.level_begin = {0, n};
     launch_hash_insert(t, 0, n, s);
@@ -1038,6 +1061,8 @@ static void ctx_free(mwb::Ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->pin_ev) cudaEventDestroy(ctx->pin_ev);
+    if (ctx->pin) cudaFreeHost(ctx->pin);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete static_cast<mw_ctx_s*>(ctx);
 }

@@ -1377,7 +1377,7 @@ static bool contraction_pencil() {
 template <typename T>
 static T* upload(Ctx* ctx, const std::vector<T>& v) {
     T* d = (T*)dalloc(ctx, sizeof(T) * std::max<size_t>(1, v.size()));
-    if (!v.empty()) MWB_CUDA(cudaMemcpyAsync(d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, ctx->stream));
+    upload_bytes(ctx, d, v.data(), sizeof(T) * v.size());
     return d;
 }
 // exclusive sum of d_in[0 .. n] into d_out (the total lands in d_out[n]); no host read-back

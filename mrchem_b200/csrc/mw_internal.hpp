@@ -50,6 +50,12 @@ struct Ctx {
     // handles that point here (worlds, networks); a destroyed context is freed with the last of them
     int refs = 0;
     bool closed = false;
+    // pinned staging arena for small host-to-device uploads (copies from pageable memory may drain the
+    // stream first); a region is reused only after the event recorded behind the latest copy completed
+    char* pin = nullptr;
+    size_t pin_cap = 0, pin_off = 0;
+    cudaEvent_t pin_ev = nullptr;
+    bool pin_pending = false;
 };
 
 struct Mra {
@@ -154,5 +160,8 @@ struct Tree {
 // device memory from the stream-ordered pool
 void* dalloc(Ctx* ctx, size_t bytes);
 void dfree(Ctx* ctx, void* p);
+// stream-ordered copy of `bytes` host bytes to device memory `dst` through the context's pinned arena
+// (pageable copy when the arena cannot hold them); the host buffer may be reused when this returns
+void upload_bytes(Ctx* ctx, void* dst, const void* src, size_t bytes);
 
 }  // namespace mwb

@@ -355,8 +355,8 @@ __global__ void k_make_children_many(const ChildTree* __restrict__ ts, const int
 }
 
 // deterministic single-block reductions (fixed summation order)
-__global__ void k_reduce_norm2(const double* __restrict__ norm2, const int* __restrict__ child0, int begin,
-                               int end, int leaves_only, int want_max, double* out) {
+__device__ __forceinline__ double reduce_norm2_block(const double* __restrict__ norm2, const int* __restrict__ child0,
+                                                     int begin, int end, int leaves_only, int want_max) {
     __shared__ double red[64];
     double s = 0.0, dummy = 0.0;
     for (int i = begin + threadIdx.x; i < end; i += blockDim.x) {
@@ -375,7 +375,25 @@ __global__ void k_reduce_norm2(const double* __restrict__ norm2, const int* __re
     } else {
         block_sum2(s, dummy, red);
     }
+    return s;
+}
+__global__ void k_reduce_norm2(const double* __restrict__ norm2, const int* __restrict__ child0, int begin,
+                               int end, int leaves_only, int want_max, double* out) {
+    const double s = reduce_norm2_block(norm2, child0, begin, end, leaves_only, want_max);
     if (threadIdx.x == 0) *out = s;
+}
+// both reductions of several trees in one launch: block b reduces tree b % nt, the leaf sum when
+// b < nt, else the largest node norm (the same blocks as k_reduce_norm2, so the same sums)
+struct NormSrc {
+    const double* norm2;
+    const int* child0;
+    int n;
+};
+__global__ void k_reduce_norm2_many(const NormSrc* __restrict__ src, int nt, double* out) {
+    const int t = blockIdx.x % nt, mx = blockIdx.x / nt;
+    const NormSrc ns = src[t];
+    const double s = reduce_norm2_block(ns.norm2, ns.child0, 0, ns.n, !mx, mx);
+    if (threadIdx.x == 0) out[mx * nt + t] = s;
 }
 
 __global__ void k_rescale(double* coef, size_t n, double c) {
@@ -514,8 +532,8 @@ void trees_finish(const std::vector<Tree*>& ts, bool sumup, bool compress, bool 
     for (Tree* t : ts) views.push_back(view(*t));
     int2* d_items = (int2*)dalloc(ctx, sizeof(int2) * items.size());
     TView* d_views = (TView*)dalloc(ctx, sizeof(TView) * views.size());
-    MWB_CUDA(cudaMemcpyAsync(d_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, s));
-    MWB_CUDA(cudaMemcpyAsync(d_views, views.data(), sizeof(TView) * views.size(), cudaMemcpyHostToDevice, s));
+    upload_bytes(ctx, d_items, items.data(), sizeof(int2) * items.size());
+    upload_bytes(ctx, d_views, views.data(), sizeof(TView) * views.size());
     WorldGeo wg = world_geo(m);
     auto level = [&](int mode, int d) {
         const int n = lvl_off[d + 1] - lvl_off[d];
@@ -643,8 +661,8 @@ void trees_add_children(const std::vector<Tree*>& ts, const std::vector<std::vec
     }
     int* d_buf = (int*)dalloc(ctx, sizeof(int) * buf.size());
     ChildTree* d_ct = (ChildTree*)dalloc(ctx, sizeof(ChildTree) * ct.size());
-    MWB_CUDA(cudaMemcpyAsync(d_buf, buf.data(), sizeof(int) * buf.size(), cudaMemcpyHostToDevice, s));
-    MWB_CUDA(cudaMemcpyAsync(d_ct, ct.data(), sizeof(ChildTree) * ct.size(), cudaMemcpyHostToDevice, s));
+    upload_bytes(ctx, d_buf, buf.data(), sizeof(int) * buf.size());
+    upload_bytes(ctx, d_ct, ct.data(), sizeof(ChildTree) * ct.size());
     k_make_children_many<<<(int)((tot + 127) / 128), 128, 0, s>>>(d_ct, d_buf + tot, d_buf, (int)tot);
     MWB_CUDA(cudaGetLastError());
     count(ctx);
@@ -655,8 +673,7 @@ void trees_add_children(const std::vector<Tree*>& ts, const std::vector<std::vec
         t.n += 8 * ns;
         t.level_begin.push_back(t.n);
     }
-    MWB_CUDA(cudaStreamSynchronize(s));  // the host vectors and the staging buffers are released
-    dfree(ctx, d_buf);
+    dfree(ctx, d_buf);  // stream-ordered; the host vectors were staged by upload_bytes
     dfree(ctx, d_ct);
 }
 
@@ -691,14 +708,14 @@ void reduce_norms_many(const std::vector<Tree*>& ts, std::vector<double>& leaf2,
     if (n == 0) return;
     Ctx* ctx = ts[0]->mra->ctx;
     double* d = (double*)dalloc(ctx, sizeof(double) * 2 * n);
-    MWB_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * 2 * n, s));
-    for (int i = 0; i < n; ++i) {
-        if (ts[i]->n == 0) continue;
-        k_reduce_norm2<<<1, 1024, 0, s>>>(ts[i]->norm2, ts[i]->child0, 0, ts[i]->n, 1, 0, d + i);
-        k_reduce_norm2<<<1, 1024, 0, s>>>(ts[i]->norm2, ts[i]->child0, 0, ts[i]->n, 0, 1, d + n + i);
-        count(ctx, 2);
-    }
+    std::vector<NormSrc> src(n);
+    for (int i = 0; i < n; ++i) src[i] = NormSrc{ts[i]->norm2, ts[i]->child0, ts[i]->n};  // n = 0: zero sums
+    NormSrc* d_src = (NormSrc*)dalloc(ctx, sizeof(NormSrc) * n);
+    upload_bytes(ctx, d_src, src.data(), sizeof(NormSrc) * n);
+    k_reduce_norm2_many<<<2 * n, 1024, 0, s>>>(d_src, n, d);
     MWB_CUDA(cudaGetLastError());
+    count(ctx);
+    dfree(ctx, d_src);
     std::vector<double> h(2 * n);
     MWB_CUDA(cudaMemcpyAsync(h.data(), d, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, s));
     MWB_CUDA(cudaStreamSynchronize(s));
