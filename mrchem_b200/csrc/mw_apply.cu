@@ -305,7 +305,7 @@ __global__ void k_multi_slots(const int* __restrict__ nchunk, int nitems, int* n
 // at positions toff[c] ..; key = item << 32 | term << 20 | line rank (dz rank << 10 | dy rank),
 // value = candidate << 32 | term entry.  A stable sort by key then groups every output node's
 // triples by (term, dz, dy), in candidate order inside a line.
-__global__ void k_texpand(const int* __restrict__ cand_item, int ncand, const Item* __restrict__ items,
+__global__ void k_texpand(const int* __restrict__ offs, const int* __restrict__ cand_item, int ncand, const Item* __restrict__ items,
                           const BTree* __restrict__ trees, const int* __restrict__ cdelta,
                           const int* __restrict__ ntrip, const int* __restrict__ toff,
                           const int* __restrict__ csrc, unsigned long long* key, unsigned long long* val, int* err) {
@@ -320,10 +320,16 @@ __global__ void k_texpand(const int* __restrict__ cand_item, int ncand, const It
         atomicOr(err, 1);
         return;
     }
+    // written mirrored inside the item's range, so that after the stable sort a line's triples come in
+    // increasing order of their offset's bound (candidates are listed in decreasing order): the tensor
+    // core's FP32 accumulation of a line's x sums rounds toward zero when it adds products of a smaller
+    // scale to a larger sum, and adding the small contributions first loses fewer of their bits
+    const int T0 = toff[offs[w]], T1 = toff[offs[w + 1]];
     for (int j = 0; j < n; ++j) {
         const int te = de.t0 + j;
-        key[p0 + j] = ((unsigned long long)w << 32) | ((unsigned long long)T.terms[te].m << 20) | (unsigned)de.lrank;
-        val[p0 + j] = ((unsigned long long)c << 32) | (unsigned)te;
+        const int q = T0 + T1 - 1 - (p0 + j);
+        key[q] = ((unsigned long long)w << 32) | ((unsigned long long)T.terms[te].m << 20) | (unsigned)de.lrank;
+        val[q] = ((unsigned long long)c << 32) | (unsigned)te;
     }
 }
 // greedy cut of each node's sorted triples into chunks of about `limit` triples, at plane
@@ -1626,7 +1632,7 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         d_tkey = (unsigned long long*)dalloc(ctx, sizeof(unsigned long long) * tcap);
         d_tval = (unsigned long long*)dalloc(ctx, sizeof(unsigned long long) * tcap);
         if (ntri > 0) {
-            k_texpand<<<(ncand + 255) / 256, 256, 0, s>>>(d_cand_item, ncand, d_items, d_trees, d_cdelta, d_ntrip,
+            k_texpand<<<(ncand + 255) / 256, 256, 0, s>>>(d_offs, d_cand_item, ncand, d_items, d_trees, d_cdelta, d_ntrip,
                                                           d_toff, d_csrc, d_tkey_in, d_tval_in, d_terr);
             MWB_CUDA(cudaGetLastError());
             int hb = 1;

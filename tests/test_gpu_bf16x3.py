@@ -1,6 +1,7 @@
 """GPU tests of the BF16x3 contraction engine (flag MW_APPLY_BF16X3): the x mode product of every
-(output, input, term) triple on the tcgen05 tensor cores, with data rows and operator rows written as
-three BF16 slices of a per-row fixed-point form so that the tensor core sums them exactly, the y and z
+(output, input, term) triple on the tcgen05 tensor cores, with data rows written as four and operator
+rows as three BF16 slices of a per-row fixed-point form so that the tensor core sums each slice pair
+exactly, the y and z
 mode products as FP32 products on the CUDA cores, and every term's contribution accumulated in FP64.
 
 Bars: integer tree structure (node keys) identical to the FP64 apply and to the FP64 CPU oracle;
