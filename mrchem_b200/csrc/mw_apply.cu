@@ -129,6 +129,10 @@ __global__ void k_bcand(const Item* __restrict__ items, int nitems, const BTree*
             }
         }
         const unsigned bal = __ballot_sync(0xffffffffu, ok);
+        if (!fill) {  // the counting pass also counts the generated-node requests
+            const unsigned gb = __ballot_sync(0xffffffffu, ok && gk != kEmptyKey);
+            if (lane == 0 && gb) atomicAdd(ngreq, __popc(gb));
+        }
         if (fill && ok) {
             const int pos = base + kept + __popc(bal & ((1u << lane) - 1u));
             cdelta[pos] = e;
@@ -1521,10 +1525,17 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     MWB_CUDA(cudaMemsetAsync(d_ngreq, 0, sizeof(int), s));
     const int cblocks = (ni * 32 + 255) / 256;
     k_bcand<<<cblocks, 256, 0, s>>>(d_items, ni, d_trees, 0, d_count, nullptr, nullptr, nullptr, nullptr, nullptr,
-                                    nullptr);
+                                    d_ngreq);
     MWB_CUDA(cudaGetLastError());
     count(ctx);
-    const int ncand = scan_total(ctx, d_count, d_offs, ni);
+    scan_only(ctx, d_count, d_offs, ni);
+    int tot0[2] = {0, 0};  // candidates, generated-node requests: one read-back
+    MWB_CUDA(cudaMemcpyAsync(&tot0[0], d_offs + ni, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MWB_CUDA(cudaMemcpyAsync(&tot0[1], d_ngreq, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
+    const int ncand = tot0[0];
+    const int ngreq = tot0[1];
+    MWB_CUDA(cudaMemsetAsync(d_ngreq, 0, sizeof(int), s));  // the fill pass numbers the requests again
     const int ncap = std::max(1, ncand);
     int* d_cdelta = (int*)dalloc(ctx, sizeof(int) * ncap);
     int* d_csrc = (int*)dalloc(ctx, sizeof(int) * ncap);
@@ -1536,9 +1547,6 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         MWB_CUDA(cudaGetLastError());
         count(ctx);
     }
-    int ngreq = 0;
-    MWB_CUDA(cudaMemcpyAsync(&ngreq, d_ngreq, sizeof(int), cudaMemcpyDeviceToHost, s));
-    MWB_CUDA(cudaStreamSynchronize(s));
 
     // 2. generated nodes
     int nu = 0;
