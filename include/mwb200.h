@@ -37,8 +37,9 @@ enum { MW_FUNC_GAUSSIANS = 1, MW_FUNC_HYDROGEN_PRODUCTS = 2 };
  * pieces, operators in three; FP32 sums inside a term, compensated summation over terms; relative
  * error 2e-7 .. 1e-6, so it serves orders k <= 10 at prec >= 1e-6 (where its error is at most about
  * prec), and other requests take the FP32 path), or BF16x3: the x mode product of every
- * (output, input, term) triple on the tensor cores with data and operator rows as three BF16 slices of a
- * per-row fixed-point form (exact FP32 sums inside a triple; FP32-level error), the y and z mode
+ * (output, input, term) triple on the tensor cores with data rows as four and operator rows as three
+ * BF16 slices of a per-row fixed-point form (exact FP32 sums of each slice pair inside a triple;
+ * FP32-level error), the y and z mode
  * products as FP32 products on the CUDA cores and every term's contribution accumulated in FP64 (orders
  * k = 7 .. 10; other orders take the FP32 path); norms, screening and refinement are FP64 in all four */
 enum { MW_APPLY_FP64 = 0, MW_APPLY_FP32 = 1, MW_APPLY_TF32X3 = 2, MW_APPLY_BF16X3 = 3 };
@@ -46,7 +47,10 @@ enum { MW_APPLY_FP64 = 0, MW_APPLY_FP32 = 1, MW_APPLY_TF32X3 = 2, MW_APPLY_BF16X
 const char* mw_last_error(void);
 int mw_version(int* major, int* minor);
 
-/* Device context on CUDA device `device`; work is issued on `stream` (NULL = a private stream). */
+/* Device context on CUDA device `device`; work is issued on `stream` (NULL = a private stream).  A
+ * context (and every handle on it) is used by one host thread at a time: its calls share the stream,
+ * the memory pool's stream order and a pinned staging buffer for small uploads.  Threads that work
+ * concurrently use one context each. */
 int mw_ctx_create(int device, void* stream, mw_ctx* out);
 int mw_ctx_destroy(mw_ctx ctx);
 int mw_ctx_synchronize(mw_ctx ctx);

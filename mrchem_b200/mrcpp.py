@@ -39,7 +39,7 @@ FUNC_HYDROGEN_PRODUCTS = 2
 APPLY_FP64 = 0
 APPLY_FP32 = 1
 APPLY_TF32X3 = 2  # split-TF32 tensor cores (k <= 10, prec >= 1e-6; otherwise the FP32 engine)
-APPLY_BF16X3 = 3  # x step on the tensor cores (three BF16 slices per row), y/z FP32, FP64 sums (k = 7..10)
+APPLY_BF16X3 = 3  # x step on the tensor cores (BF16 slices: 4 per data row, 3 per operator row), y/z FP32, FP64 sums (k = 7..10)
 
 # every symbol include/mwb200.h declares: (name, restype, argtypes)
 SYMBOLS = [
