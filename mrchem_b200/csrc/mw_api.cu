@@ -31,11 +31,49 @@ void* dalloc(Ctx* ctx, size_t bytes) {
 void dfree(Ctx* ctx, void* p) {
     if (p) cudaFreeAsync(p, ctx->stream);
 }
+// copies of up to 8 byte ranges in one launch (grid-stride, 16- or 4-byte words where both ends allow)
+struct CopyList {
+    const unsigned char* src[8];
+    unsigned char* dst[8];
+    unsigned long long n[8];
+    int count;
+};
+__global__ void k_copy_list(CopyList L) {
+    const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x, nth = (size_t)gridDim.x * blockDim.x;
+    for (int r = 0; r < L.count; ++r) {
+        const unsigned char* src = L.src[r];
+        unsigned char* dst = L.dst[r];
+        const size_t n = L.n[r];
+        const uintptr_t al = reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst);
+        size_t done = 0;
+        if ((al & 15) == 0) {
+            const size_t nw = n >> 4;
+            for (size_t i = tid; i < nw; i += nth) reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
+            done = nw << 4;
+        } else if ((al & 3) == 0) {
+            const size_t nw = n >> 2;
+            for (size_t i = tid; i < nw; i += nth)
+                reinterpret_cast<uint32_t*>(dst)[i] = reinterpret_cast<const uint32_t*>(src)[i];
+            done = nw << 2;
+        }
+        for (size_t i = done + tid; i < n; i += nth) dst[i] = src[i];
+    }
+}
+static void launch_copies(Ctx* ctx, const CopyList& L) {
+    size_t mx = 0;
+    for (int r = 0; r < L.count; ++r) mx = std::max<size_t>(mx, L.n[r]);
+    const int blocks = (int)std::max<size_t>(1, std::min<size_t>(512, (mx / 16 + 255) / 256));
+    k_copy_list<<<blocks, 256, 0, ctx->stream>>>(L);
+    MWB_CUDA(cudaGetLastError());
+    ctx->launches += 1;
+}
+
 void upload_bytes(Ctx* ctx, void* dst, const void* src, size_t bytes) {
     if (bytes == 0) return;
     constexpr size_t kArena = 32u << 20;
     if (!ctx->pin && bytes <= kArena / 4) {
-        MWB_CUDA(cudaMallocHost(&ctx->pin, kArena));
+        MWB_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&ctx->pin), kArena, cudaHostAllocMapped));
+        MWB_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->pin_dev), ctx->pin, 0));
         MWB_CUDA(cudaEventCreateWithFlags(&ctx->pin_ev, cudaEventDisableTiming));
         ctx->pin_cap = kArena;
         ctx->pin_off = 0;
@@ -48,12 +86,78 @@ void upload_bytes(Ctx* ctx, void* dst, const void* src, size_t bytes) {
         if (ctx->pin_pending) MWB_CUDA(cudaEventSynchronize(ctx->pin_ev));
         ctx->pin_off = 0;
     }
-    char* h = ctx->pin + ctx->pin_off;
-    std::memcpy(h, src, bytes);
-    MWB_CUDA(cudaMemcpyAsync(dst, h, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    std::memcpy(ctx->pin + ctx->pin_off, src, bytes);
+    CopyList L{};
+    L.src[0] = reinterpret_cast<const unsigned char*>(ctx->pin_dev + ctx->pin_off);
+    L.dst[0] = reinterpret_cast<unsigned char*>(dst);
+    L.n[0] = bytes;
+    L.count = 1;
+    launch_copies(ctx, L);
     MWB_CUDA(cudaEventRecord(ctx->pin_ev, ctx->stream));
     ctx->pin_pending = true;
     ctx->pin_off += (bytes + 255) & ~(size_t)255;
+}
+
+void readback(Ctx* ctx, std::initializer_list<ReadReq> reqs) {
+    constexpr size_t kBox = 4u << 20;
+    if (!ctx->mbox) {
+        MWB_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&ctx->mbox), kBox, cudaHostAllocMapped));
+        MWB_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->mbox_dev), ctx->mbox, 0));
+        ctx->mbox_cap = kBox;
+    }
+    if (reqs.size() > 8) throw Error(MW_ERR_ARG, "readback: at most 8 ranges");
+    CopyList L{};
+    long long at[8];  // mailbox offset of each request, -1: empty or through the copy engine
+    size_t used = 0;
+    int i = 0;
+    for (const ReadReq& r : reqs) {
+        at[i] = -1;
+        const size_t o = (used + 15) & ~(size_t)15;
+        if (r.bytes > 0 && o + r.bytes <= ctx->mbox_cap) {
+            at[i] = (long long)o;
+            L.src[L.count] = reinterpret_cast<const unsigned char*>(r.src);
+            L.dst[L.count] = reinterpret_cast<unsigned char*>(ctx->mbox_dev + o);
+            L.n[L.count] = r.bytes;
+            ++L.count;
+            used = o + r.bytes;
+        }
+        ++i;
+    }
+    if (L.count > 0) launch_copies(ctx, L);
+    i = 0;
+    for (const ReadReq& r : reqs) {  // what does not fit the mailbox (pageable: completes in the call)
+        if (r.bytes > 0 && at[i] < 0) MWB_CUDA(cudaMemcpyAsync(r.dst, r.src, r.bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        ++i;
+    }
+    MWB_CUDA(cudaStreamSynchronize(ctx->stream));
+    i = 0;
+    for (const ReadReq& r : reqs) {
+        if (at[i] >= 0) std::memcpy(r.dst, ctx->mbox + at[i], r.bytes);
+        ++i;
+    }
+}
+
+void upload_bytes(Ctx* ctx, cudaStream_t s, void* dst, const void* src, size_t bytes) {
+    if (s == ctx->stream) upload_bytes(ctx, dst, src, bytes);
+    else if (bytes > 0) MWB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+}
+void device_copy(Ctx* ctx, void* dst, const void* src, size_t bytes) {
+    if (bytes == 0) return;
+    CopyList L{};
+    L.src[0] = reinterpret_cast<const unsigned char*>(src);
+    L.dst[0] = reinterpret_cast<unsigned char*>(dst);
+    L.n[0] = bytes;
+    L.count = 1;
+    launch_copies(ctx, L);
+}
+void readback(Ctx* ctx, cudaStream_t s, std::initializer_list<ReadReq> reqs) {
+    if (s == ctx->stream) {
+        readback(ctx, reqs);
+        return;
+    }
+    for (const ReadReq& r : reqs)
+        if (r.bytes > 0) MWB_CUDA(cudaMemcpyAsync(r.dst, r.src, r.bytes, cudaMemcpyDeviceToHost, s));
+    MWB_CUDA(cudaStreamSynchronize(s));
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -90,7 +194,7 @@ void tree_reserve(Tree& t, int need) {
         auto grow = [&](auto*& p, size_t elem) {
             using T = std::remove_reference_t<decltype(*p)>;
             T* q = (T*)dalloc(ctx, elem * ncap);
-            if (p && t.n > 0) MWB_CUDA(cudaMemcpyAsync(q, p, elem * t.n, cudaMemcpyDeviceToDevice, s));
+            if (p && t.n > 0) device_copy(ctx, q, p, elem * t.n);  // on s (= the context's stream)
             dfree(ctx, p);
             p = q;
         };
@@ -1063,6 +1167,7 @@ static void ctx_free(mwb::Ctx* ctx) {
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->pin_ev) cudaEventDestroy(ctx->pin_ev);
     if (ctx->pin) cudaFreeHost(ctx->pin);
+    if (ctx->mbox) cudaFreeHost(ctx->mbox);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete static_cast<mw_ctx_s*>(ctx);
 }

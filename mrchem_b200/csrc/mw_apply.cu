@@ -1405,8 +1405,7 @@ static int scan_total(Ctx* ctx, const int* d_in, int* d_out, int n) {
     MWB_CUDA(cub::DeviceScan::ExclusiveSum(d_tmp, tmp, d_in, d_out, n + 1, ctx->stream));
     dfree(ctx, d_tmp);
     int total = 0;
-    MWB_CUDA(cudaMemcpyAsync(&total, d_out + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    MWB_CUDA(cudaStreamSynchronize(ctx->stream));
+    readback(ctx, {{&total, d_out + n, sizeof(int)}});
     return total;
 }
 
@@ -1530,9 +1529,7 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     count(ctx);
     scan_only(ctx, d_count, d_offs, ni);
     int tot0[2] = {0, 0};  // candidates, generated-node requests: one read-back
-    MWB_CUDA(cudaMemcpyAsync(&tot0[0], d_offs + ni, sizeof(int), cudaMemcpyDeviceToHost, s));
-    MWB_CUDA(cudaMemcpyAsync(&tot0[1], d_ngreq, sizeof(int), cudaMemcpyDeviceToHost, s));
-    MWB_CUDA(cudaStreamSynchronize(s));
+    readback(ctx, {{&tot0[0], d_offs + ni, sizeof(int)}, {&tot0[1], d_ngreq, sizeof(int)}});
     const int ncand = tot0[0];
     const int ngreq = tot0[1];
     MWB_CUDA(cudaMemsetAsync(d_ngreq, 0, sizeof(int), s));  // the fill pass numbers the requests again
@@ -1661,10 +1658,8 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         scan_only(ctx, d_nchunk, d_choff, ni);
         scan_only(ctx, d_nslot, d_slotoff, ni);
         int tot[3] = {0, 0, 0};  // chunks, partial slots, the expansion's error word: one read-back
-        MWB_CUDA(cudaMemcpyAsync(&tot[0], d_choff + ni, sizeof(int), cudaMemcpyDeviceToHost, s));
-        MWB_CUDA(cudaMemcpyAsync(&tot[1], d_slotoff + ni, sizeof(int), cudaMemcpyDeviceToHost, s));
-        MWB_CUDA(cudaMemcpyAsync(&tot[2], d_terr, sizeof(int), cudaMemcpyDeviceToHost, s));
-        MWB_CUDA(cudaStreamSynchronize(s));
+        readback(ctx, {{&tot[0], d_choff + ni, sizeof(int)}, {&tot[1], d_slotoff + ni, sizeof(int)},
+                       {&tot[2], d_terr, sizeof(int)}});
         if (tot[2] != 0) throw Error(-3, "input tree nodes are not in level order");
         nchunks = tot[0];
         nslots = tot[1];
@@ -1708,9 +1703,7 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         scan_only(ctx, d_nchunk, d_choff, ni);
         scan_only(ctx, d_nslot, d_slotoff, ni);
         int tot[2] = {0, 0};
-        MWB_CUDA(cudaMemcpyAsync(&tot[0], d_choff + ni, sizeof(int), cudaMemcpyDeviceToHost, s));
-        MWB_CUDA(cudaMemcpyAsync(&tot[1], d_slotoff + ni, sizeof(int), cudaMemcpyDeviceToHost, s));
-        MWB_CUDA(cudaStreamSynchronize(s));
+        readback(ctx, {{&tot[0], d_choff + ni, sizeof(int)}, {&tot[1], d_slotoff + ni, sizeof(int)}});
         nchunks = tot[0];
         nslots = tot[1];
         d_chunks = (Chunk*)dalloc(ctx, sizeof(Chunk) * std::max(1, nchunks));
@@ -1799,10 +1792,8 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     unsigned long long ntot[2] = {0, 0};
     std::vector<int> sflags(ni);
     std::vector<double> g(any_root ? nt : 0);
-    MWB_CUDA(cudaMemcpyAsync(ntot, d_ntrip_tot, sizeof(ntot), cudaMemcpyDeviceToHost, s));
-    MWB_CUDA(cudaMemcpyAsync(sflags.data(), d_sflags, sizeof(int) * ni, cudaMemcpyDeviceToHost, s));
-    if (any_root) MWB_CUDA(cudaMemcpyAsync(g.data(), d_g, sizeof(double) * nt, cudaMemcpyDeviceToHost, s));
-    MWB_CUDA(cudaStreamSynchronize(s));
+    readback(ctx, {{ntot, d_ntrip_tot, sizeof(ntot)}, {sflags.data(), d_sflags, sizeof(int) * ni},
+                   {g.data(), d_g, any_root ? sizeof(double) * nt : 0}});
     if ((ntot[1] & 0xffffffffull) != 0)
         throw Error(-2, "tensor-core contraction: an MMA or copy completion wait exceeded its time limit");
     if (ctx->prof) {

@@ -1,5 +1,6 @@
 // mw_internal.hpp -- host-side objects behind the C-ABI handles (include/mwb200.h).
 #pragma once
+#include <initializer_list>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -50,12 +51,19 @@ struct Ctx {
     // handles that point here (worlds, networks); a destroyed context is freed with the last of them
     int refs = 0;
     bool closed = false;
-    // pinned staging arena for small host-to-device uploads (copies from pageable memory may drain the
-    // stream first); a region is reused only after the event recorded behind the latest copy completed
-    char* pin = nullptr;
+    // small host<->device transfers of the passes go through mapped pinned host memory and are moved by
+    // copy kernels, not by the DMA copy engines: the engines may be busy with large tree transfers of
+    // other contexts (a caller streaming batches), and a small copy queued behind them would wait.
+    // Uploads: a staging arena, a region reused only after the event recorded behind the latest copy
+    // kernel that read it completed.  Read-backs: a mailbox written by a copy kernel before the sync.
+    char* pin = nullptr;      // host address
+    char* pin_dev = nullptr;  // its device address
     size_t pin_cap = 0, pin_off = 0;
     cudaEvent_t pin_ev = nullptr;
     bool pin_pending = false;
+    char* mbox = nullptr;
+    char* mbox_dev = nullptr;
+    size_t mbox_cap = 0;
 };
 
 struct Mra {
@@ -163,5 +171,21 @@ void dfree(Ctx* ctx, void* p);
 // stream-ordered copy of `bytes` host bytes to device memory `dst` through the context's pinned arena
 // (pageable copy when the arena cannot hold them); the host buffer may be reused when this returns
 void upload_bytes(Ctx* ctx, void* dst, const void* src, size_t bytes);
+// the same on stream s: through the arena when s is the context's stream, else a pageable copy on s
+void upload_bytes(Ctx* ctx, cudaStream_t s, void* dst, const void* src, size_t bytes);
+// device-to-device copy on the context's stream by a copy kernel (the DMA engines may be queued with
+// large host transfers of other contexts)
+void device_copy(Ctx* ctx, void* dst, const void* src, size_t bytes);
+// synchronous read-back of several device ranges into host memory: one copy kernel into the mapped
+// mailbox, a stream synchronisation, then host copies (a range that does not fit the mailbox goes
+// through the copy engine)
+struct ReadReq {
+    void* dst;        // host
+    const void* src;  // device
+    size_t bytes;
+};
+void readback(Ctx* ctx, std::initializer_list<ReadReq> reqs);
+// the same on stream s: through the mailbox when s is the context's stream, else copy-engine copies on s
+void readback(Ctx* ctx, cudaStream_t s, std::initializer_list<ReadReq> reqs);
 
 }  // namespace mwb

@@ -717,8 +717,7 @@ void reduce_norms_many(const std::vector<Tree*>& ts, std::vector<double>& leaf2,
     count(ctx);
     dfree(ctx, d_src);
     std::vector<double> h(2 * n);
-    MWB_CUDA(cudaMemcpyAsync(h.data(), d, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, s));
-    MWB_CUDA(cudaStreamSynchronize(s));
+    readback(ctx, {{h.data(), d, sizeof(double) * 2 * n}});  // on the context's stream (= s)
     dfree(ctx, d);
     for (int i = 0; i < n; ++i) {
         leaf2[i] = h[i];

@@ -301,8 +301,7 @@ std::vector<float> mlp_logits(Mlp& M, const float* d_X, int N, cudaStream_t s) {
     std::vector<float*> acts;
     mlp_forward(M, d_X, N, acts, s);
     std::vector<float> z(N);
-    MWB_CUDA(cudaMemcpyAsync(z.data(), acts.back(), sizeof(float) * N, cudaMemcpyDeviceToHost, s));
-    MWB_CUDA(cudaStreamSynchronize(s));
+    readback(M.ctx, s, {{z.data(), acts.back(), sizeof(float) * N}});
     free_acts(M, acts);
     return z;
 }
@@ -338,11 +337,11 @@ float* features(Ctx* ctx, std::vector<FeatCtx>& fc, const std::vector<int2>& ite
     }
     FeatTree* d_ft = (FeatTree*)dalloc(ctx, sizeof(FeatTree) * ft.size());
     int2* d_items = (int2*)dalloc(ctx, sizeof(int2) * n);
-    MWB_CUDA(cudaMemcpyAsync(d_ft, ft.data(), sizeof(FeatTree) * ft.size(), cudaMemcpyHostToDevice, s));
-    MWB_CUDA(cudaMemcpyAsync(d_items, items.data(), sizeof(int2) * n, cudaMemcpyHostToDevice, s));
+    upload_bytes(ctx, s, d_ft, ft.data(), sizeof(FeatTree) * ft.size());  // staged: ft / items may go
+    upload_bytes(ctx, s, d_items, items.data(), sizeof(int2) * n);
     k_features<<<(n + 127) / 128, 128, 0, s>>>(d_items, n, d_ft, d_F);
     MWB_CUDA(cudaGetLastError());
-    MWB_CUDA(cudaStreamSynchronize(s));  // ft / items leave scope
+    if (s != ctx->stream) MWB_CUDA(cudaStreamSynchronize(s));  // pageable copies: ft / items leave scope
     dfree(ctx, d_ft);
     dfree(ctx, d_items);
     return d_F;
@@ -581,6 +580,7 @@ struct RTree {  // old arrays, new arrays and hash index of one tree being rebui
     long long off;   // first global index of the tree's old nodes
     long long noff;  // first position of the tree's kept nodes in the sorted list
     int nn;
+    int cap;  // capacity of the new arrays
 };
 
 __global__ void k_gather_keys(const uint64_t* __restrict__ k, const long long* __restrict__ g, int n, uint64_t* out) {
@@ -662,22 +662,18 @@ std::vector<Miss> verify_trees(const std::vector<Tree*>& ts, const std::vector<s
     for (;;) {
         int* d_n = (int*)dalloc(ctx, sizeof(int));
         Miss* d_m = (Miss*)dalloc(ctx, sizeof(Miss) * cap);
-        MWB_CUDA(cudaMemcpyAsync(d_vt, vt.data(), sizeof(VTree) * nt, cudaMemcpyHostToDevice, s));
-        MWB_CUDA(cudaMemcpyAsync(d_th, th.data(), sizeof(double) * th.size(), cudaMemcpyHostToDevice, s));
+        upload_bytes(ctx, s, d_vt, vt.data(), sizeof(VTree) * nt);
+        upload_bytes(ctx, s, d_th, th.data(), sizeof(double) * th.size());
         MWB_CUDA(cudaMemsetAsync(d_n, 0, sizeof(int), s));
         if (maxn > 0) {
             k_verify<<<dim3((maxn + 255) / 256, nt), 256, 0, s>>>(d_vt, d_th, depth_limit, d_keep, d_n, d_m, cap);
             MWB_CUDA(cudaGetLastError());
         }
         int nm = 0;
-        MWB_CUDA(cudaMemcpyAsync(&nm, d_n, sizeof(int), cudaMemcpyDeviceToHost, s));
-        MWB_CUDA(cudaStreamSynchronize(s));
+        readback(ctx, s, {{&nm, d_n, sizeof(int)}});
         if (nm <= cap) {
             out.resize(nm);
-            if (nm > 0) {
-                MWB_CUDA(cudaMemcpyAsync(out.data(), d_m, sizeof(Miss) * nm, cudaMemcpyDeviceToHost, s));
-                MWB_CUDA(cudaStreamSynchronize(s));
-            }
+            if (nm > 0) readback(ctx, s, {{out.data(), d_m, sizeof(Miss) * nm}});
             dfree(ctx, d_n);
             dfree(ctx, d_m);
             break;
@@ -706,7 +702,7 @@ long long trees_rebuild_device(const std::vector<Tree*>& ts, const unsigned char
     uint64_t* d_k = (uint64_t*)dalloc(ctx, sizeof(uint64_t) * N);
     for (int i = 0; i < nt; ++i)
         if (ts[i]->n > 0)
-            MWB_CUDA(cudaMemcpyAsync(d_k + offs[i], ts[i]->key, sizeof(uint64_t) * ts[i]->n, cudaMemcpyDeviceToDevice, s));
+            device_copy(ctx, d_k + offs[i], ts[i]->key, sizeof(uint64_t) * ts[i]->n);  // on s (= the context's stream)
     // kept global indices, ascending (grouped by tree)
     long long* d_g = (long long*)dalloc(ctx, sizeof(long long) * N);
     int* d_nsel = (int*)dalloc(ctx, sizeof(int));
@@ -719,8 +715,7 @@ long long trees_rebuild_device(const std::vector<Tree*>& ts, const unsigned char
         dfree(ctx, d_tmp);
     }
     int n = 0;
-    MWB_CUDA(cudaMemcpyAsync(&n, d_nsel, sizeof(int), cudaMemcpyDeviceToHost, s));
-    MWB_CUDA(cudaStreamSynchronize(s));
+    readback(ctx, s, {{&n, d_nsel, sizeof(int)}});
     // sort the kept nodes by key, then stably by tree: grouped by tree, key order inside a tree
     uint64_t* d_kk = (uint64_t*)dalloc(ctx, sizeof(uint64_t) * std::max(1, n));
     uint64_t* d_kk2 = (uint64_t*)dalloc(ctx, sizeof(uint64_t) * std::max(1, n));
@@ -729,7 +724,7 @@ long long trees_rebuild_device(const std::vector<Tree*>& ts, const unsigned char
     unsigned* d_tid2 = (unsigned*)dalloc(ctx, sizeof(unsigned) * std::max(1, n));
     long long* d_offs = (long long*)dalloc(ctx, sizeof(long long) * (nt + 1));
     int* d_cnt = (int*)dalloc(ctx, sizeof(int) * nt);
-    MWB_CUDA(cudaMemcpyAsync(d_offs, offs.data(), sizeof(long long) * (nt + 1), cudaMemcpyHostToDevice, s));
+    upload_bytes(ctx, s, d_offs, offs.data(), sizeof(long long) * (nt + 1));
     MWB_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(int) * nt, s));
     k_gather_keys<<<(n + 255) / 256, 256, 0, s>>>(d_k, d_g, n, d_kk);
     {
@@ -751,8 +746,7 @@ long long trees_rebuild_device(const std::vector<Tree*>& ts, const unsigned char
     }
     MWB_CUDA(cudaGetLastError());
     std::vector<int> cnt(nt);
-    MWB_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int) * nt, cudaMemcpyDeviceToHost, s));
-    MWB_CUDA(cudaStreamSynchronize(s));
+    readback(ctx, s, {{cnt.data(), d_cnt, sizeof(int) * nt}});
     // new arrays, gather, swap
     std::vector<RTree> rt(nt);
     long long noff = 0;
@@ -764,12 +758,15 @@ long long trees_rebuild_device(const std::vector<Tree*>& ts, const unsigned char
         R.ocoef = t.coef;
         R.on2 = t.norm2;
         R.ow2 = t.wnorm2;
-        R.nkey = (uint64_t*)dalloc(ctx, sizeof(uint64_t) * std::max(1, nn));
-        R.ncoef = (double*)dalloc(ctx, sizeof(double) * BS * std::max(1, nn));
-        R.nn2 = (double*)dalloc(ctx, sizeof(double) * std::max(1, nn));
-        R.nw2 = (double*)dalloc(ctx, sizeof(double) * std::max(1, nn));
-        R.nparent = (int*)dalloc(ctx, sizeof(int) * std::max(1, nn));
-        R.nchild0 = (int*)dalloc(ctx, sizeof(int) * std::max(1, nn));
+        // room beyond the kept nodes: the next apply into this tree (proposals overshoot) grows it in place
+        const int capn = nn + nn / 4 + 64;
+        R.cap = capn;
+        R.nkey = (uint64_t*)dalloc(ctx, sizeof(uint64_t) * capn);
+        R.ncoef = (double*)dalloc(ctx, sizeof(double) * BS * capn);
+        R.nn2 = (double*)dalloc(ctx, sizeof(double) * capn);
+        R.nw2 = (double*)dalloc(ctx, sizeof(double) * capn);
+        R.nparent = (int*)dalloc(ctx, sizeof(int) * capn);
+        R.nchild0 = (int*)dalloc(ctx, sizeof(int) * capn);
         R.hkey = t.hkey;
         R.hval = t.hval;
         R.hcap = t.hcap;
@@ -779,7 +776,7 @@ long long trees_rebuild_device(const std::vector<Tree*>& ts, const unsigned char
         noff += nn;
     }
     RTree* d_rt = (RTree*)dalloc(ctx, sizeof(RTree) * nt);
-    MWB_CUDA(cudaMemcpyAsync(d_rt, rt.data(), sizeof(RTree) * nt, cudaMemcpyHostToDevice, s));
+    upload_bytes(ctx, s, d_rt, rt.data(), sizeof(RTree) * nt);
     if (n > 0) k_rebuild_gather<<<n, 256, 0, s>>>(d_g, d_tid2, n, d_rt, BS);
     MWB_CUDA(cudaGetLastError());
     for (int i = 0; i < nt; ++i) {
@@ -798,7 +795,7 @@ long long trees_rebuild_device(const std::vector<Tree*>& ts, const unsigned char
         t.parent = R.nparent;
         t.child0 = R.nchild0;
         t.n = R.nn;
-        t.cap = std::max(1, R.nn);
+        t.cap = R.cap;
         launch_hash_reset(t, s);
         launch_hash_insert(t, 0, t.n, s);
     }
@@ -808,8 +805,7 @@ long long trees_rebuild_device(const std::vector<Tree*>& ts, const unsigned char
     if (n > 0) k_rebuild_links<<<(n + 255) / 256, 256, 0, s>>>(d_tid2, n, d_rt, d_lb);
     MWB_CUDA(cudaGetLastError());
     std::vector<int> lb((size_t)nt * (kMaxLevels + 1));
-    MWB_CUDA(cudaMemcpyAsync(lb.data(), d_lb, sizeof(int) * lb.size(), cudaMemcpyDeviceToHost, s));
-    MWB_CUDA(cudaStreamSynchronize(s));
+    readback(ctx, s, {{lb.data(), d_lb, sizeof(int) * lb.size()}});
     for (int i = 0; i < nt; ++i) {
         Tree& t = *ts[i];
         const int* L = lb.data() + (size_t)i * (kMaxLevels + 1);
