@@ -1541,13 +1541,19 @@ int mw_tree_assign(mw_tree dst, mw_tree src) {
         dst->n = 0;
         tree_reserve(*dst, src->n);
         const size_t n = (size_t)src->n, BS = a.bsize();
-        if (n > 0) {
-            MWB_CUDA(cudaMemcpyAsync(dst->key, src->key, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, s));
-            MWB_CUDA(cudaMemcpyAsync(dst->parent, src->parent, sizeof(int) * n, cudaMemcpyDeviceToDevice, s));
-            MWB_CUDA(cudaMemcpyAsync(dst->child0, src->child0, sizeof(int) * n, cudaMemcpyDeviceToDevice, s));
-            MWB_CUDA(cudaMemcpyAsync(dst->coef, src->coef, sizeof(double) * BS * n, cudaMemcpyDeviceToDevice, s));
-            MWB_CUDA(cudaMemcpyAsync(dst->norm2, src->norm2, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-            MWB_CUDA(cudaMemcpyAsync(dst->wnorm2, src->wnorm2, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        if (n > 0) {  // one copy kernel on dst's stream (the DMA engines may be busy with host transfers)
+            mwb::CopyList L{};
+            const void* from[6] = {src->key, src->parent, src->child0, src->coef, src->norm2, src->wnorm2};
+            void* to[6] = {dst->key, dst->parent, dst->child0, dst->coef, dst->norm2, dst->wnorm2};
+            const size_t bytes[6] = {sizeof(uint64_t) * n, sizeof(int) * n, sizeof(int) * n, sizeof(double) * BS * n,
+                                     sizeof(double) * n, sizeof(double) * n};
+            for (int q = 0; q < 6; ++q) {
+                L.src[q] = reinterpret_cast<const unsigned char*>(from[q]);
+                L.dst[q] = reinterpret_cast<unsigned char*>(to[q]);
+                L.n[q] = bytes[q];
+            }
+            L.count = 6;
+            mwb::launch_copies(a.ctx, L);
         }
         dst->n = src->n;
         dst->level_begin = src->level_begin;
