@@ -796,8 +796,8 @@ static void apply_batched(double prec, int n, Tree** out, Op** op, Tree** inp, i
         std::vector<Tree*> ins(inp, inp + n);
         std::vector<double> l2, m2;
         reduce_norms_many(ins, l2, m2, s);
+        trees_make_roots(std::vector<Tree*>(out, out + n));
         for (int i = 0; i < n; ++i) {
-            tree_make_roots(*out[i]);
             fnorm[i] = std::sqrt(l2[i]);
             nu_max[i] = std::sqrt(m2[i]);
         }
@@ -935,8 +935,8 @@ static void apply_learned(double prec, int n, Tree** out, Op** op, Tree** inp, i
         std::vector<Tree*> ins(inp, inp + n);
         std::vector<double> l2, m2;
         reduce_norms_many(ins, l2, m2, s);
+        trees_make_roots(std::vector<Tree*>(out, out + n));
         for (int i = 0; i < n; ++i) {
-            tree_make_roots(*out[i]);
             fnorm[i] = std::sqrt(l2[i]);
             nu_max[i] = std::sqrt(m2[i]);
             ents.push_back(Entry{i, 0, 0, out[i]->n});

@@ -7,6 +7,7 @@
 // conflicts; each thread owns whole pencils, which makes every 1-D transform safe in place.
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <cstdio>
 
 #include "mw_device.cuh"
@@ -804,6 +805,74 @@ void launch_gather_blocks(const double* src, const int* perm, int n, size_t bs, 
 
 // host copies of the key helpers for the driver
 uint64_t host_make_key(int depth, long long tx, long long ty, long long tz) { return make_key(depth, tx, ty, tz); }
+
+// the root level of several trees on one world, in two launches: each tree's hash index cleared
+// (blockIdx.y = tree), then node i = root key i (Morton order) with no parent, no children and zero
+// norms, entered into the index
+struct RootTree {
+    uint64_t* key;
+    int* parent;
+    int* child0;
+    double* norm2;
+    double* wnorm2;
+    uint64_t* hkey;
+    int* hval;
+    uint32_t hcap;
+};
+__global__ void k_hash_reset_many(const RootTree* __restrict__ ts) {
+    const RootTree T = ts[blockIdx.y];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < T.hcap; i += gridDim.x * blockDim.x) {
+        T.hkey[i] = kEmptyKey;
+        T.hval[i] = -1;
+    }
+}
+__global__ void k_roots_many(const RootTree* __restrict__ ts, const uint64_t* __restrict__ rk, int nroot) {
+    const RootTree T = ts[blockIdx.y];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nroot) return;
+    T.key[i] = rk[i];
+    T.parent[i] = -1;
+    T.child0[i] = -1;
+    T.norm2[i] = 0.0;
+    T.wnorm2[i] = 0.0;
+    hash_insert_one(T.hkey, T.hval, T.hcap, rk[i], i);
+}
+void trees_make_roots(const std::vector<Tree*>& ts) {
+    if (ts.empty()) return;
+    const Mra& m = *ts[0]->mra;
+    Ctx* ctx = m.ctx;
+    cudaStream_t s = ctx->stream;
+    std::vector<uint64_t> keys;
+    for (int z = 0; z < m.boxes[2]; ++z)
+        for (int y = 0; y < m.boxes[1]; ++y)
+            for (int x = 0; x < m.boxes[0]; ++x) keys.push_back(host_make_key(0, x, y, z));
+    std::sort(keys.begin(), keys.end());
+    const int nroot = (int)keys.size();
+    std::vector<RootTree> rt;
+    uint32_t maxcap = 0;
+    for (Tree* t : ts) {
+        t->n = 0;
+        t->level_begin.clear();
+        tree_reserve(*t, nroot);
+        rt.push_back(RootTree{t->key, t->parent, t->child0, t->norm2, t->wnorm2, t->hkey, t->hval, t->hcap});
+        maxcap = std::max(maxcap, t->hcap);
+    }
+    uint64_t* d_rk = (uint64_t*)dalloc(ctx, sizeof(uint64_t) * nroot);
+    RootTree* d_rt = (RootTree*)dalloc(ctx, sizeof(RootTree) * rt.size());
+    upload_bytes(ctx, d_rk, keys.data(), sizeof(uint64_t) * nroot);
+    upload_bytes(ctx, d_rt, rt.data(), sizeof(RootTree) * rt.size());
+    const unsigned nt = (unsigned)rt.size();
+    k_hash_reset_many<<<dim3(std::min<uint32_t>((maxcap + 255) / 256, 1024), nt), 256, 0, s>>>(d_rt);
+    k_roots_many<<<dim3((nroot + 255) / 256, nt), 256, 0, s>>>(d_rt, d_rk, nroot);
+    MWB_CUDA(cudaGetLastError());
+    count(ctx, 2);
+    dfree(ctx, d_rk);
+    dfree(ctx, d_rt);
+    for (Tree* t : ts) {
+        t->n = nroot;
+        t->level_begin = {0, nroot};
+    }
+}
 void host_key_trans(uint64_t k, long long t[3]) { key_trans(k, t); }
 
 }  // namespace mwb
