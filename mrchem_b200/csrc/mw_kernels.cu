@@ -837,6 +837,39 @@ __global__ void k_roots_many(const RootTree* __restrict__ ts, const uint64_t* __
     T.wnorm2[i] = 0.0;
     hash_insert_one(T.hkey, T.hval, T.hcap, rk[i], i);
 }
+// every node of several trees into their (cleared) hash indices: blockIdx.y = tree
+__global__ void k_hash_insert_many(const RootTree* __restrict__ ts, const int* __restrict__ n) {
+    const RootTree T = ts[blockIdx.y];
+    const int nn = n[blockIdx.y];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x)
+        hash_insert_one(T.hkey, T.hval, T.hcap, T.key[i], i);
+}
+void trees_rehash(const std::vector<Tree*>& ts) {
+    if (ts.empty()) return;
+    Ctx* ctx = ts[0]->mra->ctx;
+    cudaStream_t s = ctx->stream;
+    std::vector<RootTree> rt;
+    std::vector<int> n;
+    uint32_t maxcap = 0;
+    int maxn = 0;
+    for (Tree* t : ts) {
+        rt.push_back(RootTree{t->key, t->parent, t->child0, t->norm2, t->wnorm2, t->hkey, t->hval, t->hcap});
+        n.push_back(t->n);
+        maxcap = std::max(maxcap, t->hcap);
+        maxn = std::max(maxn, t->n);
+    }
+    RootTree* d_rt = (RootTree*)dalloc(ctx, sizeof(RootTree) * rt.size());
+    int* d_n = (int*)dalloc(ctx, sizeof(int) * n.size());
+    upload_bytes(ctx, d_rt, rt.data(), sizeof(RootTree) * rt.size());
+    upload_bytes(ctx, d_n, n.data(), sizeof(int) * n.size());
+    const unsigned nt = (unsigned)rt.size();
+    k_hash_reset_many<<<dim3(std::min<uint32_t>((maxcap + 255) / 256, 1024), nt), 256, 0, s>>>(d_rt);
+    if (maxn > 0) k_hash_insert_many<<<dim3(std::min((maxn + 255) / 256, 1024), nt), 256, 0, s>>>(d_rt, d_n);
+    MWB_CUDA(cudaGetLastError());
+    count(ctx, maxn > 0 ? 2 : 1);
+    dfree(ctx, d_rt);
+    dfree(ctx, d_n);
+}
 void trees_make_roots(const std::vector<Tree*>& ts) {
     if (ts.empty()) return;
     const Mra& m = *ts[0]->mra;

@@ -66,6 +66,8 @@ void tree_reserve(Tree& t, int need);
 void tree_make_roots(Tree& t);
 // the root level of several trees of one world at once (two launches for the batch)
 void trees_make_roots(const std::vector<Tree*>& ts);
+// rebuild the hash indices of several trees of one context from their node keys (two launches)
+void trees_rehash(const std::vector<Tree*>& ts);
 void tree_compress_bottom_up(Tree& t);
 // split the nodes of the last level whose wavelet norm exceeds thr; returns the number of new nodes
 int tree_refine_last_level(Tree& t, double thr);

@@ -796,9 +796,12 @@ long long trees_rebuild_device(const std::vector<Tree*>& ts, const unsigned char
         t.child0 = R.nchild0;
         t.n = R.nn;
         t.cap = R.cap;
-        launch_hash_reset(t, s);
-        launch_hash_insert(t, 0, t.n, s);
+        if (s != ctx->stream) {
+            launch_hash_reset(t, s);
+            launch_hash_insert(t, 0, t.n, s);
+        }
     }
+    if (s == ctx->stream) trees_rehash(ts);  // all the rebuilt indices in two launches
     // links and level starts from the rebuilt hash indices
     int* d_lb = (int*)dalloc(ctx, sizeof(int) * (size_t)nt * (kMaxLevels + 1));
     MWB_CUDA(cudaMemsetAsync(d_lb, 0xff, sizeof(int) * (size_t)nt * (kMaxLevels + 1), s));
