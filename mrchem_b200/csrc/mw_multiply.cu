@@ -53,7 +53,7 @@ struct MulItem {
     int node;
 };
 
-constexpr int kMulThreads = 256;
+constexpr int kMulThreads = 416;  // 13 warps: one pencil of a (2k)^3 block per thread at k = 10
 
 template <int K>
 struct MulCfg {
