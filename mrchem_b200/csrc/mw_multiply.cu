@@ -327,6 +327,21 @@ void build_grid(Tree& out, Tree& inp) {
     tree_add_keys(out, add, s);
 }
 
+// split flags of the last levels of several trees in one launch: item q = (tree, node)
+struct SplitTree {
+    const double* wnorm2;
+    const uint64_t* key;
+    double thr;
+};
+__global__ void k_split_flags_many(const int2* __restrict__ items, int n, const SplitTree* __restrict__ ts,
+                                   int depth_limit, int* flags) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int2 it = items[q];
+    const SplitTree T = ts[it.x];
+    flags[q] = (key_depth(T.key[it.y]) < depth_limit && sqrt(T.wnorm2[it.y]) > T.thr) ? 1 : 0;
+}
+
 // Refinement passes shared by the product and the linear combination: every pass computes the work
 // nodes of all output trees with one launch (`launch(items, d_items)`), then, unless prec <= 0 or the
 // pass limit is reached, splits the computed nodes whose wavelet norm exceeds prec ||out|| 2^{-depth/2}
@@ -365,23 +380,66 @@ void refine_passes(double prec, int n, Tree** out, int max_iter, LaunchF&& launc
         std::vector<double> leaf2, max2;
         reduce_norms_many(ts, leaf2, max2, s);
         bool any = false;
+        // trees whose work is the whole last level (always so when a tree grows from the roots): split
+        // flags of all of them in one launch and one read-back, children appended as the next level
+        std::vector<int> full;
         for (int i = 0; i < n; ++i) {
-            Tree& o = *out[i];
+            const Tree& o = *out[i];
             if (work[i].empty()) continue;
-            // work = the whole last level (always so when the tree grows from the roots): split on
-            // the device, children appended as the next level
             const int L = o.levels();
             const int lb = o.level_begin[L - 1], le = o.level_begin[L];
-            if ((int)work[i].size() == le - lb && work[i].front() == lb && work[i].back() == le - 1) {
-                const int added = tree_refine_last_level(o, mul_split_threshold(prec, std::sqrt(leaf2[i]), L - 1));
-                work[i].clear();
-                if (added > 0) {
-                    any = true;
-                    for (int q = le; q < le + added; ++q) work[i].push_back(q);
-                    keys[i].clear();  // host keys are refreshed when the general path needs them
-                }
-                continue;
+            if ((int)work[i].size() == le - lb && work[i].front() == lb && work[i].back() == le - 1) full.push_back(i);
+        }
+        if (!full.empty()) {
+            std::vector<int2> its;
+            std::vector<SplitTree> st(n, SplitTree{nullptr, nullptr, 0.0});
+            for (int i : full) {
+                Tree& o = *out[i];
+                const int L = o.levels();
+                st[i] = SplitTree{o.wnorm2, o.key, mul_split_threshold(prec, std::sqrt(leaf2[i]), L - 1)};
+                for (int q = o.level_begin[L - 1]; q < o.level_begin[L]; ++q) its.push_back(int2{i, q});
             }
+            const int ni = (int)its.size();
+            int2* d_its = (int2*)dalloc(ctx, sizeof(int2) * ni);
+            SplitTree* d_st = (SplitTree*)dalloc(ctx, sizeof(SplitTree) * n);
+            int* d_flags = (int*)dalloc(ctx, sizeof(int) * ni);
+            upload_bytes(ctx, s, d_its, its.data(), sizeof(int2) * ni);
+            upload_bytes(ctx, s, d_st, st.data(), sizeof(SplitTree) * n);
+            k_split_flags_many<<<(ni + 255) / 256, 256, 0, s>>>(d_its, ni, d_st, m->depth_limit, d_flags);
+            MWB_CUDA(cudaGetLastError());
+            ctx->launches++;
+            std::vector<int> flags(ni);
+            readback(ctx, s, {{flags.data(), d_flags, sizeof(int) * ni}});
+            dfree(ctx, d_its);
+            dfree(ctx, d_st);
+            dfree(ctx, d_flags);
+            std::vector<Tree*> grow;
+            std::vector<std::vector<int>> lists;
+            std::vector<int> gi;
+            size_t q = 0;
+            for (int i : full) {  // items are grouped by tree in `full` order
+                std::vector<int> l;
+                for (; q < its.size() && its[q].x == i; ++q)
+                    if (flags[q]) l.push_back(its[q].y);
+                work[i].clear();
+                if (l.empty()) continue;
+                grow.push_back(out[i]);
+                lists.push_back(std::move(l));
+                gi.push_back(i);
+            }
+            std::vector<int> before(gi.size());
+            for (size_t g = 0; g < gi.size(); ++g) before[g] = out[gi[g]]->n;
+            trees_add_children(grow, lists, s);
+            for (size_t g = 0; g < gi.size(); ++g) {
+                const int i = gi[g];
+                any = true;
+                for (int v = before[g]; v < out[i]->n; ++v) work[i].push_back(v);
+                keys[i].clear();  // host keys are refreshed when the general path needs them
+            }
+        }
+        for (int i = 0; i < n; ++i) {
+            Tree& o = *out[i];
+            if (work[i].empty() || std::find(full.begin(), full.end(), i) != full.end()) continue;
             if (keys[i].size() != (size_t)o.n) keys[i] = host_keys(o, s);
             std::vector<double> w2(o.n);
             MWB_CUDA(cudaMemcpyAsync(w2.data(), o.wnorm2, sizeof(double) * o.n, cudaMemcpyDeviceToHost, s));
