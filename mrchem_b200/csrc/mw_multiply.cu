@@ -354,8 +354,15 @@ void refine_passes(double prec, int n, Tree** out, int max_iter, LaunchF&& launc
     // work: the current leaves of every output tree (roots for an empty tree)
     std::vector<std::vector<int>> work(n);
     std::vector<std::vector<uint64_t>> keys(n);
+    std::vector<Tree*> empty;
+    for (int i = 0; i < n; ++i)
+        if (out[i]->n == 0) empty.push_back(out[i]);
+    trees_make_roots(empty);  // all empty trees at once; their work is every root (host keys on demand)
     for (int i = 0; i < n; ++i) {
-        if (out[i]->n == 0) tree_make_roots(*out[i]);
+        if (std::find(empty.begin(), empty.end(), out[i]) != empty.end()) {
+            for (int q = 0; q < out[i]->n; ++q) work[i].push_back(q);
+            continue;
+        }
         std::vector<int> c0(out[i]->n);
         MWB_CUDA(cudaMemcpyAsync(c0.data(), out[i]->child0, sizeof(int) * out[i]->n, cudaMemcpyDeviceToHost, s));
         MWB_CUDA(cudaStreamSynchronize(s));
@@ -369,11 +376,10 @@ void refine_passes(double prec, int n, Tree** out, int max_iter, LaunchF&& launc
             for (int q : work[i]) items.push_back({i, q});
         if (items.empty()) break;
         MulItem* d_items = (MulItem*)dalloc(ctx, sizeof(MulItem) * items.size());
-        MWB_CUDA(cudaMemcpyAsync(d_items, items.data(), sizeof(MulItem) * items.size(), cudaMemcpyHostToDevice, s));
+        upload_bytes(ctx, s, d_items, items.data(), sizeof(MulItem) * items.size());
         launch(items, d_items);
         MWB_CUDA(cudaGetLastError());
         ctx->launches++;
-        MWB_CUDA(cudaStreamSynchronize(s));  // the item list leaves scope
         dfree(ctx, d_items);
         if (prec <= 0.0 || (max_iter >= 0 && iter >= max_iter)) break;
         std::vector<Tree*> ts(out, out + n);
