@@ -394,7 +394,7 @@ def run_gpu(args):
         out_bufs.append({"depth": pinned((cap,), torch.int32), "parent": pinned((cap,), torch.int32),
                          "child0": pinned((cap,), torch.int32), "trans": pinned((3 * cap,), torch.int64),
                          "coef": pinned((cap * bs_k,), torch.float64)})
-    n_e2e = min(16, max(8, args.steps))  # a stream of batches: pipeline fill and drain amortised over 8+ steps
+    n_e2e = 16  # a stream of 16 batches: the pipeline's fill and drain amortised
     h2d = sum(sum(v.nbytes for v in h.values()) for h in host)
     node_bytes = 4 + 24 + 4 + 4 + 8 * bs_k
     nb = nloc
@@ -750,10 +750,11 @@ def run_exchange(args):
 def run_density_sweep(args):
     """Poisson potential of a 20-atom density (4 normalised Gaussians per atom, exponents
     log-U[0.3, 1e3], atoms in a 12 Bohr box) at interpolating orders 7/9/11 and precisions
-    1e-5/1e-6/1e-7: FP64, mixed (FP32 products, FP64 accumulation) and split-TF32 tensor-core applies
-    on the GPU, each timed over --steps steps after --warmup, with the relative errors of the mixed and
-    tensor-core potentials against FP64 (coefficient differences) and the CPU restatement's time for
-    one apply at order 7, prec 1e-5.  (At order 11, k = 12, the tensor-core flag runs the FP32 engine.)"""
+    1e-5/1e-6/1e-7: FP64, mixed (FP32 products, FP64 accumulation) and BF16x3 tensor-core applies (with
+    --tf32x3 also split-TF32) on the GPU, each timed over --steps steps after --warmup, with the relative
+    errors of the mixed and tensor-core potentials against FP64 (coefficient differences) and the CPU
+    restatement's time for one apply at order 7, prec 1e-5.  (At order 11, k = 12, the BF16x3 flag runs
+    the FP32 engine.)"""
     import torch
 
     world, rank, local = dist_env()

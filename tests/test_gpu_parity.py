@@ -304,6 +304,36 @@ def test_exchange_pair_against_oracle(gpu_mod, oracle_mod, flags):
         assert G.distance(pot, back) / np.sqrt(back.square_norm()) <= 2e-7
 
 
+def test_config4_density_against_oracle(gpu_mod, oracle_mod):
+    """The Poisson potential of the 20-atom density (4 normalised Gaussians per atom, exponents
+    log-U[0.3, 1e3]; CoulombPotential.cpp:85) at order 7, prec 1e-5, on the 10^3-root world: FP64,
+    FP32 and BF16x3 against the oracle's FP64 apply of the same input tree -- identical node keys for
+    every engine; FP64 coefficients to 1e-10 of the largest, the mixed engines' relative error below
+    prec / 10 (measured 1e-8 FP32, 4e-8 BF16x3 against the GPU FP64 potential)."""
+    from mrchem_b200 import workloads as W
+
+    G, O = gpu_mod, oracle_mod
+    prec = 1e-5
+    world = (W.WORLD["min_scale"], W.WORLD["corner"], W.WORLD["boxes"])
+    mg, mo = pair(G, O, 7, max_depth=15, world=world)
+    rho = G.FunctionTree(mg)
+    G.project(prec, rho, W.density_20_atoms())
+    pot_o = O.FunctionTree(mo)
+    O.apply(prec, pot_o, O.PoissonOperator(mo, prec), to_oracle(O, mo, rho))
+    eo = pot_o.export()
+    back = G.FunctionTree(mg)
+    back.load(eo["depth"], eo["trans"], eo["parent"], eo["child0"], eo["coef"])
+    P = G.PoissonOperator(mg, prec)
+    for flags in (G.APPLY_FP64, G.APPLY_FP32, G.APPLY_BF16X3):
+        pot = G.FunctionTree(mg)
+        G.apply(prec, pot, P, rho, flags)
+        eg = pot.export()
+        if flags == G.APPLY_FP64:
+            assert_same_tree(eg, eo)
+        else:
+            assert set(keyed(eg)) == set(keyed(eo)), flags
+            assert G.distance(pot, back) / np.sqrt(back.square_norm()) <= prec / 10, flags
+
 def test_upload_download_roundtrip(gpu_mod, oracle_mod):
     G, O = gpu_mod, oracle_mod
     mg, mo = pair(G, O, 7)
