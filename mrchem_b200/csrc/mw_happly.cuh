@@ -360,7 +360,6 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
             // its first TILES_GEN tiles and first K step, but the first triple of a line clears every tile;
             // below the root also the s->s block's sums (x', x < k; first TILES_GEN tiles)
             constexpr uint32_t idesc = umma_idesc_bf16(128, C::NCOL);
-            constexpr uint32_t idesc2 = umma_idesc_bf16(128, C::NBQ);
             auto issue = [&](int b, bool first, bool gen) {
                 const uint32_t base = sbase + (uint32_t)(b * C::BUF);
                 const uint64_t da = umma_sdesc(base, R * 16, 128);
@@ -370,15 +369,21 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
                     constexpr int tl = decltype(TL)::value;
                     const bool live = !gen || tl < C::TILES_GEN;
                     // below the root the first tiles also take the s->s block's sums (N = NCOL + NCOL2)
-                    const uint32_t id = (!root && tl < C::TILES_GEN) ? idesc2 : idesc;
+                    const bool ss = !root && tl < C::TILES_GEN;
                     static_for<4>([&](auto SQ) {  // x = 0 .. 15 of data slice sq against its operand
                         constexpr int sq = decltype(SQ)::value;
                         constexpr int oq = sq < 3 ? sq : 2;  // slice 3 takes slice 2's operand
+                        // operand rows (output columns) below oq W are zero for this slice: the MMA starts
+                        // at the 16-row boundary below them, fewer B bytes for the same sums
+                        constexpr int r0 = oq * C::W / 16 * 16;
+                        static_assert(r0 <= oq * C::W && (C::NCOL - r0) % 16 == 0 && C::NCOL - r0 >= 16, "MMA N");
+                        constexpr uint32_t id_full = umma_idesc_bf16(128, C::NCOL - r0);
+                        constexpr uint32_t id_ss = umma_idesc_bf16(128, C::NBQ - r0);
                         const bool init = first && sq == 0;
                         if (!live && !init) return;
                         const uint64_t ad = da + (uint64_t)((sq * C::NCHM * R * 16 + tl * 2048) >> 4);
-                        const uint64_t bd = dbq + (uint64_t)((oq * C::OPB_Q) >> 4);
-                        umma_bf16(tbase + (uint32_t)C::tcol(tl), ad, bd, id, init ? 0u : 1u);
+                        const uint64_t bd = dbq + (uint64_t)((oq * C::OPB_Q + r0 * 16) >> 4);
+                        umma_bf16(tbase + (uint32_t)(C::tcol(tl) + r0), ad, bd, ss ? id_ss : id_full, init ? 0u : 1u);
                     });
                     if constexpr (C::PACK) {  // x = 16 .. K2-1 of all slices in one step (whole matrix only)
                         if (!gen) {
