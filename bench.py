@@ -394,7 +394,7 @@ def run_gpu(args):
         out_bufs.append({"depth": pinned((cap,), torch.int32), "parent": pinned((cap,), torch.int32),
                          "child0": pinned((cap,), torch.int32), "trans": pinned((3 * cap,), torch.int64),
                          "coef": pinned((cap * bs_k,), torch.float64)})
-    n_e2e = 16  # a stream of 16 batches: the pipeline's fill and drain amortised
+    n_e2e = 32  # a stream of 32 batches: the pipeline's fill and drain (about 1.5 steps) amortised
     h2d = sum(sum(v.nbytes for v in h.values()) for h in host)
     node_bytes = 4 + 24 + 4 + 4 + 8 * bs_k
     nb = nloc
@@ -427,10 +427,8 @@ def run_gpu(args):
     c_in = [G.FunctionTree(m) for _ in range(nb)]
     c_out = [G.FunctionTree(m) for _ in range(nb)]
 
-    def upload(q):
-        for i in range(nb):
-            h = host[i]
-            stage_in[q][i].load(h["depth"], h["trans"], h["parent"], h["child0"], h["coef"])
+    def upload(q):  # the whole batch in one call: its copies stream back to back
+        G.load_many(stage_in[q], host)
 
     def compute(q):
         for i in range(nb):
@@ -442,10 +440,7 @@ def run_gpu(args):
             stage_out[q][i].assign(c_out[i])
 
     def download(q):
-        d = 0
-        for i in range(nb):
-            d += stage_out[q][i].export_into(out_bufs[i]) * node_bytes
-        return d
+        return sum(G.export_many_into(stage_out[q], out_bufs)) * node_bytes
 
     # untimed pass through every stage (staging trees grow to size)
     for q in (0, 1):
@@ -573,10 +568,11 @@ def run_gpu(args):
                        "l2": f"inputs larger than L2 ({in_bytes / 1e9:.2f} GB of input blocks per step)"},
             "e2e": {"value": e2e_val, "unit": "applies/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "host_memory": "pinned, allocated once",
-                    "path": "per step: mw_tree_upload x32 (upload thread, own context), mw_tree_assign x32 (device "
-                            "copy into the compute context), mw_apply_learned, mw_tree_assign x32 (device copy out), "
-                            "mw_tree_download x32 (download thread, own context); double-buffered staging trees, "
-                            "so a step's transfers overlap the previous and next steps' compute",
+                    "path": "per step: mw_tree_upload_many of the 32 trees (upload thread, own context), "
+                            "mw_tree_assign x32 (device copy into the compute context), mw_apply_learned, "
+                            "mw_tree_assign x32 (device copy out), mw_tree_download_many of the 32 trees (download "
+                            "thread, own context); double-buffered staging trees, so a step's transfers overlap "
+                            "the previous and next steps' compute",
                     "steps": n_e2e,
                     "outputs_equal_headline": bool(e2e_same)},
             "plain_fp64": {"value": job_applies * args.steps / (ms64 / 1e3), "unit": "applies/s",

@@ -97,6 +97,18 @@ int mw_tree_upload(mw_tree tree, int n, const int* depth, const long long* trans
                    const int* child0, const double* coef);
 /* copy the device tree to host buffers sized with mw_tree_nnodes (any pointer may be NULL) */
 int mw_tree_download(mw_tree tree, int* depth, long long* trans, int* parent, int* child0, double* coef);
+/* Batched transfers of ntrees distinct trees (arrays of per-tree pointers; n[i] nodes for tree i): the
+ * same checks, node order and results as mw_tree_upload / mw_tree_download for every tree, with the
+ * copies of all trees queued back to back and one synchronisation per call, so that the copy engine
+ * streams a whole batch from or to pinned host buffers without idling between trees.  The upload checks
+ * every tree before it queues any copy.  The download's trans[i] (3 n_i words) also receives the keys
+ * before they are expanded in place; entries of depth/trans/parent/child0/coef may be NULL as in
+ * mw_tree_download.  No reference counterpart (MRCPP keeps its trees in host memory). */
+int mw_tree_upload_many(int ntrees, mw_tree* trees, const int* n, const int* const* depth,
+                        const long long* const* trans, const int* const* parent, const int* const* child0,
+                        const double* const* coef);
+int mw_tree_download_many(int ntrees, mw_tree* trees, int* const* depth, long long* const* trans,
+                          int* const* parent, int* const* child0, double* const* coef);
 /* dst = a deep copy of src (structure, coefficients, norms), device to device.  The two trees may
  * belong to different contexts (streams) of the same device, on worlds with the same parameters: a
  * thread that streams trees to or from the host on its own context hands them to the context that

@@ -1204,6 +1204,109 @@ static void mra_release(mwb::Mra* m) {
 #define MW_ARG(cond, msg) \
     if (!(cond)) throw mwb::Error(MW_ERR_ARG, msg)
 
+// Host half of a tree upload: checks, (depth, Morton) order (parents before children, siblings in child
+// order), parent / child indices relinked to that order, level starts.
+struct HostTree {
+    int n = 0;
+    bool sorted = true;
+    std::vector<uint64_t> key;  // in (depth, Morton) order
+    std::vector<int> parent, child0, ord, lb;
+};
+static void upload_prepare(const Mra& m, int n, const int* depth, const long long* trans, const int* parent,
+                           const int* child0, HostTree& h) {
+    std::vector<uint64_t> key(n);
+    int maxd = 0;
+    for (int i = 0; i < n; ++i) {
+        MW_ARG(depth[i] >= 0 && depth[i] <= m.depth_limit, "node depth out of range");
+        for (int d = 0; d < 3; ++d)
+            MW_ARG(trans[3 * i + d] >= 0 && trans[3 * i + d] < ((long long)m.boxes[d] << depth[i]),
+                   "node translation outside the world");
+        key[i] = host_make_key(depth[i], trans[3 * i], trans[3 * i + 1], trans[3 * i + 2]);
+        maxd = std::max(maxd, depth[i]);
+    }
+    // nodes already in (depth, Morton) order -- every tree this library exports -- are copied straight from
+    // the caller's buffers (pinned buffers: one DMA each); otherwise the blocks are reordered on the device
+    h.n = n;
+    h.sorted = std::is_sorted(key.begin(), key.end());
+    h.ord.resize(n);
+    std::iota(h.ord.begin(), h.ord.end(), 0);
+    if (!h.sorted) std::sort(h.ord.begin(), h.ord.end(), [&](int a, int b) { return key[a] < key[b]; });
+    std::vector<int> pos(n);
+    for (int i = 0; i < n; ++i) pos[h.ord[i]] = i;
+    const int nroot = (int)((long long)m.boxes[0] * m.boxes[1] * m.boxes[2]);
+    h.key.resize(n);
+    h.parent.resize(n);
+    h.child0.resize(n);
+    h.lb.assign(maxd + 2, 0);
+    int roots = 0;
+    for (int i = 0; i < n; ++i) {
+        const int o = h.ord[i];
+        MW_ARG(parent[o] >= -1 && parent[o] < n && child0[o] >= -1 && child0[o] < n, "bad parent/child index");
+        h.key[i] = key[o];
+        h.parent[i] = parent[o] < 0 ? -1 : pos[parent[o]];
+        h.child0[i] = child0[o] < 0 ? -1 : pos[child0[o]];
+        if (depth[o] == 0) ++roots;
+        h.lb[depth[o] + 1]++;
+    }
+    MW_ARG(roots == nroot, "tree must contain every root box");
+    for (int i = 0; i < n; ++i) {
+        if (h.child0[i] < 0) continue;
+        const int o = h.ord[i];
+        for (int c = 0; c < 8; ++c) {
+            const int ch = child0[o] + c;
+            MW_ARG(ch < n && pos[ch] == h.child0[i] + c && parent[ch] == o, "children must be 8 consecutive nodes");
+        }
+    }
+    for (int d = 1; d < (int)h.lb.size(); ++d) h.lb[d] += h.lb[d - 1];
+}
+// Device half, in three steps on the tree's stream (nothing waits): the node arrays (through the pinned
+// arena when `staged`, else direct copies that complete within the call), the coefficient blocks, then the
+// hash index and norms.  upload_enqueue with a non-null coef runs all three.
+static void upload_enqueue_coef(Tree& t, const HostTree& h, const double* coef) {
+    Ctx* ctx = t.mra->ctx;
+    cudaStream_t s = ctx->stream;
+    const size_t BS = t.mra->bsize(), n = (size_t)h.n;
+    if (h.sorted) {
+        MWB_CUDA(cudaMemcpyAsync(t.coef, coef, sizeof(double) * BS * n, cudaMemcpyHostToDevice, s));
+    } else {
+        double* stage = (double*)dalloc(ctx, sizeof(double) * BS * n);
+        MWB_CUDA(cudaMemcpyAsync(stage, coef, sizeof(double) * BS * n, cudaMemcpyHostToDevice, s));
+        int* d_ord = (int*)dalloc(ctx, sizeof(int) * n);
+        upload_bytes(ctx, d_ord, h.ord.data(), sizeof(int) * n);
+        launch_gather_blocks(stage, d_ord, h.n, BS, t.coef, s);
+        dfree(ctx, stage);
+        dfree(ctx, d_ord);
+    }
+}
+static void upload_enqueue_index(Tree& t, const HostTree& h) {
+    cudaStream_t s = t.mra->ctx->stream;
+    t.n = h.n;
+    t.level_begin = h.lb;
+    launch_hash_reset(t, s);
+    launch_hash_insert(t, 0, h.n, s);
+    launch_node_norms(t, 0, h.n, s);
+}
+static void upload_enqueue(Tree& t, const HostTree& h, const double* coef, bool staged) {
+    Ctx* ctx = t.mra->ctx;
+    cudaStream_t s = ctx->stream;
+    const size_t n = (size_t)h.n;
+    t.n = 0;
+    tree_reserve(t, h.n);
+    if (staged) {
+        upload_bytes(ctx, t.key, h.key.data(), sizeof(uint64_t) * n);
+        upload_bytes(ctx, t.parent, h.parent.data(), sizeof(int) * n);
+        upload_bytes(ctx, t.child0, h.child0.data(), sizeof(int) * n);
+    } else {
+        MWB_CUDA(cudaMemcpyAsync(t.key, h.key.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(t.parent, h.parent.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+        MWB_CUDA(cudaMemcpyAsync(t.child0, h.child0.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    }
+    if (coef) {
+        upload_enqueue_coef(t, h, coef);
+        upload_enqueue_index(t, h);
+    }
+}
+
 extern "C" {
 
 const char* mw_last_error(void) { return g_err.c_str(); }
@@ -1454,74 +1557,37 @@ int mw_tree_upload(mw_tree t, int n, const int* depth, const long long* trans, c
         MW_ARG(n > 0, "empty tree");
         const Mra& m = *t->mra;
         MWB_CUDA(cudaSetDevice(m.ctx->device));
-        cudaStream_t s = m.ctx->stream;
-        // validate and order by (depth, Morton): parents before children, siblings in child order
-        std::vector<uint64_t> key(n);
-        int maxd = 0;
-        for (int i = 0; i < n; ++i) {
-            MW_ARG(depth[i] >= 0 && depth[i] <= m.depth_limit, "node depth out of range");
-            for (int d = 0; d < 3; ++d)
-                MW_ARG(trans[3 * i + d] >= 0 && trans[3 * i + d] < ((long long)m.boxes[d] << depth[i]),
-                       "node translation outside the world");
-            key[i] = host_make_key(depth[i], trans[3 * i], trans[3 * i + 1], trans[3 * i + 2]);
-            maxd = std::max(maxd, depth[i]);
+        HostTree h;
+        upload_prepare(m, n, depth, trans, parent, child0, h);
+        upload_enqueue(*t, h, coef, false);
+        MWB_CUDA(cudaStreamSynchronize(m.ctx->stream));
+    })
+}
+
+int mw_tree_upload_many(int ntrees, mw_tree* trees, const int* n, const int* const* depth, const long long* const* trans,
+                        const int* const* parent, const int* const* child0, const double* const* coef) {
+    MW_TRY({
+        MW_ARG(ntrees >= 0 && (ntrees == 0 || (trees && n && depth && trans && parent && child0 && coef)),
+               "null pointer");
+        std::vector<HostTree> h(ntrees);
+        std::vector<cudaStream_t> streams;
+        for (int i = 0; i < ntrees; ++i) {  // every check before any copy is queued
+            MW_ARG(trees[i] && depth[i] && trans[i] && parent[i] && child0[i] && coef[i], "null pointer");
+            MW_ARG(n[i] > 0, "empty tree");
+            for (int j = 0; j < i; ++j) MW_ARG(trees[j] != trees[i], "a tree appears twice in the batch");
+            MW_ARG(trees[i]->mra->ctx->device == trees[0]->mra->ctx->device, "trees on different devices");
+            upload_prepare(*trees[i]->mra, n[i], depth[i], trans[i], parent[i], child0[i], h[i]);
+            const cudaStream_t s = trees[i]->mra->ctx->stream;
+            if (std::find(streams.begin(), streams.end(), s) == streams.end()) streams.push_back(s);
         }
-        // nodes already in (depth, Morton) order -- every tree this library exports -- are copied
-        // straight from the caller's buffers (pinned buffers: one DMA each); otherwise the blocks are
-        // copied as given and reordered on the device
-        const bool sorted = std::is_sorted(key.begin(), key.end());
-        std::vector<int> ord(n);
-        std::iota(ord.begin(), ord.end(), 0);
-        if (!sorted) std::sort(ord.begin(), ord.end(), [&](int a, int b) { return key[a] < key[b]; });
-        std::vector<int> pos(n);
-        for (int i = 0; i < n; ++i) pos[ord[i]] = i;
-        int nroot = (int)((long long)m.boxes[0] * m.boxes[1] * m.boxes[2]);
-        std::vector<uint64_t> k2(n);
-        std::vector<int> p2(n), c2(n);
-        std::vector<int> lb(maxd + 2, 0);
-        int roots = 0;
-        for (int i = 0; i < n; ++i) {
-            const int o = ord[i];
-            MW_ARG(parent[o] >= -1 && parent[o] < n && child0[o] >= -1 && child0[o] < n, "bad parent/child index");
-            k2[i] = key[o];
-            p2[i] = parent[o] < 0 ? -1 : pos[parent[o]];
-            c2[i] = child0[o] < 0 ? -1 : pos[child0[o]];
-            if (depth[o] == 0) ++roots;
-            lb[depth[o] + 1]++;
-        }
-        MW_ARG(roots == nroot, "tree must contain every root box");
-        for (int i = 0; i < n; ++i) {
-            if (c2[i] < 0) continue;
-            const int o = ord[i];
-            for (int c = 0; c < 8; ++c) {
-                const int ch = child0[o] + c;
-                MW_ARG(ch < n && pos[ch] == c2[i] + c && parent[ch] == o, "children must be 8 consecutive nodes");
-            }
-        }
-        for (int d = 1; d < (int)lb.size(); ++d) lb[d] += lb[d - 1];
-        t->n = 0;
-        tree_reserve(*t, n);
-        const size_t BS = m.bsize();
-        MWB_CUDA(cudaMemcpyAsync(t->key, k2.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s));
-        MWB_CUDA(cudaMemcpyAsync(t->parent, p2.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
-        MWB_CUDA(cudaMemcpyAsync(t->child0, c2.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
-        if (sorted) {
-            MWB_CUDA(cudaMemcpyAsync(t->coef, coef, sizeof(double) * BS * n, cudaMemcpyHostToDevice, s));
-        } else {
-            double* stage = (double*)dalloc(m.ctx, sizeof(double) * BS * n);
-            int* d_ord = (int*)dalloc(m.ctx, sizeof(int) * n);
-            MWB_CUDA(cudaMemcpyAsync(stage, coef, sizeof(double) * BS * n, cudaMemcpyHostToDevice, s));
-            MWB_CUDA(cudaMemcpyAsync(d_ord, ord.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
-            launch_gather_blocks(stage, d_ord, n, BS, t->coef, s);
-            dfree(m.ctx, stage);
-            dfree(m.ctx, d_ord);
-        }
-        t->n = n;
-        t->level_begin = lb;
-        launch_hash_reset(*t, s);
-        launch_hash_insert(*t, 0, n, s);
-        launch_node_norms(*t, 0, n, s);
-        MWB_CUDA(cudaStreamSynchronize(s));
+        if (ntrees == 0) return MW_OK;
+        MWB_CUDA(cudaSetDevice(trees[0]->mra->ctx->device));
+        // node arrays first (small copies from the pinned arena), then the coefficient blocks of all trees back
+        // to back, then the hash indices and norms: the copy engine streams the batch without gaps
+        for (int i = 0; i < ntrees; ++i) upload_enqueue(*trees[i], h[i], nullptr, true);
+        for (int i = 0; i < ntrees; ++i) upload_enqueue_coef(*trees[i], h[i], coef[i]);
+        for (int i = 0; i < ntrees; ++i) upload_enqueue_index(*trees[i], h[i]);
+        for (cudaStream_t s : streams) MWB_CUDA(cudaStreamSynchronize(s));
     })
 }
 
@@ -1586,6 +1652,61 @@ int mw_tree_download(mw_tree t, int* depth, long long* trans, int* parent, int* 
             if (depth) depth[i] = (int)(key[i] >> 59);
             if (trans)
                 for (int d = 0; d < 3; ++d) trans[3 * i + d] = tr[d];
+        }
+    })
+}
+
+int mw_tree_download_many(int ntrees, mw_tree* trees, int* const* depth, long long* const* trans, int* const* parent,
+                          int* const* child0, double* const* coef) {
+    MW_TRY({
+        MW_ARG(ntrees >= 0 && (ntrees == 0 || (trees && depth && trans && parent && child0 && coef)), "null pointer");
+        std::vector<cudaStream_t> streams;
+        for (int i = 0; i < ntrees; ++i) {
+            MW_ARG(trees[i], "null tree");
+            MW_ARG(trees[i]->mra->ctx->device == trees[0]->mra->ctx->device, "trees on different devices");
+            for (int j = 0; j < i; ++j) MW_ARG(trees[j] != trees[i], "a tree appears twice in the batch");
+            const cudaStream_t s = trees[i]->mra->ctx->stream;
+            if (std::find(streams.begin(), streams.end(), s) == streams.end()) streams.push_back(s);
+        }
+        if (ntrees == 0) return MW_OK;
+        MWB_CUDA(cudaSetDevice(trees[0]->mra->ctx->device));
+        // keys land in the caller's trans buffer (n 8-byte words of its 3n) and are expanded in place once
+        // the copies are done; without a trans buffer in a host vector
+        std::vector<std::vector<uint64_t>> spare(ntrees);
+        for (int i = 0; i < ntrees; ++i) {
+            Tree& t = *trees[i];
+            const int nn = t.n;
+            if (nn == 0) continue;
+            cudaStream_t s = t.mra->ctx->stream;
+            void* kdst = trans[i];
+            if (!kdst) {
+                spare[i].resize(nn);
+                kdst = spare[i].data();
+            }
+            MWB_CUDA(cudaMemcpyAsync(kdst, t.key, sizeof(uint64_t) * nn, cudaMemcpyDeviceToHost, s));
+            if (parent[i]) MWB_CUDA(cudaMemcpyAsync(parent[i], t.parent, sizeof(int) * nn, cudaMemcpyDeviceToHost, s));
+            if (child0[i]) MWB_CUDA(cudaMemcpyAsync(child0[i], t.child0, sizeof(int) * nn, cudaMemcpyDeviceToHost, s));
+        }
+        for (int i = 0; i < ntrees; ++i) {  // the blocks of all trees back to back
+            Tree& t = *trees[i];
+            if (t.n > 0 && coef[i])
+                MWB_CUDA(cudaMemcpyAsync(coef[i], t.coef, sizeof(double) * t.n * t.mra->bsize(), cudaMemcpyDeviceToHost,
+                                         t.mra->ctx->stream));
+        }
+        for (cudaStream_t s : streams) MWB_CUDA(cudaStreamSynchronize(s));
+        for (int i = 0; i < ntrees; ++i) {
+            const int nn = trees[i]->n;
+            const unsigned char* kb =
+                trans[i] ? reinterpret_cast<const unsigned char*>(trans[i]) : reinterpret_cast<const unsigned char*>(spare[i].data());
+            for (int q = nn - 1; q >= 0; --q) {  // trans[3q ..] lies at or above key q: read before written
+                uint64_t k;
+                std::memcpy(&k, kb + sizeof(uint64_t) * q, sizeof(k));
+                long long tr[3];
+                host_key_trans(k, tr);
+                if (depth[i]) depth[i][q] = (int)(k >> 59);
+                if (trans[i])
+                    for (int d = 0; d < 3; ++d) trans[i][3 * q + d] = tr[d];
+            }
         }
     })
 }

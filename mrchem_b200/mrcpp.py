@@ -67,6 +67,8 @@ SYMBOLS = [
     ("mw_tree_square_norm", ctypes.c_int, [_vp, _dp]),
     ("mw_tree_upload", ctypes.c_int, [_vp, ctypes.c_int, _ip, _lp, _ip, _ip, _dp]),
     ("mw_tree_download", ctypes.c_int, [_vp, _ip, _lp, _ip, _ip, _dp]),
+    ("mw_tree_upload_many", ctypes.c_int, [ctypes.c_int, _vpp, _ip, _vpp, _vpp, _vpp, _vpp, _vpp]),
+    ("mw_tree_download_many", ctypes.c_int, [ctypes.c_int, _vpp, _vpp, _vpp, _vpp, _vpp, _vpp]),
     ("mw_tree_device_arrays", ctypes.c_int, [_vp, _vpp, _vpp, _vpp]),
     ("mw_tree_rescale", ctypes.c_int, [_vp, ctypes.c_double]),
     ("mw_tree_serialized_size", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_ulonglong)]),
@@ -328,6 +330,45 @@ class FunctionTree:
         c, k, n = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
         _check(_lib.mw_tree_device_arrays(self._h, ctypes.byref(c), ctypes.byref(k), ctypes.byref(n)))
         return c.value, k.value, n.value
+
+
+def _ptrs(arrays):
+    return (ctypes.c_void_p * max(1, len(arrays)))(*[None if a is None else a.ctypes.data for a in arrays])
+
+
+def load_many(trees, arrays):
+    """Upload a batch of host trees in one call (mw_tree_upload_many): ``arrays[i]`` is a dict with the
+    arguments of ``FunctionTree.load`` ('depth', 'trans', 'parent', 'child0', 'coef') for ``trees[i]``.
+    Same checks and results as one ``load`` per tree; the copies of all trees are queued back to back."""
+    if len(trees) != len(arrays):
+        raise MWError("load_many: one array set per tree")
+    conv = {"depth": np.int32, "trans": np.int64, "parent": np.int32, "child0": np.int32, "coef": np.float64}
+    keep = [{k: np.ascontiguousarray(a[k], dt) for k, dt in conv.items()} for a in arrays]
+    n = np.array([len(a["depth"]) for a in keep], np.int32)
+    _check(_lib.mw_tree_upload_many(len(trees), (ctypes.c_void_p * max(1, len(trees)))(*[t._h for t in trees]),
+                                    n.ctypes.data_as(_ip), *[_ptrs([a[k] for a in keep]) for k in conv]))
+
+
+def export_many_into(trees, bufs):
+    """Download a batch of trees in one call (mw_tree_download_many) into caller-owned arrays: ``bufs[i]``
+    is a dict as for ``FunctionTree.export_into``.  Returns the node counts."""
+    if len(trees) != len(bufs):
+        raise MWError("export_many_into: one buffer set per tree")
+    names = {"depth": np.int32, "trans": np.int64, "parent": np.int32, "child0": np.int32, "coef": np.float64}
+    counts = []
+    for t, b in zip(trees, bufs):
+        n = t.nnodes()
+        k = t.mra.k
+        size = {"depth": n, "trans": 3 * n, "parent": n, "child0": n, "coef": n * (2 * k) ** 3}
+        for name, dt in names.items():
+            a = b[name]
+            if a.dtype != dt or not a.flags.c_contiguous or not a.flags.writeable or a.size < size[name]:
+                raise MWError(f"export_many_into: buffer '{name}' must be writable C-contiguous "
+                              f"{np.dtype(dt).name} of >= {size[name]}")
+        counts.append(n)
+    _check(_lib.mw_tree_download_many(len(trees), (ctypes.c_void_p * max(1, len(trees)))(*[t._h for t in trees]),
+                                      *[_ptrs([b[k] for b in bufs]) for k in names]))
+    return counts
 
 
 def gauss_params(coefs, alphas, centers, powers=None):

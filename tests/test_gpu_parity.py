@@ -334,6 +334,7 @@ def test_config4_density_against_oracle(gpu_mod, oracle_mod):
             assert set(keyed(eg)) == set(keyed(eo)), flags
             assert G.distance(pot, back) / np.sqrt(back.square_norm()) <= prec / 10, flags
 
+
 def test_upload_download_roundtrip(gpu_mod, oracle_mod):
     G, O = gpu_mod, oracle_mod
     mg, mo = pair(G, O, 7)
@@ -369,6 +370,71 @@ def test_ordered_upload_and_export_into(gpu_mod):
     assert np.array_equal(bufs["child0"][:n], ea["child0"])
     with pytest.raises(G.MWError):
         b.export_into(dict(bufs, coef=np.zeros(5)))
+
+
+def _sibling_groups_reversed(e):
+    """The same tree in another valid node order: roots first, then the sibling groups (8 consecutive
+    nodes in the library's order) in reverse order, parent / child indices relinked."""
+    n = len(e["depth"])
+    nroot = int((e["depth"] == 0).sum())
+    order = np.array(list(range(nroot)) + [j for g in reversed(range(nroot, n, 8)) for j in range(g, g + 8)])
+    pos = np.empty(n, np.int64)
+    pos[order] = np.arange(n)
+    par, ch = e["parent"][order], e["child0"][order]
+    return dict(depth=e["depth"][order], trans=e["trans"][order], coef=e["coef"][order],
+                parent=np.where(par < 0, -1, pos[np.maximum(par, 0)]).astype(np.int32),
+                child0=np.where(ch < 0, -1, pos[np.maximum(ch, 0)]).astype(np.int32))
+
+
+def test_batched_upload_and_download(gpu_mod):
+    """load_many / export_many_into (mw_tree_upload_many / mw_tree_download_many) give exactly the trees
+    and buffers of one load / export_into per tree, for trees in the library's order and in another valid
+    order; a batch with an invalid or repeated tree is refused before anything is copied."""
+    G = gpu_mod
+    m = G.MultiResolutionAnalysis(*WORLD, 7, 14)
+    funcs = [two_gaussians(G), G.gauss_params([1.0], [2.0], [(0.2, 0.0, 0.0)]),
+             G.gauss_params([3.0], [40.0], [(-0.3, 0.1, 0.2)])]
+    src = []
+    for f in funcs:
+        t = G.FunctionTree(m)
+        G.project(1e-5, t, f)
+        src.append(t.export())
+    arrays = [src[0], _sibling_groups_reversed(src[1]), src[2]]
+    assert len(src[1]["depth"]) > 1000 and not np.array_equal(arrays[1]["trans"], src[1]["trans"])
+    names = ("depth", "trans", "parent", "child0", "coef")
+    one = [G.FunctionTree(m) for _ in arrays]
+    for t, a in zip(one, arrays):
+        t.load(*(a[k] for k in ("depth", "trans", "parent", "child0", "coef")))
+    many = [G.FunctionTree(m) for _ in arrays]
+    G.load_many(many, arrays)
+    for a, b in zip(one, many):
+        ea, eb = a.export(), b.export()
+        for k in names:
+            assert np.array_equal(ea[k], eb[k]), k
+        assert a.square_norm() == b.square_norm()
+    bufs = []
+    for t in many:
+        n, k = t.nnodes(), t.mra.k
+        bufs.append({"depth": np.zeros(n + 3, np.int32), "parent": np.zeros(n + 3, np.int32),
+                     "child0": np.zeros(n + 3, np.int32), "trans": np.zeros(3 * (n + 3), np.int64),
+                     "coef": np.zeros(n * (2 * k) ** 3 + 7)})
+    counts = G.export_many_into(many, bufs)
+    for t, b, c in zip(many, bufs, counts):
+        e = t.export()
+        assert c == t.nnodes()
+        assert np.array_equal(b["depth"][:c], e["depth"])
+        assert np.array_equal(b["trans"][:3 * c], e["trans"].ravel())
+        assert np.array_equal(b["parent"][:c], e["parent"])
+        assert np.array_equal(b["child0"][:c], e["child0"])
+        assert np.array_equal(b["coef"][:e["coef"].size], e["coef"].ravel())
+    bad = dict(src[1], trans=src[1]["trans"].copy())
+    bad["trans"][-1, 0] = 1 << 40
+    with pytest.raises(G.MWError):
+        G.load_many([many[0], many[1]], [src[2], bad])
+    with pytest.raises(G.MWError):
+        G.load_many([many[0], many[0]], [src[2], src[2]])
+    e0 = many[0].export()
+    assert np.array_equal(e0["coef"], src[0]["coef"]) and np.array_equal(e0["trans"], src[0]["trans"])
 
 
 def test_rescale_and_dot(gpu_mod, oracle_mod):
