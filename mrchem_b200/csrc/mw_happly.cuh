@@ -208,13 +208,13 @@ __device__ __forceinline__ float bf16_to_f32(uint16_t h) { return __uint_as_floa
 // tile is (rt, ct).  Fully unrolled, so the loads of step k + 1 issue ahead of the FMAs of step k.  Columns
 // 0-3 of the tile run as two packed FP32 pairs per row (fma.rn.f32x2, bit-identical to two fmaf), the
 // fifth column as single FMAs: 15 FMA instructions per step of a 5 x 5 tile instead of 25.
+// The tile's result stays packed: columns (0, 1) and (2, 3) of row i in p01[i] and p23[i], column 4 in c4[i].
 template <int MT, int NT, int NTILE, int LDA, int LDB, int KD>
-__device__ __forceinline__ void gemm_tile_split(const float* __restrict__ A, const float* __restrict__ B, int rt, int ct,
-                                                float (&c)[MT][NT]) {
+__device__ __forceinline__ void gemm_tile_packed(const float* __restrict__ A, const float* __restrict__ B, int rt,
+                                                 int ct, unsigned long long (&p01)[MT], unsigned long long (&p23)[MT],
+                                                 float (&c4)[MT]) {
     static_assert(MT == 4 || MT == 5, "tile");
     static_assert(NT == 4 || NT == 5, "tile");
-    unsigned long long p01[MT], p23[MT];
-    float c4[MT];
 #pragma unroll
     for (int i = 0; i < MT; ++i) {
         p01[i] = p23[i] = 0ull;  // (+0.0f, +0.0f)
@@ -245,11 +245,38 @@ __device__ __forceinline__ void gemm_tile_split(const float* __restrict__ A, con
             if constexpr (NT == 5) c4[i] = fmaf(a[i], b4, c4[i]);
         }
     }
+}
+template <int MT, int NT, int NTILE, int LDA, int LDB, int KD>
+__device__ __forceinline__ void gemm_tile_split(const float* __restrict__ A, const float* __restrict__ B, int rt, int ct,
+                                                float (&c)[MT][NT]) {
+    unsigned long long p01[MT], p23[MT];
+    float c4[MT];
+    gemm_tile_packed<MT, NT, NTILE, LDA, LDB, KD>(A, B, rt, ct, p01, p23, c4);
 #pragma unroll
     for (int i = 0; i < MT; ++i) {
         unpack_f32x2(p01[i], c[i][0], c[i][1]);
         unpack_f32x2(p23[i], c[i][2], c[i][3]);
         if constexpr (NT == 5) c[i][4] = c4[i];
+    }
+}
+__device__ __forceinline__ unsigned long long add_f32x2(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));  // two round-to-nearest adds
+    return d;
+}
+// acc (+)= the tile's result, in packed form (bit-identical to the scalar adds)
+template <int MT, int NT, int NTILE, int LDA, int LDB, int KD>
+__device__ __forceinline__ void gemm_tile_split_add(const float* __restrict__ A, const float* __restrict__ B, int rt,
+                                                    int ct, unsigned long long (&a01)[MT], unsigned long long (&a23)[MT],
+                                                    float (&a4)[MT]) {
+    unsigned long long p01[MT], p23[MT];
+    float c4[MT];
+    gemm_tile_packed<MT, NT, NTILE, LDA, LDB, KD>(A, B, rt, ct, p01, p23, c4);
+#pragma unroll
+    for (int i = 0; i < MT; ++i) {
+        a01[i] = add_f32x2(a01[i], p01[i]);
+        a23[i] = add_f32x2(a23[i], p23[i]);
+        if constexpr (NT == 5) a4[i] += c4[i];
     }
 }
 
@@ -483,7 +510,8 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
         const int nq = (C::NWARP - quarter + 3) / 4;  // warps of this lane quarter
         uint32_t lph = 0;
         bool plane_gen = true, first_line = true;
-        float yacc[MT][NT];
+        unsigned long long ya01[MT], ya23[MT];  // the plane's y sums of this thread's tile, packed as the GEMM's
+        float ya4[MT];
         bool lgen = true;
         for (int t = ch.c0; t < ch.c1; ++t) {
             const HTri h0 = rec(t);
@@ -561,27 +589,25 @@ __global__ void __launch_bounds__(HCfg<K>::NTHR, 1)
                 // line is zero when its z index c >= k)
                 if (first_line) {
 #pragma unroll
-                    for (int i = 0; i < MT; ++i)
-#pragma unroll
-                        for (int j = 0; j < NT; ++j) yacc[i][j] = 0.0f;
+                    for (int i = 0; i < MT; ++i) {
+                        ya01[i] = ya23[i] = 0ull;
+                        ya4[i] = 0.0f;
+                    }
                 }
                 if (!(lgen && !(tc0 < K))) {
-                    float c[MT][NT];
-                    if (lgen) gemm_tile_split<MT, NT, NTILE, KP, LDT, K>(My, T1, rt, ct, c);
-                    else gemm_tile_split<MT, NT, NTILE, KP, LDT, K2>(My, T1, rt, ct, c);
-#pragma unroll
-                    for (int i = 0; i < MT; ++i)
-#pragma unroll
-                        for (int j = 0; j < NT; ++j) yacc[i][j] += c[i][j];
+                    if (lgen) gemm_tile_split_add<MT, NT, NTILE, KP, LDT, K>(My, T1, rt, ct, ya01, ya23, ya4);
+                    else gemm_tile_split_add<MT, NT, NTILE, KP, LDT, K2>(My, T1, rt, ct, ya01, ya23, ya4);
                 }
                 if (pend) {  // the plane's y sums -> T2[c][a' + P b'] for the z step
                     float* row = T2 + tc0 * LDT;
 #pragma unroll
                     for (int i = 0; i < MT; ++i) {
                         const int m = tb0 + KP * (o0 + i);  // column a' + P b' of the tile's first value
-                        *reinterpret_cast<float4*>(row + 4 * (m / NT)) =
-                            make_float4(yacc[i][0], yacc[i][1], yacc[i][2], yacc[i][3]);
-                        if constexpr (NT == 5) row[4 * NTILE + m / NT] = yacc[i][4];
+                        float y0, y1, y2, y3;
+                        unpack_f32x2(ya01[i], y0, y1);
+                        unpack_f32x2(ya23[i], y2, y3);
+                        *reinterpret_cast<float4*>(row + 4 * (m / NT)) = make_float4(y0, y1, y2, y3);
+                        if constexpr (NT == 5) row[4 * NTILE + m / NT] = ya4[i];
                     }
                 }
             }
