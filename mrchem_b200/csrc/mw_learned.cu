@@ -54,9 +54,12 @@ struct FeatTree {
 __device__ inline float lg(double v) { return (float)(log10(v + 1e-30) * 0.1); }
 
 // one thread per (entry, node): writes kNF features
+// One warp per candidate node: lane j < 27 takes neighbour j (dz, dy, dx in -1..1, dx fastest), lane 27
+// the node's own features; the neighbours' hash probes and ancestor walks run side by side
 __global__ void k_features(const int2* __restrict__ items, int n, const FeatTree* __restrict__ trees, float* F) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= n || lane > 27) return;
     const int2 it = items[i];
     const FeatTree& T = trees[it.x];
     const uint64_t key = T.okey[it.y];
@@ -65,32 +68,31 @@ __global__ void k_features(const int2* __restrict__ items, int n, const FeatTree
     key_trans(key, t);
     const double thr = T.thr0 * pow(2.0, -0.5 * d);
     float* f = F + (size_t)i * kNF;
+    if (lane < 27) {
+        const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
+        const long long u[3] = {t[0] + dx, t[1] + dy, t[2] + dz};
+        bool inside = true;
+        for (int q = 0; q < 3; ++q) inside &= u[q] >= 0 && u[q] < ((long long)T.boxes[q] << d);
+        float fb = -3.0f, fw = -3.0f;
+        if (inside) {
+            int idx = hlookup(T.hkey, T.hval, T.hcap, make_key(d, u[0], u[1], u[2]));
+            if (idx >= 0) {
+                fb = lg(sqrt(T.inorm2[idx]) / thr);
+                fw = lg(sqrt(T.iwnorm2[idx]) / thr);
+            } else {
+                for (int da = d - 1; da >= 0 && idx < 0; --da) {
+                    const int sh = d - da;
+                    idx = hlookup(T.hkey, T.hval, T.hcap, make_key(da, u[0] >> sh, u[1] >> sh, u[2] >> sh));
+                    if (idx >= 0) fb = lg(sqrt(T.inorm2[idx]) * pow(2.0, -1.5 * sh) / thr);
+                }
+            }
+        }
+        f[4 + 2 * lane] = fb;
+        f[5 + 2 * lane] = fw;
+        return;
+    }
     f[0] = d / 16.0f;
     for (int q = 0; q < 3; ++q) f[1 + q] = (float)(2.0 * (t[q] + 0.5) / ((double)T.boxes[q] * (1ll << d)) - 1.0);
-    int p = 4;
-    for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx) {
-                const long long u[3] = {t[0] + dx, t[1] + dy, t[2] + dz};
-                bool inside = true;
-                for (int q = 0; q < 3; ++q) inside &= u[q] >= 0 && u[q] < ((long long)T.boxes[q] << d);
-                float fb = -3.0f, fw = -3.0f;
-                if (inside) {
-                    int idx = hlookup(T.hkey, T.hval, T.hcap, make_key(d, u[0], u[1], u[2]));
-                    if (idx >= 0) {
-                        fb = lg(sqrt(T.inorm2[idx]) / thr);
-                        fw = lg(sqrt(T.iwnorm2[idx]) / thr);
-                    } else {
-                        for (int da = d - 1; da >= 0 && idx < 0; --da) {
-                            const int sh = d - da;
-                            idx = hlookup(T.hkey, T.hval, T.hcap, make_key(da, u[0] >> sh, u[1] >> sh, u[2] >> sh));
-                            if (idx >= 0) fb = lg(sqrt(T.inorm2[idx]) * pow(2.0, -1.5 * sh) / thr);
-                        }
-                    }
-                }
-                f[p++] = fb;
-                f[p++] = fw;
-            }
     f[58] = (float)log10(T.mu + 1e-3);
     f[59] = (float)(log10(T.prec) * 0.1);
     const double edge = ldexp(1.0, -(T.n0 + d));
@@ -339,7 +341,7 @@ float* features(Ctx* ctx, std::vector<FeatCtx>& fc, const std::vector<int2>& ite
     int2* d_items = (int2*)dalloc(ctx, sizeof(int2) * n);
     upload_bytes(ctx, s, d_ft, ft.data(), sizeof(FeatTree) * ft.size());  // staged: ft / items may go
     upload_bytes(ctx, s, d_items, items.data(), sizeof(int2) * n);
-    k_features<<<(n + 127) / 128, 128, 0, s>>>(d_items, n, d_ft, d_F);
+    k_features<<<(unsigned)(((size_t)n * 32 + 255) / 256), 256, 0, s>>>(d_items, n, d_ft, d_F);  // a warp per node
     MWB_CUDA(cudaGetLastError());
     if (s != ctx->stream) MWB_CUDA(cudaStreamSynchronize(s));  // pageable copies: ft / items leave scope
     dfree(ctx, d_ft);
