@@ -184,6 +184,38 @@ __global__ void k_bresolve_gen(int* csrc, int ncand, const uint64_t* __restrict_
 // 2. generated input nodes: reconstruct the leaf ancestor, take the child on the path, descend
 //    with zero wavelets (s_c = H_c^T s per dimension)
 // ---------------------------------------------------------------------------------------------
+// One direction of the two-scale reconstruction of a padded (2k)^3 shared block (out[o] = sum_i M[o][i]
+// in[i], as pencil_transform) restricted to what child cc needs: outputs o in [cc[DIM] k, cc[DIM] k + k)
+// only, on the pencils whose earlier directions' indices lie in the child's halves.
+template <int K, int DIM>
+__device__ static inline void child_transform(const double* __restrict__ M, double* A, const int (&cc)[3]) {
+    using G = Geo<K>;
+    constexpr int NPC = DIM == 0 ? G::K2 * G::K2 : DIM == 1 ? K * G::K2 : K * K;
+    for (int p = threadIdx.x; p < NPC; p += blockDim.x) {
+        int base, stride;
+        if (DIM == 0) {  // all (y, z)
+            base = G::P * ((p % G::K2) + G::K2 * (p / G::K2));
+            stride = 1;
+        } else if (DIM == 1) {  // x in the child's half, all z
+            base = (cc[0] * K + p % K) + G::P * G::K2 * (p / K);
+            stride = G::P;
+        } else {  // x and y in the child's halves
+            base = (cc[0] * K + p % K) + G::P * (cc[1] * K + p / K);
+            stride = G::P * G::K2;
+        }
+        double x[G::K2];
+#pragma unroll
+        for (int i = 0; i < G::K2; ++i) x[i] = A[base + i * stride];
+#pragma unroll 1
+        for (int o = cc[DIM] * K; o < cc[DIM] * K + K; ++o) {
+            double s = 0.0;
+#pragma unroll
+            for (int i = 0; i < G::K2; ++i) s = fma(M[o * G::K2 + i], x[i], s);
+            A[base + o * stride] = s;
+        }
+    }
+}
+
 template <int K>
 __global__ void __launch_bounds__(256) k_bgenerate(const uint64_t* __restrict__ ukey, const int* __restrict__ uleaf,
                                                    const BTree* __restrict__ trees,
@@ -204,19 +236,21 @@ __global__ void __launch_bounds__(256) k_bgenerate(const uint64_t* __restrict__ 
         const int a = e % G::K2, b = (e / G::K2) % G::K2, c = e / (G::K2 * G::K2);
         A[G::at(a, b, c)] = T.in.coef[(size_t)leaf * G::BS + e];
     }
-    __syncthreads();
-    pencil_transform<K, 0>(M, A);
-    __syncthreads();
-    pencil_transform<K, 1>(M, A);
-    __syncthreads();
-    pencil_transform<K, 2>(M, A);
-    __syncthreads();
     long long t[3], tl[3];
     key_trans(gkey & ((1ull << 57) - 1), t);
     key_trans(T.inkey[leaf], tl);
     const int dl = depth - key_depth(T.inkey[leaf]);
-    int cc[3];
+    int cc[3];  // the leaf's child on the way down
     for (int q = 0; q < 3; ++q) cc[q] = (int)((t[q] >> (dl - 1)) - 2 * tl[q]);
+    __syncthreads();
+    // the leaf's reconstruction restricted to child cc: each direction computes only the outputs of the
+    // child's half, over the inputs the next direction reads (same sums as the full transform)
+    child_transform<K, 0>(M, A, cc);
+    __syncthreads();
+    child_transform<K, 1>(M, A, cc);
+    __syncthreads();
+    child_transform<K, 2>(M, A, cc);
+    __syncthreads();
     for (int e = threadIdx.x; e < K * K * K; e += blockDim.x) {
         const int a = e % K, b = (e / K) % K, c = e / (K * K);
         S[e] = A[G::at(cc[0] * K + a, cc[1] * K + b, cc[2] * K + c)];
