@@ -1463,9 +1463,8 @@ static void* launch_simage(Ctx* ctx, long long nimg, const ImgSrc* d_srcs, int n
                            long long nreal, cudaStream_t s) {
     if constexpr (HCfg<K>::FITS) {
         void* img = dalloc(ctx, (size_t)nimg * HCfg<K>::IMGB);
-        const int smem = (int)(sizeof(double) * 4 * K * K * (2 * K + 1));
-        MWB_CUDA(cudaFuncSetAttribute(k_simage<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        k_simage<K><<<(unsigned)nimg, 512, smem, s>>>(d_srcs, nt, d_gblk, nreal, (unsigned char*)img);
+        const long long rows = nimg * (long long)HCfg<K>::R;  // one thread per data row
+        k_simage<K><<<(unsigned)((rows + 255) / 256), 256, 0, s>>>(d_srcs, nt, d_gblk, nreal, nimg, (unsigned char*)img);
         return img;
     } else {
         throw Error(-1, "BF16x3 engine: unsupported order");

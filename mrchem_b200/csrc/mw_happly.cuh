@@ -111,19 +111,22 @@ struct HCfg {
                                  SMEM + SMEM_STATIC <= 232448 && 2 * NCT <= NCW && 8 * KKK <= 4 * KP * LDT && NWARP >= 8 && (TILES * 128 - R) * 16 <= OPB;
 };
 
-// Block images of the tensor-core x step, one CTA per block: the FP64 block (or the generated k^3
-// scaling block) is read coalesced into shared memory (row stride K2 + 1 doubles: no bank conflicts
-// between the rows of a warp), every data row (y, z) is sliced (mw_slice.hpp) and written as 16-byte
-// chunks.  Slot numbering as k_ximage.
+// Block images of the tensor-core x step, one thread per data row (y, z) of a block: the row's 2k FP64
+// values are contiguous in the block (x fastest), so a warp reads 32 consecutive rows as whole sectors
+// straight from global memory (16-byte streaming loads, nothing staged in shared memory); the row is
+// sliced (mw_slice.hpp) and written as 16-byte chunks, consecutive rows side by side.  A generated node's
+// rows come from its k^3 scaling block (zero where y, z or x >= k).  Slot numbering as k_ximage.
 template <int K>
-__global__ void __launch_bounds__(512) k_simage(const ImgSrc* __restrict__ srcs, int nsrc, const double* __restrict__ gblk,
-                                                long long nreal, unsigned char* __restrict__ img) {
+__global__ void __launch_bounds__(256) k_simage(const ImgSrc* __restrict__ srcs, int nsrc, const double* __restrict__ gblk,
+                                                long long nreal, long long nimg, unsigned char* __restrict__ img) {
     using C = HCfg<K>;
-    constexpr int K2 = C::K2, R = C::R, NCHM = C::NCHM, BS = K2 * K2 * K2, KKK = K * K * K, LDR = K2 + 1;
-    constexpr int NLD = (BS + 511) / 512;  // values per thread (512 threads)
-    extern __shared__ __align__(16) unsigned char smraw[];
-    double* blk = reinterpret_cast<double*>(smraw);  // [R][LDR]
-    const long long slot = blockIdx.x;
+    constexpr int K2 = C::K2, R = C::R, NCHM = C::NCHM, BS = K2 * K2 * K2, KKK = K * K * K;
+    static_assert(K2 % 2 == 0, "rows of whole 16-byte pairs");
+    const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long slot = gid / R;
+    const int r = (int)(gid - slot * R);
+    if (slot >= nimg) return;
+    double row[K2];
     if (slot < nreal) {
         int lo = 0, hi = nsrc - 1;  // last entry with base <= slot
         while (lo < hi) {
@@ -132,72 +135,54 @@ __global__ void __launch_bounds__(512) k_simage(const ImgSrc* __restrict__ srcs,
             else hi = mid - 1;
         }
         const ImgSrc sr = srcs[lo];
-        const double* b = sr.coef + (size_t)(sr.lb + (slot - sr.base)) * BS;
-        double v[NLD];  // every load of this thread in flight before the first shared store
+        const double2* b = reinterpret_cast<const double2*>(sr.coef + (size_t)(sr.lb + (slot - sr.base)) * BS + (size_t)r * K2);
 #pragma unroll
-        for (int i = 0; i < NLD; ++i) {
-            const int e = threadIdx.x + 512 * i;
-            v[i] = e < BS ? __ldcs(b + e) : 0.0;
-        }
-#pragma unroll
-        for (int i = 0; i < NLD; ++i) {
-            const int e = threadIdx.x + 512 * i;
-            if (e < BS) blk[(e / K2) * LDR + e % K2] = v[i];
+        for (int i = 0; i < K2 / 2; ++i) {
+            const double2 u = __ldcs(b + i);
+            row[2 * i] = u.x;
+            row[2 * i + 1] = u.y;
         }
     } else {
         const double* g = gblk + (size_t)(slot - nreal) * KKK;
-        double v[NLD];
+        const int y = r % K2, z = r / K2;
 #pragma unroll
-        for (int i = 0; i < NLD; ++i) {
-            const int e = threadIdx.x + 512 * i;
-            const int a = e % K2, bb = (e / K2) % K2, c = e / (K2 * K2);
-            v[i] = (e < BS && a < K && bb < K && c < K) ? g[a + K * (bb + K * c)] : 0.0;
-        }
-#pragma unroll
-        for (int i = 0; i < NLD; ++i) {
-            const int e = threadIdx.x + 512 * i;
-            if (e < BS) blk[(e / K2) * LDR + e % K2] = v[i];
-        }
+        for (int x = 0; x < K2; ++x) row[x] = (x < K && y < K && z < K) ? g[x + K * (y + K * z)] : 0.0;
     }
-    __syncthreads();
     unsigned char* out = img + (size_t)slot * C::IMGB;
-    auto put = [&](int chunk, int r, const float* v) {
+    auto put = [&](int chunk, const float* v) {
         uint32_t w[4];
 #pragma unroll
         for (int h = 0; h < 4; ++h)
             w[h] = (uint32_t)bf16_bits_exact(v[2 * h]) | ((uint32_t)bf16_bits_exact(v[2 * h + 1]) << 16);
         *reinterpret_cast<uint4*>(out + ((size_t)chunk * R + r) * 16) = make_uint4(w[0], w[1], w[2], w[3]);
     };
-    for (int r = threadIdx.x; r < R; r += blockDim.x) {
-        const double* row = blk + r * LDR;
-        double m = 0.0;
+    double m = 0.0;
 #pragma unroll
-        for (int x = 0; x < K2; ++x) m = fmax(m, fabs(row[x]));
-        int e = 0;
-        if (m > 0.0) frexp(m, &e);
-        const double scale = ldexp(1.0, -e);
-        const float inv256 = ldexpf(1.0f, e - 8);
+    for (int x = 0; x < K2; ++x) m = fmax(m, fabs(row[x]));
+    int e = 0;
+    if (m > 0.0) frexp(m, &e);
+    const double scale = ldexp(1.0, -e);
+    const float inv256 = ldexpf(1.0f, e - 8);
 #pragma unroll
-        for (int c = 0; c < NCHM; ++c) {  // x = 8 c .. 8 c + 7 of the four slices
-            float s[4][8];
+    for (int c = 0; c < NCHM; ++c) {  // x = 8 c .. 8 c + 7 of the four slices
+        float s[4][8];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                if (8 * c + j < K2) slice4_value(row[8 * c + j], scale, inv256, s[0][j], s[1][j], s[2][j], s[3][j]);
-                else s[0][j] = s[1][j] = s[2][j] = s[3][j] = 0.0f;
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q) put(q * NCHM + c, r, s[q]);
+        for (int j = 0; j < 8; ++j) {
+            if (8 * c + j < K2) slice4_value(row[8 * c + j], scale, inv256, s[0][j], s[1][j], s[2][j], s[3][j]);
+            else s[0][j] = s[1][j] = s[2][j] = s[3][j] = 0.0f;
         }
-        if constexpr (C::PACK) {  // [s0 | s1 | s2 | s3] of x = 16 .., four K slots per slice
-            float pk[16];
 #pragma unroll
-            for (int l = 0; l < 4; ++l) {
-                if (16 + l < K2) slice4_value(row[16 + l], scale, inv256, pk[l], pk[4 + l], pk[8 + l], pk[12 + l]);
-                else pk[l] = pk[4 + l] = pk[8 + l] = pk[12 + l] = 0.0f;
-            }
-            put(4 * NCHM, r, pk);
-            put(4 * NCHM + 1, r, pk + 8);
+        for (int q = 0; q < 4; ++q) put(q * NCHM + c, s[q]);
+    }
+    if constexpr (C::PACK) {  // [s0 | s1 | s2 | s3] of x = 16 .., four K slots per slice
+        float pk[16];
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            if (16 + l < K2) slice4_value(row[16 + l], scale, inv256, pk[l], pk[4 + l], pk[8 + l], pk[12 + l]);
+            else pk[l] = pk[4 + l] = pk[8 + l] = pk[12 + l] = 0.0f;
         }
+        put(4 * NCHM, pk);
+        put(4 * NCHM + 1, pk + 8);
     }
 }
 
