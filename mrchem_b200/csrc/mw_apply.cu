@@ -1345,6 +1345,12 @@ __global__ void __launch_bounds__(GCfg<K, R>::NTHR, GCfg<K, R>::MINB)
 #include "mw_happly.cuh"
 namespace mwb {
 
+// triples of every chunk (the sort key of the longest-first launch order); chunks never exceed 2^16 triples
+__global__ void k_chunk_len(const Chunk* __restrict__ chunks, int n, int* __restrict__ len) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) len[i] = min(chunks[i].c1 - chunks[i].c0, 65535);
+}
+
 // add the partial blocks of a multi-chunk node in chunk order; write block and norms
 template <int K>
 __global__ void __launch_bounds__(256) k_breduce(const Chunk* __restrict__ chunks, const int* __restrict__ choff,
@@ -1746,6 +1752,23 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     MWB_CUDA(cudaGetLastError());
     count(ctx);
     double* d_partials = (double*)dalloc(ctx, sizeof(double) * BS * std::max(1, nslots));
+    // the tensor-core engine runs a copy of the chunk list sorted longest first, so that a launch's last
+    // wave of CTAs holds the short chunks (the reduction keeps reading the list in item order)
+    Chunk* d_run = d_chunks;
+    if (hyb && nchunks > 1) {
+        int* d_len = (int*)dalloc(ctx, sizeof(int) * 2 * (size_t)nchunks);
+        d_run = (Chunk*)dalloc(ctx, sizeof(Chunk) * (size_t)nchunks);
+        k_chunk_len<<<(nchunks + 255) / 256, 256, 0, s>>>(d_chunks, nchunks, d_len);
+        size_t tmp = 0;
+        MWB_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, d_len, d_len + nchunks, d_chunks, d_run, nchunks,
+                                                           0, 16, s));
+        void* d_tmp = dalloc(ctx, tmp);
+        MWB_CUDA(cub::DeviceRadixSort::SortPairsDescending(d_tmp, tmp, d_len, d_len + nchunks, d_chunks, d_run, nchunks,
+                                                           0, 16, s));
+        dfree(ctx, d_tmp);
+        dfree(ctx, d_len);
+        count(ctx, 2);
+    }
 
     // 5. contraction + reduction of multi-chunk nodes
     unsigned long long* d_ntrip_tot = (unsigned long long*)dalloc(ctx, 2 * sizeof(unsigned long long));
@@ -1755,7 +1778,7 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
 #define L_AP(KK)                                                                                             \
     {                                                                                                        \
         if (hyb) {                                                                                           \
-            launch_happly<KK>(nchunks, d_chunks, d_items, d_trees, d_tkey, d_tval, d_csrc,                   \
+            launch_happly<KK>(nchunks, d_run, d_items, d_trees, d_tkey, d_tval, d_csrc,                      \
                               (const unsigned char*)d_ximg, nreal, d_partials, d_ntrip_tot, d_kerr, s);       \
         } else if (bp.precision == 2 && TCfg<KK>::FITS && !pencil && tc_prec_ok) {                           \
             size_t smem = TCfg<KK>::SMEM;                                                                    \
@@ -1792,6 +1815,7 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
 #undef L_AP
     MWB_CUDA(cudaGetLastError());
     if (ctx->prof) MWB_CUDA(cudaEventRecord(ctx->ev1, s));
+    if (d_run != d_chunks) dfree(ctx, d_run);
     count(ctx);
     ctx->apply_launches++;
     ctx->apply_ctas += nchunks;
