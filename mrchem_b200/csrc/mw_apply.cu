@@ -1752,10 +1752,11 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
     MWB_CUDA(cudaGetLastError());
     count(ctx);
     double* d_partials = (double*)dalloc(ctx, sizeof(double) * BS * std::max(1, nslots));
-    // the tensor-core engine runs a copy of the chunk list sorted longest first, so that a launch's last
-    // wave of CTAs holds the short chunks (the reduction keeps reading the list in item order)
+    // the line-ordered engines (tensor-core and CUDA-core) run a copy of the chunk list sorted longest
+    // first, so that a launch's last wave of CTAs holds the short chunks (the reduction keeps reading the
+    // list in item order)
     Chunk* d_run = d_chunks;
-    if (hyb && nchunks > 1) {
+    if (lined && nchunks > 1) {
         int* d_len = (int*)dalloc(ctx, sizeof(int) * 2 * (size_t)nchunks);
         d_run = (Chunk*)dalloc(ctx, sizeof(Chunk) * (size_t)nchunks);
         k_chunk_len<<<(nchunks + 255) / 256, 256, 0, s>>>(d_chunks, nchunks, d_len);
@@ -1788,13 +1789,13 @@ void run_batch_pass(BatchPass& bp, cudaStream_t s) {
         } else if (bp.precision >= 1 && GCfg<KK, float>::FITS && !pencil) {                                  \
             size_t smem = GCfg<KK, float>::SMEM;                                                             \
             MWB_CUDA(cudaFuncSetAttribute(k_gapply<KK, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-            k_gapply<KK, float><<<nchunks, GCfg<KK, float>::NTHR, smem, s>>>(d_chunks, d_items, d_trees, d_tkey, \
+            k_gapply<KK, float><<<nchunks, GCfg<KK, float>::NTHR, smem, s>>>(d_run, d_items, d_trees, d_tkey,    \
                                                                               d_tval, d_csrc, (const float*)d_ximg, \
                                                                               nreal, d_partials, d_ntrip_tot);     \
         } else if (bp.precision != 1 && GCfg<KK, double>::FITS && !pencil) {                                  \
             size_t smem = GCfg<KK, double>::SMEM;                                                            \
             MWB_CUDA(cudaFuncSetAttribute(k_gapply<KK, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-            k_gapply<KK, double><<<nchunks, GCfg<KK, double>::NTHR, smem, s>>>(d_chunks, d_items, d_trees, d_tkey, \
+            k_gapply<KK, double><<<nchunks, GCfg<KK, double>::NTHR, smem, s>>>(d_run, d_items, d_trees, d_tkey,   \
                                                                                 d_tval, d_csrc, (const double*)d_ximg, \
                                                                                 nreal, d_partials, d_ntrip_tot);    \
         } else if (bp.precision >= 1) {                                                                      \
